@@ -1,0 +1,76 @@
+"""Pins the FP64 oracle to the gromosXX reference runs shipped with gromos-rs.
+
+Step-0 LJ and CRF energy totals must agree to the fixtures' 10 significant
+digits (relative 1e-8, the tolerance the reference's own harness uses,
+crates/gromos-md/tests/test_gromosXX_references.rs:22-25); step-0 forces must
+agree to 1e-6 kJ/(mol nm) wherever the fixture has no covalent energy (then
+FREEFORCERED is the pure nonbonded force); the per-energy-group nonbonded
+block of ch4_water_fep pins the group attribution.
+"""
+import numpy as np
+import pytest
+
+import oracle_binding as ob
+from golden_loader import FIXTURE_NAMES, load_fixture
+
+
+@pytest.mark.parametrize("name", FIXTURE_NAMES)
+def test_step0_energies(name):
+    s, ex = load_fixture(name)
+    r = ob.OracleForcefield(s).apply()
+    for key in ("e_lj", "e_crf"):
+        want = ex[key]
+        assert abs(r[key] - want) <= 1e-8 * max(abs(want), 1e-12) + 1e-12, (key, r[key], want)
+
+
+@pytest.mark.parametrize("name", FIXTURE_NAMES)
+def test_step0_forces(name):
+    s, ex = load_fixture(name)
+    if ex["e_covalent"] != 0.0:
+        pytest.skip("fixture forces include bonded terms")
+    r = ob.OracleForcefield(s).apply()
+    assert r["forces"].shape == ex["forces"].shape
+    np.testing.assert_allclose(r["forces"], ex["forces"], atol=1e-6, rtol=0)
+
+
+def test_energy_group_split_fep():
+    s, ex = load_fixture("ch4_water_fep")
+    r = ob.OracleForcefield(s).apply()
+    g = ex["nonbonded_groups"]  # rows (1,1), (1,2), (2,2); columns LJ, CRF, ...
+    got_lj = [r["egroup_lj"][0, 0], r["egroup_lj"][0, 1], r["egroup_lj"][1, 1]]
+    got_crf = [r["egroup_crf"][0, 0], r["egroup_crf"][0, 1], r["egroup_crf"][1, 1]]
+    np.testing.assert_allclose(got_lj, g[:, 0], rtol=1e-8, atol=1e-9)
+    np.testing.assert_allclose(got_crf, g[:, 1], rtol=1e-8, atol=1e-9)
+    assert abs(sum(got_lj) - r["e_lj"]) < 1e-8 * abs(r["e_lj"])
+
+
+def test_lambda_params_known_answers():
+    """perturbed.rs:715-745: λ = 0.5, n = 2."""
+    import ctypes as C
+    out = np.zeros(17)
+    ob.lib().orc_lambda_params(0.5, 0.5, 0.5, 0.5, 1.0, 1.0, 1.0, 1.0, 2, out.ctypes.data_as(C.POINTER(C.c_double)))
+    a_lj_n, b_lj_n, _, _, a_lj_n1, b_lj_n1 = out[:6]
+    assert b_lj_n == 0.25 and a_lj_n == 0.25
+    assert b_lj_n1 == 0.5 and a_lj_n1 == 0.5
+    assert out[11] == 0.25 and out[10] == 0.25  # b_ljs2, a_ljs2
+
+
+def test_crf_parameters():
+    """CRFParameters::new(1.4, 1, 61, 0) closed form (params.rs:78-96)."""
+    c = ob.crf_params(1.4, 1.0, 61.0, 0.0)
+    crf = 2.0 * (1.0 - 61.0) / (1.0 + 2.0 * 61.0)
+    assert np.isclose(c[2], crf / 1.4**3, rtol=1e-15)
+    assert np.isclose(c[1], crf / 1.4**3 / 2, rtol=1e-15)
+    assert np.isclose(c[0], (1 - crf / 2) / 1.4, rtol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["water_216_box", "water_1000_spc_gridcell", "ch4_water_fep", "nacl_water_box"])
+def test_cell_list_matches_standard(name):
+    """pairlist.rs:1121-1302: Standard and CellList give the same pair SET."""
+    s, _ = load_fixture(name)
+    a = ob.pairlist(s, algorithm=0)
+    b = ob.pairlist(s, algorithm=2)
+    for k in range(4):
+        sa = set(map(tuple, np.sort(a[k], axis=1).tolist()))
+        sb = set(map(tuple, np.sort(b[k], axis=1).tolist()))
+        assert sa == sb, (k, len(sa), len(sb))
