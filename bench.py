@@ -1,0 +1,309 @@
+#!/usr/bin/env python
+"""Benchmark of the gromos-rs nonbonded hot path on B200.
+
+Workload (one "step" = one Forcefield::apply nonbonded evaluation): 30,000
+SPC waters (90,000 atoms) in a 9.65 nm cubic box, twin-range cutoffs
+0.8/1.4 nm, reaction field EPSRF 61, pairlist rebuilt every NSNB = 5 steps;
+short-range pairs every step, long-range pairs (twin-range cache) at every
+rebuild.  Synthetic seeded coordinates (no external data).
+
+Metric: atom-pair interactions per second (pair-int/s) = atom pairs of the
+listed charge-group pairs evaluated per step (short every step, long on
+rebuild steps) / device time; ns/day follows for dt = 2 fs.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--kernel fixed|plain]
+  python bench.py --impl reference ...   # CPU reference arm (FP64, all host threads)
+
+Under torchrun each rank evaluates its own replica of the workload (the
+path has no exchange step: replicas only); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "gromos-rs_b200"), os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+DT_PS = 0.002
+OPS_PER_PAIR = 37          # FP32 pipe ops per atom pair, energies + virial step
+METRIC = "pair-int/s"
+WORKLOAD = "spc30000_twinrange_0.8_1.4_nsnb5"
+
+
+def ns_per_day(ms_per_step: float) -> float:
+    return 86400.0 / (ms_per_step * 1e-3) * DT_PS * 1e-3
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_sample(seconds_budget: float = 20.0):
+    """FP64 oracle (threaded fold/reduce) on the host's cores: a bounded sample
+    of the same workload (one rebuild + short-range steps)."""
+    import oracle_binding as ob
+    from gromos_nb import generators
+
+    s = generators.config2_spc30000()
+    nth = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    orc = ob.OracleForcefield(s, nthreads=nth)
+    t_build = time.perf_counter() - t0
+    lists = ob.pairlist(s, algorithm=2, nthreads=nth)
+    n_short = len(lists[0]) + 9 * len(lists[2])
+    n_long = len(lists[1]) + len(lists[3])
+    steps = 0
+    pairs = 0
+    t0 = time.perf_counter()
+    while True:
+        orc.apply(s.pos)
+        pairs += n_short + (n_long if steps % s.params.nsnb == 0 else 0)
+        steps += 1
+        el = time.perf_counter() - t0
+        if steps >= s.params.nsnb and (el > seconds_budget / 2 or steps >= 10):
+            break
+    el = time.perf_counter() - t0 + t_build  # the first pairlist build is part of the work
+    orc.close()
+    return {"value": pairs / el, "unit": METRIC, "cores": nth, "kind": "port",
+            "sample": f"{steps} Forcefield::apply steps of {WORKLOAD} incl. 1 cell-list pairlist build and "
+                      f"1 long-range refresh, FP64 C++ restatement, {nth} threads",
+            "ms_per_step": 1e3 * el / steps}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import oracle_binding as ob
+    from gromos_nb import generators
+
+    s = generators.config2_spc30000()
+    nth = os.cpu_count() or 1
+    lists = ob.pairlist(s, algorithm=2, nthreads=nth)
+    n_short = len(lists[0]) + 9 * len(lists[2])
+    n_long = len(lists[1]) + len(lists[3])
+    orc = ob.OracleForcefield(s, nthreads=nth)
+    for _ in range(args.warmup):
+        orc.apply(s.pos)
+    # continue the NSNB cadence from where warm-up left it
+    pairs = 0
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        orc.apply(s.pos)
+        pairs += n_short + (n_long if (args.warmup + k) % s.params.nsnb == 0 else 0)
+    el = time.perf_counter() - t0
+    orc.close()
+    v = pairs / el
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "ns_per_day": ns_per_day(1e3 * el / args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded SPC water box)",
+            "config": {"workload": WORKLOAD, "n_atoms": s.topo.n_atoms, "rcutp": 0.8, "rcutl": 1.4, "nsnb": 5,
+                       "pairlist": "cell list", "parallelism": f"host threads x{nth}"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": nth, "kind": "port",
+                             "sample": f"{args.steps} steps of {WORKLOAD}, FP64 C++ restatement of the gromos-rs "
+                                       f"nonbonded path (the Rust reference cannot be built here), {nth} threads"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+
+    from gromos_nb import generators
+    from gromos_nb.nonbonded import Forcefield, ffma_peak
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    s = generators.config2_spc30000(seed=1002 + rank)
+    ff = Forcefield(s, kernel=args.kernel, device=local_rank)
+    # pair counts of this configuration (short per step, long per rebuild)
+    r0 = ff.apply(s.pos, count_pairs=True)
+    n_short, n_long = int(r0["n_pairs_short"]), int(r0["n_pairs_long"])
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        ff.eval_async()
+    torch.cuda.synchronize()
+    # continue the cadence: the next eval after (1 + warmup) evals
+    evals_done = 1 + args.warmup
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = ff.launches()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms, short_ms, long_ms = [], [], []
+    pairs = 0
+    rebuilds = 0
+    for k in range(args.steps):
+        flush.zero_()                      # L2 flush between steps (not in the step's events)
+        torch.cuda.synchronize()
+        rebuild = (evals_done % s.params.nsnb) == 0
+        ff.eval_async()
+        evals_done += 1
+        t = ff.timings()                   # CUDA events on the library's stream
+        step_ms.append(t[4])
+        if rebuild:
+            rebuilds += 1
+            long_ms.append(t[2])
+        else:
+            short_ms.append(t[1])
+        pairs += n_short + (n_long if rebuild else 0)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches = ff.launches() - launches0
+    clk = clocks.stop()
+    total_ms = float(sum(step_ms))
+    if dist is not None:
+        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        pp = torch.tensor([float(pairs)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(pp, op=dist.ReduceOp.SUM)
+        pairs_all = float(pp.item())
+    else:
+        pairs_all = float(pairs)
+    value = pairs_all / (total_ms * 1e-3)
+    ms_per_step = total_ms / args.steps
+    # end to end through the public API: host positions in, host forces out
+    pinned = torch.from_numpy(np.ascontiguousarray(s.pos)).pin_memory().numpy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_pairs = 0
+    for k in range(args.steps):
+        rebuild = (evals_done % s.params.nsnb) == 0
+        ff.apply(pinned, count_pairs=False)
+        evals_done += 1
+        e2e_pairs += n_short + (n_long if rebuild else 0)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = e2e_pairs * world / e2e_s
+    h2d = s.topo.n_atoms * 3 * 8
+    d2h = s.topo.n_atoms * 3 * 8 + 8 * (2 * ff.G * ff.G + 10)
+    out = None
+    if rank == 0:
+        peak = ffma_peak(local_rank)
+        t_short = statistics.median(short_ms) if short_ms else float("nan")
+        achieved = OPS_PER_PAIR * n_short / (t_short * 1e-3)
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline_sample()
+        out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "ns_per_day": ns_per_day(ms_per_step) * 1.0,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64",
+               "data": "synthetic (seeded SPC water box)",
+               "config": {"workload": WORKLOAD, "n_atoms": s.topo.n_atoms, "box_nm": 9.65, "rcutp": 0.8,
+                          "rcutl": 1.4, "nsnb": 5, "kernel": args.kernel, "pairs_short_per_step": n_short,
+                          "pairs_long_per_rebuild": n_long, "rebuild_steps_timed": rebuilds,
+                          "l2": "flushed (256 MiB write) between steps, outside the step events",
+                          "step": "force evaluation only (positions static; MD integration not timed)",
+                          "parallelism": "replicas" if world > 1 else "single system"},
+               "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+               "roofline": {"bound": "fp32", "kernel": "k_water_force (short range) + k_water_prep",
+                            "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s (FP32 pipe)",
+                            "frac": achieved / peak, "traffic": None,
+                            "peak_source": "measured FFMA-chain kernel (gr_ffma_peak), one FFMA = one op",
+                            "ops_per_pair": OPS_PER_PAIR, "short_kernel_ms": t_short,
+                            "long_kernel_ms": statistics.median(long_ms) if long_ms else None},
+               "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
+        print(json.dumps(out), flush=True)
+    ff.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--kernel", default="fixed", choices=["fixed", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,5 @@
+// Single translation unit for libgromos_nb.so: kernel templates and their
+// launch sites are compiled together (whole-program CUDA compilation).
+#include "pairlist.cu"
+#include "forces.cu"
+#include "api.cu"

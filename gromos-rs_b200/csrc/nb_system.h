@@ -1,0 +1,73 @@
+// nb_system.h -- host-side owner of one system's device state.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <string>
+#include <vector>
+
+#include "../../include/gromos_nb.h"
+#include "nb_common.cuh"
+
+namespace gnb {
+
+void set_error(const std::string& m);
+void crf_params(double cutoff, double epsilon, double rf_epsilon, double rf_kappa, double out[4]);
+void lambda_params(double lam, int n, double lp[17]);
+
+class NbSystem {
+   public:
+    ~NbSystem();
+    void release();
+    gr_status upload(const gr_topology* t);
+    gr_status set_params(const gr_nb_params* p);
+    gr_status set_box(const double box[3]);
+    gr_status build_pairlist(cudaStream_t s);
+    gr_status expand_cg_pairs(cudaStream_t s);
+    gr_status eval(cudaStream_t s, int flags, bool record_events);
+    gr_status download(cudaStream_t s, gr_result* out);
+    gr_status pair_counts(cudaStream_t s, long long* n_short, long long* n_long);
+    gr_status push_descriptor(cudaStream_t s);
+    int sm_count();
+
+    // sizes
+    int N = 0, NCG = 0, NSCG = 0, NSA = 0, NT = 0, G = 1, aps = 3, W = 4;
+    int n_pert = 0, solvent_group = -1;
+    double fpe = 138.9354;
+    gr_nb_params prm{};
+    // host copies needed for list expansion
+    std::vector<int> h_cg_off, h_excl_off, h_excl, h_o14_off, h_o14, h_egroup;
+    // device descriptor (host mirror + device copy)
+    SysDev h{};
+    SysDev* d_sys = nullptr;
+    unsigned long long* d_cg_key = nullptr;
+    // state
+    bool uploaded = false, params_set = false, box_set = false, pos_set = false;
+    bool built = false, lr_computed = false, last_rebuilt = false, last_long = false;
+    bool cgp_valid = false, pair_count_valid = false;
+    int steps_since_update = 0;
+    int n_cgp_host[2] = {0, 0};
+    long long pairs_short = 0, pairs_long = 0;
+    int water_blocks_per_sm = 4;
+    long long launches = 0;  // kernels launched by this system
+    // capacities
+    int cells_alloc = 0, clus_alloc = 0, wcap_alloc = 0, scap_alloc = 0, pcap_alloc = 0, cgp_alloc = 0;
+    int wcap_want = 0, scap_want = 0, pcap_want = 0;
+    long long cgp_want = 0;
+    int regrow_count = 0;
+    size_t bytes = 0;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+
+   private:
+    template <class T>
+    gr_status alloc(T** p, size_t n);
+    template <class T>
+    gr_status upload_array(T** p, const T* host, size_t n);
+    gr_status ensure_capacity();
+    gr_status ensure_cgp_capacity();
+    gr_status check_errors(cudaStream_t s, bool* retry);
+    std::vector<void*> allocs;
+    int sms_cached = 0;
+};
+
+}  // namespace gnb

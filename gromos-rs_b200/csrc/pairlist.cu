@@ -1,0 +1,551 @@
+// pairlist.cu -- cell-grid charge-group pairlist on the device.
+//
+// Semantics are those of gromos-rs StandardPairlistAlgorithm::
+// update_chargegroup_based (crates/gromos-core/src/pairlist.rs:183-442); the
+// candidate generation follows the cell-list idea of
+// CellListPairlistAlgorithm (pairlist.rs:537-777) but the pair SET, not the
+// order, is what is reproduced, and the distance test is the reference's
+// FP64 arithmetic bit for bit (nb_common.cuh):
+//   * solute CG reference = centre of geometry (topology.rs:408-417),
+//     solvent CG reference = its first atom;
+//   * d2 = |nearest_image(ref_1, ref_2)|^2; d2 > (rcl+skin)^2 -> no pair,
+//     d2 > (rcs+skin)^2 -> long range, else short range (strict '>').
+//
+// Stages: k_refpos (reference positions, cell keys) -> k_scan_cells ->
+// k_scatter -> k_cell_sort (bitonic, per cell, deterministic) ->
+// k_scan_clusters -> k_cluster_setup (solvent i-clusters of W CGs) ->
+// k_cluster_search (water-water j-lists with W-bit masks) and
+// k_solute_search (per solute CG j-lists with exclusion masks) ->
+// k_pert_pairs (explicit perturbed atom pairs for the FEP correction).
+#include "nb_common.cuh"
+
+namespace gnb {
+
+__device__ __forceinline__ int imod(int a, int m) {
+    int r = a % m;
+    return r < 0 ? r + m : r;
+}
+
+__device__ __forceinline__ int cell_coord(double x, double cs, int g, double* frac) {
+    double q = x / cs;
+    double f = floor(q);
+    *frac = q - f;
+    long long c = static_cast<long long>(f);
+    long long r = c % g;
+    if (r < 0) r += g;
+    return static_cast<int>(r);
+}
+
+__device__ __forceinline__ unsigned spread3(unsigned v) {  // 3-bit Morton spread
+    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+}
+
+// Reference positions + cell keys (pairlist.rs:196-198, 577-585, 658-663).
+__global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __restrict__ cg_key) {
+    const SysDev& s = sys[blockIdx.y];
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= s.n_cg) return;
+    int a0 = s.cg_off[c], a1 = s.cg_off[c + 1];
+    double rx, ry, rz;
+    if (c < s.n_solute_cg) {
+        // ChargeGroup::center_of_geometry: sum from ZERO, then / len
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int a = a0; a < a1; ++a) {
+            sx = __dadd_rn(sx, s.pos[3 * a]);
+            sy = __dadd_rn(sy, s.pos[3 * a + 1]);
+            sz = __dadd_rn(sz, s.pos[3 * a + 2]);
+        }
+        double len = static_cast<double>(a1 - a0);
+        rx = __ddiv_rn(sx, len);
+        ry = __ddiv_rn(sy, len);
+        rz = __ddiv_rn(sz, len);
+    } else {
+        rx = s.pos[3 * a0];
+        ry = s.pos[3 * a0 + 1];
+        rz = s.pos[3 * a0 + 2];
+    }
+    s.ref[3 * c] = rx;
+    s.ref[3 * c + 1] = ry;
+    s.ref[3 * c + 2] = rz;
+    double fx = 0, fy = 0, fz = 0;
+    int cx = 0, cy = 0, cz = 0;
+    if (s.boundary == 1) {
+        cx = cell_coord(rx, s.cell_size[0], s.gdim[0], &fx);
+        cy = cell_coord(ry, s.cell_size[1], s.gdim[1], &fy);
+        cz = cell_coord(rz, s.cell_size[2], s.gdim[2], &fz);
+    }
+    int cell = cx + s.gdim[0] * (cy + s.gdim[1] * cz);
+    unsigned sx3 = min(7u, static_cast<unsigned>(fx * 8.0));
+    unsigned sy3 = min(7u, static_cast<unsigned>(fy * 8.0));
+    unsigned sz3 = min(7u, static_cast<unsigned>(fz * 8.0));
+    unsigned morton = spread3(sx3) | (spread3(sy3) << 1) | (spread3(sz3) << 2);
+    unsigned long long solvent = c >= s.n_solute_cg ? 1ull : 0ull;
+    cg_key[c] = (static_cast<unsigned long long>(cell) << 42) | (solvent << 41) |
+                (static_cast<unsigned long long>(morton) << 32) | static_cast<unsigned>(c);
+    s.cg_cell[c] = cell;
+    s.cg_slot[c] = -1;
+    atomicAdd(&s.cell_count[cell], 1);
+}
+
+// Exclusive scan of n values (single block, blockDim.x == 1024).  out has n+1
+// entries; out may alias in.  Also returns the total in *total (if given).
+__device__ void block_exclusive_scan(const int* in, int* out, int n, int* total) {
+    __shared__ int warp_tot[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int base = 0; base < n; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = i < n ? in[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int t = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;
+        }
+        __syncthreads();
+        int excl = x - v + (wid > 0 ? warp_tot[wid - 1] : 0) + carry;
+        __syncthreads();
+        if (i < n) out[i] = excl;
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[n] = carry;
+        if (total) *total = carry;
+    }
+}
+
+__global__ void k_scan_cells(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[blockIdx.y];
+    block_exclusive_scan(s.cell_count, s.cell_start, s.n_cells, nullptr);
+}
+
+__global__ void k_scatter(const SysDev* __restrict__ sys, const unsigned long long* __restrict__ cg_key) {
+    const SysDev& s = sys[blockIdx.y];
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= s.n_cg) return;
+    int cell = s.cg_cell[c];
+    int p = s.cell_start[cell] + atomicAdd(&s.cell_fill[cell], 1);
+    s.keys[p] = cg_key[c];
+}
+
+// One block (1024 threads) per cell: bitonic sort of the cell's keys.
+__global__ void k_cell_sort(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[blockIdx.y];
+    __shared__ unsigned long long sk[kMaxCellCGs];
+    int cell = blockIdx.x;
+    int start = s.cell_start[cell], n = s.cell_start[cell + 1] - start;
+    if (n > kMaxCellCGs) {
+        if (threadIdx.x == 0) atomicOr(&s.err[0], ERR_CELL_TOO_DENSE);
+        return;
+    }
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) sk[i] = i < n ? s.keys[start + i] : ~0ull;
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    unsigned long long a = sk[i], b = sk[ixj];
+                    bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        sk[i] = b;
+                        sk[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    __shared__ int nsol;
+    if (threadIdx.x == 0) nsol = 0;
+    __syncthreads();
+    int local = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        unsigned long long key = sk[i];
+        int cg = static_cast<int>(key & 0xffffffffull);
+        s.keys[start + i] = key;
+        s.sorted_cg[start + i] = cg;
+        s.cg_spos[cg] = start + i;
+        if (((key >> 41) & 1ull) == 0ull) ++local;
+    }
+    atomicAdd(&nsol, local);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s.cell_nsolute[cell] = nsol;
+        int nsolv = n - nsol;
+        s.cell_nclus[cell] = (nsolv + s.W - 1) / s.W;
+    }
+}
+
+__global__ void k_scan_clusters(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[blockIdx.y];
+    __shared__ int total;
+    block_exclusive_scan(s.cell_nclus, s.cell_nclus, s.n_cells, &total);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (total > s.max_clusters) {
+            atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
+            total = s.max_clusters;
+        }
+        s.n_clusters[0] = total;
+    }
+}
+
+// One warp per cell: write the cluster records and the slot <-> CG maps.
+__global__ void k_cluster_setup(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[blockIdx.y];
+    int cell = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (cell >= s.n_cells) return;
+    int c0 = s.cell_nclus[cell], c1 = s.cell_nclus[cell + 1];
+    int first_solv = s.cell_start[cell] + s.cell_nsolute[cell];
+    int nsolv = s.cell_start[cell + 1] - first_solv;
+    for (int k = c0 + lane; k < c1; k += 32) {
+        if (k >= s.max_clusters) break;
+        int local = k - c0;
+        int first = first_solv + local * s.W;
+        int n = min(s.W, nsolv - local * s.W);
+        s.clus_cell[k] = cell;
+        s.clus_first[k] = first;
+        s.clus_n[k] = n;
+        for (int m = 0; m < s.W; ++m) {
+            int slot = k * s.W + m;
+            if (m < n) {
+                int cg = s.sorted_cg[first + m];
+                s.slot_cg[slot] = cg;
+                s.cg_slot[cg] = slot;
+            } else {
+                s.slot_cg[slot] = -1;
+            }
+        }
+    }
+}
+
+// Neighbour cell offsets along one axis, de-duplicated for grids of 1 or 2
+// cells (the reference de-duplicates with a HashSet, pairlist.rs:675-692).
+__device__ __forceinline__ int axis_offsets(int g, int* off) {
+    if (g >= 3) {
+        off[0] = -1;
+        off[1] = 0;
+        off[2] = 1;
+        return 3;
+    }
+    if (g == 2) {
+        off[0] = 0;
+        off[1] = 1;
+        return 2;
+    }
+    off[0] = 0;
+    return 1;
+}
+
+// Water-water search: one warp per solvent i-cluster.  Candidate j = solvent
+// CG in a neighbour cell; pair {i_k, j} belongs to this cluster iff j's sorted
+// position is after i_k's, so every unordered CG pair is listed once.  Bit k
+// of the short (long) mask is set when the exact reference test puts
+// (i_k, j) in the short (long) range; the solvent reference point is the
+// first atom for both CGs (pairlist.rs:359-368).
+template <int W>
+__global__ void k_cluster_search(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int ci = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (ci >= s.n_clusters[0]) return;
+    const int cell = s.clus_cell[ci], first = s.clus_first[ci], n = s.clus_n[ci];
+    double xi[W], yi[W], zi[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+        if (k < n) {
+            int a0 = s.cg_off[s.sorted_cg[first + k]];
+            xi[k] = s.pos[3 * a0];
+            yi[k] = s.pos[3 * a0 + 1];
+            zi[k] = s.pos[3 * a0 + 2];
+        } else {
+            xi[k] = yi[k] = zi[k] = 0.0;
+        }
+    }
+    // bounding sphere around the first CG for the conservative FP32 prefilter
+    float rad = 0.f;
+#pragma unroll
+    for (int k = 1; k < W; ++k)
+        if (k < n) {
+            float dx = float(xi[k] - xi[0]), dy = float(yi[k] - yi[0]), dz = float(zi[k] - zi[0]);
+            rad = fmaxf(rad, sqrtf(dx * dx + dy * dy + dz * dz));
+        }
+    const float reach = sqrtf(float(s.c2l)) + rad + 1e-3f;
+    const float reach2 = reach * reach;
+    int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
+    int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
+    int ox[3], oy[3], oz[3];
+    int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
+    uint32_t* outs = s.wl_s + static_cast<size_t>(ci) * s.wcap;
+    uint32_t* outl = s.wl_l + static_cast<size_t>(ci) * s.wcap;
+    int cnt_s = 0, cnt_l = 0;
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
+                if (nc < cell) continue;
+                int j0 = s.cell_start[nc] + s.cell_nsolute[nc], j1 = s.cell_start[nc + 1];
+                if (nc == cell) j0 = max(j0, first + 1);
+                for (int base = j0; base < j1; base += 32) {
+                    int sp = base + lane;
+                    unsigned ms = 0, ml = 0;
+                    int slot = 0;
+                    if (sp < j1) {
+                        int cgj = s.sorted_cg[sp];
+                        slot = s.cg_slot[cgj];
+                        int a0 = s.cg_off[cgj];
+                        double xj = s.pos[3 * a0], yj = s.pos[3 * a0 + 1], zj = s.pos[3 * a0 + 2];
+                        float dx = float(xi[0] - xj), dy = float(yi[0] - yj), dz = float(zi[0] - zj);
+                        if (s.boundary == 1) {
+                            dx -= s.boxf[0] * rintf(dx * s.inv_boxf[0]);
+                            dy -= s.boxf[1] * rintf(dy * s.inv_boxf[1]);
+                            dz -= s.boxf[2] * rintf(dz * s.inv_boxf[2]);
+                        }
+                        if (dx * dx + dy * dy + dz * dz <= reach2) {
+#pragma unroll
+                            for (int k = 0; k < W; ++k) {
+                                if (k < n && sp > first + k) {
+                                    double rx, ry, rz;
+                                    nearest_image_exact(s, xi[k], yi[k], zi[k], xj, yj, zj, rx, ry, rz);
+                                    double d2 = len2_exact(rx, ry, rz);
+                                    if (!(d2 > s.c2l)) {
+                                        if (d2 > s.c2s)
+                                            ml |= 1u << k;
+                                        else
+                                            ms |= 1u << k;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
+                    unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
+                    unsigned below = (1u << lane) - 1u;
+                    if (ms) {
+                        int p = cnt_s + __popc(bs & below);
+                        if (p < s.wcap) outs[p] = (static_cast<uint32_t>(slot) << 8) | ms;
+                    }
+                    if (ml) {
+                        int p = cnt_l + __popc(bl & below);
+                        if (p < s.wcap) outl[p] = (static_cast<uint32_t>(slot) << 8) | ml;
+                    }
+                    cnt_s += __popc(bs);
+                    cnt_l += __popc(bl);
+                }
+            }
+    if (lane == 0) {
+        if (cnt_s > s.wcap || cnt_l > s.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
+        s.wn_s[ci] = min(cnt_s, s.wcap);
+        s.wn_l[ci] = min(cnt_l, s.wcap);
+    }
+}
+
+// Topology::is_excluded_or_14 (topology.rs:853-864).
+__device__ bool excluded_or_14(const SysDev& s, int i, int j) {
+    for (int pass = 0; pass < 2; ++pass) {
+        int a = pass ? j : i, b = pass ? i : j;
+        int lo = s.excl_off[a], hi = s.excl_off[a + 1] - 1;
+        while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            int v = s.excl[mid];
+            if (v == b) return true;
+            if (v < b)
+                lo = mid + 1;
+            else
+                hi = mid - 1;
+        }
+        for (int k = s.o14_off[a]; k < s.o14_off[a + 1]; ++k)
+            if (s.o14[k] == b) return true;
+    }
+    return false;
+}
+
+// Excluded atom pairs of CG pair (ci, cj) as bits a*8+b; for ci == cj the
+// pairs with a >= b are marked too (only a < b is a pair).
+__device__ unsigned long long excl_mask(const SysDev& s, int ci, int cj) {
+    unsigned long long m = 0;
+    int i0 = s.cg_off[ci], ni = s.cg_off[ci + 1] - i0;
+    int j0 = s.cg_off[cj], nj = s.cg_off[cj + 1] - j0;
+    for (int a = 0; a < ni; ++a)
+        for (int b = 0; b < nj; ++b) {
+            bool ex = (ci == cj && b <= a) || excluded_or_14(s, i0 + a, j0 + b);
+            if (ex) m |= 1ull << (a * 8 + b);
+        }
+    return m;
+}
+
+// Solute CG i against every CG in the neighbour cells: solute j > i
+// (COG-COG, with exclusions for the short range) and every solvent CG
+// (COG-first atom, no exclusion check), pairlist.rs:237-350.  One warp per
+// solute CG.  Entry = (j << 1 | long); the first entry is the CG itself
+// (intra-CG pairs, pairlist.rs:239-249).
+__global__ void k_solute_search(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int ci = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (ci >= s.n_solute_cg) return;
+    if (s.cg_off[ci + 1] - s.cg_off[ci] > kMaxCGAtoms) {
+        if (lane == 0) atomicOr(&s.err[0], ERR_CG_TOO_LARGE);
+        return;
+    }
+    int* out = s.sl + static_cast<size_t>(ci) * s.scap;
+    unsigned long long* outx = s.sl_excl + static_cast<size_t>(ci) * s.scap;
+    int cnt = 0;
+    if (lane == 0) {
+        out[0] = ci << 1;
+        outx[0] = excl_mask(s, ci, ci);
+    }
+    cnt = 1;
+    double xi = s.ref[3 * ci], yi = s.ref[3 * ci + 1], zi = s.ref[3 * ci + 2];
+    int cell = s.cg_cell[ci];
+    int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
+    int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
+    int ox[3], oy[3], oz[3];
+    int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
+                int j0 = s.cell_start[nc], j1 = s.cell_start[nc + 1];
+                for (int base = j0; base < j1; base += 32) {
+                    int sp = base + lane;
+                    int entry = -1;
+                    unsigned long long xm = 0;
+                    if (sp < j1) {
+                        int cj = s.sorted_cg[sp];
+                        bool solute_j = cj < s.n_solute_cg;
+                        if (!solute_j || cj > ci) {
+                            double rx, ry, rz;
+                            nearest_image_exact(s, xi, yi, zi, s.ref[3 * cj], s.ref[3 * cj + 1],
+                                                s.ref[3 * cj + 2], rx, ry, rz);
+                            double d2 = len2_exact(rx, ry, rz);
+                            if (!(d2 > s.c2l)) {
+                                int lr = d2 > s.c2s ? 1 : 0;
+                                if (solute_j && s.cg_off[cj + 1] - s.cg_off[cj] > kMaxCGAtoms) {
+                                    atomicOr(&s.err[0], ERR_CG_TOO_LARGE);
+                                } else {
+                                    entry = (cj << 1) | lr;
+                                    if (solute_j && !lr) xm = excl_mask(s, ci, cj);
+                                }
+                            }
+                        }
+                    }
+                    unsigned b = __ballot_sync(0xffffffffu, entry >= 0);
+                    if (entry >= 0) {
+                        int p = cnt + __popc(b & ((1u << lane) - 1u));
+                        if (p < s.scap) {
+                            out[p] = entry;
+                            outx[p] = xm;
+                        }
+                    }
+                    cnt += __popc(b);
+                }
+            }
+    if (lane == 0) {
+        if (cnt > s.scap) atomicOr(&s.err[0], ERR_SLIST_OVERFLOW);
+        s.sn[ci] = min(cnt, s.scap);
+    }
+}
+
+// Explicit list of atom pairs that the FEP correction visits: pairs of the
+// solute lists whose first atom (the atom of the lower-index CG) is
+// perturbed (perturbed.rs:324-332).  One thread per (solute CG, entry).
+__global__ void k_pert_pairs(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[blockIdx.y];
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    int ci = gid / s.scap, e = gid % s.scap;
+    if (ci >= s.n_solute_cg || e >= s.sn[ci]) return;
+    int entry = s.sl[static_cast<size_t>(ci) * s.scap + e];
+    unsigned long long xm = s.sl_excl[static_cast<size_t>(ci) * s.scap + e];
+    int cj = entry >> 1, lr = entry & 1;
+    int i0 = s.cg_off[ci], i1 = s.cg_off[ci + 1];
+    int j0 = s.cg_off[cj], j1 = s.cg_off[cj + 1];
+    for (int a = i0; a < i1; ++a) {
+        if (s.pert_idx[a] < 0) continue;
+        for (int b = j0; b < j1; ++b) {
+            if (xm & (1ull << ((a - i0) * 8 + (b - j0)))) continue;
+            int p = atomicAdd(s.n_pert_pairs, 1);
+            if (p < s.pcap) {
+                s.pert_pairs[3 * p] = a;
+                s.pert_pairs[3 * p + 1] = b;
+                s.pert_pairs[3 * p + 2] = lr;
+            } else {
+                atomicOr(&s.err[0], ERR_PERT_OVERFLOW);
+            }
+        }
+    }
+}
+
+// Explicit CG-pair list (i, j, long) + exclusion mask, for the plain kernel
+// and for downloading the pair set.  Water-water pairs from the cluster
+// masks, then solute entries.  One thread per (cluster, entry) / (solute
+// CG, entry).
+__global__ void k_expand_cgpairs(const SysDev* __restrict__ sys, int long_range) {
+    const SysDev& s = sys[blockIdx.y];
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    int nclus = s.n_clusters[0];
+    long long nwater = static_cast<long long>(nclus) * s.wcap;
+    if (gid < nwater) {
+        int ci = gid / s.wcap, e = gid % s.wcap;
+        const int* wn = long_range ? s.wn_l : s.wn_s;
+        if (e >= wn[ci]) return;
+        uint32_t ent = (long_range ? s.wl_l : s.wl_s)[static_cast<size_t>(ci) * s.wcap + e];
+        int cj = s.slot_cg[ent >> 8];
+        unsigned mask = ent & 0xffu;
+        for (int k = 0; k < s.W; ++k)
+            if (mask & (1u << k)) {
+                int cik = s.slot_cg[ci * s.W + k];
+                int p = atomicAdd(&s.n_cgp[long_range], 1);
+                int idx = long_range ? s.cgp_cap - 1 - p : p;
+                if (p < s.cgp_cap) {
+                    s.cgp[3 * idx] = min(cik, cj);
+                    s.cgp[3 * idx + 1] = max(cik, cj);
+                    s.cgp[3 * idx + 2] = long_range;
+                    s.cgp_excl[idx] = 0ull;
+                } else {
+                    atomicOr(&s.err[0], ERR_CGPAIR_OVERFLOW);
+                }
+            }
+        return;
+    }
+    long long g2 = gid - nwater;
+    int ci = static_cast<int>(g2 / s.scap), e = static_cast<int>(g2 % s.scap);
+    if (ci >= s.n_solute_cg || e >= s.sn[ci]) return;
+    int entry = s.sl[static_cast<size_t>(ci) * s.scap + e];
+    if ((entry & 1) != long_range) return;
+    int p = atomicAdd(&s.n_cgp[long_range], 1);
+    int idx = long_range ? s.cgp_cap - 1 - p : p;
+    if (p < s.cgp_cap) {
+        s.cgp[3 * idx] = ci;
+        s.cgp[3 * idx + 1] = entry >> 1;
+        s.cgp[3 * idx + 2] = long_range;
+        s.cgp_excl[idx] = s.sl_excl[static_cast<size_t>(ci) * s.scap + e];
+    } else {
+        atomicOr(&s.err[0], ERR_CGPAIR_OVERFLOW);
+    }
+}
+
+}  // namespace gnb
+
+namespace gnb {
+template __global__ void k_cluster_search<4>(const SysDev*);
+template __global__ void k_cluster_search<8>(const SysDev*);
+}  // namespace gnb

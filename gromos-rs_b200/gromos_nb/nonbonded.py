@@ -1,0 +1,265 @@
+"""Host-side mirror of gromos-rs's nonbonded interface, backed by the CUDA library.
+
+Names follow the reference so that callers and tests read the same:
+
+* :class:`CRFParameters` -- ``CRFParameters::new``
+  (crates/gromos-forces/src/nonbonded/params.rs:61-97)
+* :class:`PairlistContainer` -- cutoffs, skin and NSNB
+  (crates/gromos-core/src/pairlist.rs:59-126)
+* :class:`Forcefield` -- ``Forcefield::apply``'s nonbonded part
+  (crates/gromos-integrators/src/algorithms/forcefield.rs:226-1020): one
+  :meth:`Forcefield.apply` per MD step, pairlist rebuilt every NSNB calls,
+  twin-range long-range forces cached between rebuilds.
+* :func:`lj_crf_innerloop` -- the C-ABI stub ``rust_lj_crf_innerloop``
+  (crates/gromos-core/src/ffi.rs:55-103) with a body.
+
+Every evaluation runs on the GPU through include/gromos_nb.h; errors from the
+library raise :class:`GromosNbError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import GromosNbError, check  # noqa: F401  (re-exported)
+from .system import NonbondedParams, System, Topology
+
+KERNELS = {"fixed": _lib.GR_KERNEL_FIXED, "plain": _lib.GR_KERNEL_PLAIN}
+
+
+@dataclasses.dataclass
+class CRFParameters:
+    crf_cut: float
+    crf_2cut3i: float
+    crf_cut3i: float
+    cutoff_sq: float
+
+    @staticmethod
+    def new(cutoff: float, epsilon: float, rf_epsilon: float, rf_kappa: float) -> "CRFParameters":
+        kc = rf_kappa * cutoff
+        kc2 = kc * kc
+        crf = (2.0 * (epsilon - rf_epsilon) * (1.0 + kc) - rf_epsilon * kc2) / (
+            (epsilon + 2.0 * rf_epsilon) * (1.0 + kc) + rf_epsilon * kc2)
+        crf_cut3i = crf * (1.0 / (cutoff * cutoff * cutoff))
+        return CRFParameters((1.0 - crf / 2.0) / cutoff, crf_cut3i / 2.0, crf_cut3i, cutoff * cutoff)
+
+
+@dataclasses.dataclass
+class PairlistContainer:
+    short_range_cutoff: float
+    long_range_cutoff: float
+    skin: float = 0.0
+    update_frequency: int = 5
+
+
+def _p(a, ct):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ct))
+
+
+class _TopologyStruct:
+    """gr_topology plus the arrays it points into (kept alive here)."""
+
+    def __init__(self, topo: Topology):
+        t = topo.normalized()
+        self.t = t
+        s = _lib.GrTopology()
+        s.n_atoms, s.n_solute_atoms = t.n_atoms, t.n_solute_atoms
+        s.n_chargegroups, s.n_solute_chargegroups = t.n_cg, t.n_solute_cg
+        s.cg_offsets, s.charge, s.iac = _p(t.cg_offsets, C.c_int32), _p(t.charge, C.c_double), _p(t.iac, C.c_int32)
+        s.n_types, s.lj = t.n_types, _p(t.lj, C.c_double)
+        s.excl_offsets, s.excl = _p(t.excl_off, C.c_int32), _p(t.excl, C.c_int32)
+        s.o14_offsets, s.o14 = _p(t.o14_off, C.c_int32), _p(t.o14, C.c_int32)
+        s.energy_group = _p(t.egroup, C.c_int32)
+        s.n_energy_groups = int(t.n_egroups)
+        s.atoms_per_solvent = t.atoms_per_solvent
+        s.four_pi_eps_i = t.four_pi_eps_i
+        self.pert = None
+        self.pairs = None
+        if t.pert_idx is not None and t.n_pert > 0:
+            atoms = np.nonzero(t.pert_idx >= 0)[0]
+            arr = (_lib.GrPerturbedAtom * len(atoms))()
+            for n, a in enumerate(atoms):
+                k = int(t.pert_idx[a])
+                arr[n] = _lib.GrPerturbedAtom(int(a), int(t.pert_a_iac[k]), int(t.pert_b_iac[k]),
+                                              float(t.pert_a_q[k]), float(t.pert_b_q[k]),
+                                              float(t.pert_alpha_lj[k]), float(t.pert_alpha_crf[k]))
+            self.pert = arr
+            s.n_perturbed = len(atoms)
+            s.perturbed = C.cast(arr, C.POINTER(_lib.GrPerturbedAtom))
+        if t.pp_i is not None and t.n_pert_pairs > 0:
+            arr = (_lib.GrPerturbedPair * t.n_pert_pairs)()
+            for n in range(t.n_pert_pairs):
+                arr[n] = _lib.GrPerturbedPair(int(t.pp_i[n]), int(t.pp_j[n]), int(t.pp_a_type[n]), int(t.pp_b_type[n]))
+            self.pairs = arr
+            s.n_perturbed_pairs = t.n_pert_pairs
+            s.perturbed_pairs = C.cast(arr, C.POINTER(_lib.GrPerturbedPair))
+        self.struct = s
+
+
+def make_params(p: NonbondedParams, kernel: str = "fixed") -> _lib.GrNbParams:
+    q = _lib.GrNbParams()
+    q.rcutp, q.rcutl, q.skin = p.rcutp, p.rcutl, p.skin
+    q.epsilon, q.epsrf, q.kappa = p.epsilon, p.epsrf, p.kappa
+    q.nsnb, q.boundary, q.lam, q.nlam = p.nsnb, p.boundary, p.lam, p.nlam
+    q.kernel = KERNELS[kernel]
+    q.cluster_size = 0
+    return q
+
+
+class Forcefield:
+    """Nonbonded ``Forcefield`` on one GPU.
+
+    ``Forcefield(system)`` uploads the topology, parameters and box; the first
+    :meth:`apply` builds the pairlist (md.rs:864-867 builds it before the
+    first step), later calls rebuild it every ``nsnb`` calls.
+    """
+
+    def __init__(self, system: System, kernel: str = "fixed", device: int = 0):
+        L = _lib.lib()
+        self._L = L
+        self.system = system
+        self.kernel = kernel
+        h = C.c_void_p()
+        check(L.gr_ctx_create(device, C.byref(h)))
+        self._h = h
+        self._topo = _TopologyStruct(system.topo)
+        check(L.gr_system_upload(h, C.byref(self._topo.struct)))
+        self._params = make_params(system.params, kernel)
+        check(L.gr_set_params(h, C.byref(self._params)))
+        self.set_box(system.box)
+        self.n_atoms = system.topo.n_atoms
+        self.G = max(1, int(system.topo.n_egroups))
+        self.crf = CRFParameters.new(system.params.rcutl, system.params.epsilon, system.params.epsrf,
+                                     system.params.kappa)
+        self.pairlist = PairlistContainer(system.params.rcutp, system.params.rcutl, system.params.skin,
+                                          system.params.nsnb)
+
+    # ---- set-up
+    def set_box(self, box) -> None:
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        check(self._L.gr_set_box(self._h, _p(b, C.c_double)))
+
+    def upload_positions(self, pos) -> None:
+        x = np.ascontiguousarray(pos, dtype=np.float64)
+        if x.shape != (self.n_atoms, 3):
+            raise ValueError(f"positions must be ({self.n_atoms}, 3)")
+        check(self._L.gr_positions_upload(self._h, _p(x, C.c_double)))
+
+    # ---- evaluation
+    def apply(self, pos=None, virial: bool = True, force_rebuild: bool = False, count_pairs: bool = True,
+              download_forces: bool = True) -> Dict:
+        if pos is not None:
+            self.upload_positions(pos)
+        flags = (_lib.GR_EVAL_VIRIAL if virial else 0) | (_lib.GR_EVAL_FORCE_REBUILD if force_rebuild else 0)
+        f = np.zeros((self.n_atoms, 3)) if download_forces else None
+        glj = np.zeros((self.G, self.G))
+        gcrf = np.zeros((self.G, self.G))
+        r = _lib.GrResult()
+        r.forces = _p(f, C.c_double)
+        r.egroup_lj, r.egroup_crf = _p(glj, C.c_double), _p(gcrf, C.c_double)
+        r.n_pairs_short = 0 if count_pairs else -1
+        check(self._L.gr_forces_eval(self._h, flags, C.byref(r)))
+        return {"forces": f, "e_lj": r.e_lj, "e_crf": r.e_crf, "dhdl": r.dhdl,
+                "virial": np.asarray(list(r.virial)).reshape(3, 3), "egroup_lj": glj, "egroup_crf": gcrf,
+                "n_pairs_short": r.n_pairs_short, "n_pairs_long": r.n_pairs_long, "rebuilt": bool(r.rebuilt)}
+
+    def eval_async(self, force_rebuild: bool = False) -> None:
+        """Evaluate without reading results back (device-resident pipelines)."""
+        flags = _lib.GR_EVAL_VIRIAL | _lib.GR_EVAL_NO_DOWNLOAD | (_lib.GR_EVAL_FORCE_REBUILD if force_rebuild else 0)
+        check(self._L.gr_forces_eval(self._h, flags, None))
+
+    def timings(self) -> List[float]:
+        ms = (C.c_float * 5)()
+        check(self._L.gr_last_timings(self._h, ms))
+        return list(ms)
+
+    def launches(self) -> int:
+        n = C.c_int64(0)
+        check(self._L.gr_ctx_launches(self._h, C.byref(n)))
+        return int(n.value)
+
+    def stream(self) -> int:
+        return int(self._L.gr_ctx_stream(self._h) or 0)
+
+    def positions_device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(self._L.gr_positions_device(self._h, C.byref(p)))
+        return int(p.value)
+
+    def forces_device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(self._L.gr_forces_device(self._h, C.byref(p)))
+        return int(p.value)
+
+    # ---- pairlist
+    def build_pairlist(self) -> None:
+        check(self._L.gr_pairlist_build(self._h))
+
+    def pairlist_lists(self) -> List[np.ndarray]:
+        """solute_short, solute_long, solvent_short, solvent_long as sorted (n, 2) int32."""
+        counts = (C.c_int64 * 4)()
+        check(self._L.gr_pairlist_counts(self._h, counts))
+        out = [np.zeros((int(counts[k]), 2), dtype=np.int32) for k in range(4)]
+        check(self._L.gr_pairlist_download(self._h, *[_p(a, C.c_int32) for a in out]))
+        return out
+
+    def cg_pairs(self) -> np.ndarray:
+        n = C.c_int64(0)
+        check(self._L.gr_pairlist_cg_pairs(self._h, None, C.byref(n)))
+        out = np.zeros((n.value, 3), dtype=np.int32)
+        n2 = C.c_int64(n.value)
+        check(self._L.gr_pairlist_cg_pairs(self._h, _p(out, C.c_int32), C.byref(n2)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.gr_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ffma_peak(device: int = 0) -> float:
+    """Measured FP32 FMA operations per second of the device (one FFMA = one op)."""
+    v = C.c_double(0.0)
+    check(_lib.lib().gr_ffma_peak(device, C.byref(v)))
+    return float(v.value)
+
+
+def lj_crf_innerloop(positions, charges, iac, pairlist, lj_params, crf: CRFParameters, box=None):
+    """``lj_crf_innerloop`` over an explicit atom-pair list, on the GPU.
+
+    Same arguments as the reference C-ABI stub (ffi.rs:55-103): FP32
+    positions/charges, (c6, c12) per type pair, per-atom nearest image
+    (box=None -> vacuum).  Returns (forces (N,3) float32, e_lj, e_crf, virial 3x3).
+    """
+    L = _lib.lib()
+    pos = np.ascontiguousarray(positions, dtype=np.float32)
+    q = np.ascontiguousarray(charges, dtype=np.float32)
+    ia = np.ascontiguousarray(iac, dtype=np.uint32)
+    pl = np.ascontiguousarray(pairlist, dtype=np.uint32)
+    lj = np.ascontiguousarray(lj_params, dtype=np.float64)
+    n_types = int(round(np.sqrt(lj.size // 2)))
+    n = pos.shape[0]
+    f = np.zeros((n, 3), dtype=np.float32)
+    e = np.zeros(2)
+    v = np.zeros(9)
+    bx = np.ascontiguousarray(box if box is not None else np.zeros(3), dtype=np.float64)
+    fn = L.gr_lj_crf_innerloop
+    fn.restype = C.c_int32
+    u32 = C.POINTER(C.c_uint32)
+    fn.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), u32, C.c_uint32, u32, C.c_uint32,
+                   C.POINTER(C.c_double), C.c_uint32, C.POINTER(C.c_double), C.c_uint32, C.c_double, C.c_double,
+                   C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    check(fn(_p(pos, C.c_float), _p(q, C.c_float), _p(ia, C.c_uint32), n, _p(pl, C.c_uint32), pl.shape[0],
+             _p(lj, C.c_double), n_types, _p(bx, C.c_double), 0 if box is None else 1, crf.crf_cut,
+             crf.crf_2cut3i, crf.crf_cut3i, _p(f, C.c_float), _p(e, C.c_double), _p(v, C.c_double)))
+    return f, e[0], e[1], v.reshape(3, 3)

@@ -1,0 +1,203 @@
+/*
+ * gromos_nb.h -- C ABI of the B200 nonbonded library (libgromos_nb.so).
+ *
+ * This is the drop-in boundary for gromos-rs's nonbonded hot path: the
+ * charge-group twin-range pairlist and the Lennard-Jones + reaction-field
+ * (LJ/CRF) force / energy / virial evaluation, with the soft-core FEP
+ * corrections.  Every entry point names the gromos-rs interface it replaces
+ * (paths relative to the gromos-rs repository).  A Rust `-sys` crate binds
+ * these declarations one to one; ctypes does the same
+ * from Python.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Host pointers unless a name says
+ *    "device".  The library owns all device memory; the caller owns host
+ *    buffers.
+ *  - Every call returns gr_status (0 = GR_OK).  gr_last_error() returns a
+ *    thread-local message for the last failing call on this thread.
+ *  - One context per host thread (or an external lock).  All work of a
+ *    context runs on its own CUDA stream.
+ *  - Positions are FP64 xyz triples (the layout of gromos-rs `Vec3 = DVec3`),
+ *    forces are returned as FP64 xyz triples.
+ *  - Charge groups are contiguous atom ranges given by offsets; solute CGs
+ *    first, then one CG per solvent molecule (gromos-rs Topology order).
+ */
+#ifndef GROMOS_NB_H
+#define GROMOS_NB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gr_status;
+enum {
+    GR_OK = 0,
+    GR_ERR_INVALID = 1,      /* bad argument or inconsistent topology */
+    GR_ERR_CUDA = 2,         /* CUDA runtime error */
+    GR_ERR_OOM = 3,          /* device allocation failed / over budget */
+    GR_ERR_STATE = 4,        /* call order violated (e.g. eval before upload) */
+    GR_ERR_UNSUPPORTED = 5,  /* feature outside this library's scope */
+    GR_ERR_OVERFLOW = 6,     /* a device list overflowed and could not be regrown */
+    GR_ERR_TIMEOUT = 7,      /* a bounded device wait gave up */
+    GR_ERR_NO_DEVICE = 8     /* no CUDA device / library built without it */
+};
+
+/* Which force kernel evaluates the pair lists. */
+enum {
+    GR_KERNEL_FIXED = 0,  /* CG-relative FP32 pair math, 64-bit fixed-point accumulation (default) */
+    GR_KERNEL_PLAIN = 1   /* absolute FP32 coordinates, FP32 atomics (baseline) */
+};
+
+/* gr_forces_eval flags */
+enum {
+    GR_EVAL_VIRIAL = 1,           /* compute the virial tensor */
+    GR_EVAL_FORCE_REBUILD = 2,    /* rebuild the pairlist now regardless of NSNB */
+    GR_EVAL_NO_DOWNLOAD = 4       /* keep results on the device (read them later) */
+};
+
+/* Perturbed atom: PertAtomInfo (crates/gromos-forces/src/nonbonded/perturbed.rs:271-279);
+ * alpha_lj / alpha_crf are the per-atom soft-core alphas ALREADY multiplied
+ * by ALPHLJ / ALPHC (forcefield.rs:146-170). */
+typedef struct {
+    int32_t atom;
+    int32_t a_iac, b_iac;
+    double a_charge, b_charge;
+    double alpha_lj, alpha_crf;
+} gr_perturbed_atom;
+
+/* PERTATOMPAIR entry (crates/gromos-core/src/topology.rs:227-236); b_type -1 = None. */
+typedef struct {
+    int32_t i, j, a_type, b_type;
+} gr_perturbed_pair;
+
+/* Topology subset read by the nonbonded path (topology.rs:619-712). */
+typedef struct {
+    int32_t n_atoms;
+    int32_t n_solute_atoms;
+    int32_t n_chargegroups;
+    int32_t n_solute_chargegroups;
+    const int32_t* cg_offsets;   /* n_chargegroups+1 */
+    const double* charge;        /* n_atoms */
+    const int32_t* iac;          /* n_atoms, 0-based */
+    int32_t n_types;
+    const double* lj;            /* n_types*n_types*4: c6, c12, cs6, cs12 (LJParamMatrix, params.rs:30-58) */
+    const int32_t* excl_offsets; /* n_atoms+1, symmetric sorted exclusions */
+    const int32_t* excl;
+    const int32_t* o14_offsets;  /* n_atoms+1, 1-4 partners (INE14) */
+    const int32_t* o14;
+    const int32_t* energy_group; /* n_atoms or NULL (one group) */
+    int32_t n_energy_groups;
+    int32_t atoms_per_solvent;   /* 3 for SPC */
+    int32_t n_perturbed;
+    const gr_perturbed_atom* perturbed;
+    int32_t n_perturbed_pairs;
+    const gr_perturbed_pair* perturbed_pairs;
+    double four_pi_eps_i;        /* PHYSICALCONSTANTS FPEPSI (md.rs:1108) */
+} gr_topology;
+
+/* IMD PAIRLIST / NONBONDED / PERTURBATION fields (imd.rs:81-92, 168-176). */
+typedef struct {
+    double rcutp, rcutl, skin;   /* PairlistContainer::new (pairlist.rs:90-102) */
+    double epsilon, epsrf, kappa;/* CRFParameters::new(rcutl, epsilon, epsrf, kappa) (params.rs:78-96) */
+    int32_t nsnb;                /* rebuild interval (pairlist.rs:105-107) */
+    int32_t boundary;            /* 0 vacuum, 1 rectangular */
+    double lambda;               /* RLAM */
+    int32_t nlam;                /* NLAM */
+    int32_t kernel;              /* GR_KERNEL_* */
+    int32_t cluster_size;        /* solvent i-cluster width 4 or 8 (0 = autotuned/default) */
+} gr_nb_params;
+
+/* Results of one evaluation (ForceStorage + Energy, params.rs:100-138). */
+typedef struct {
+    double* forces;       /* host n_atoms*3 or NULL */
+    double e_lj, e_crf;   /* totals */
+    double dhdl;          /* nonbonded dH/dlambda */
+    double virial[9];     /* virial[a*3+b] = sum r_a F_b (forcefield.rs:976-1000) */
+    double* egroup_lj;    /* host G*G or NULL; [min(g_i,g_j)][max] */
+    double* egroup_crf;   /* host G*G or NULL */
+    int64_t n_pairs_short;/* atom-pair interactions evaluated this call, short range */
+    int64_t n_pairs_long; /* long-range atom pairs evaluated this call (rebuild steps) */
+    int32_t rebuilt;      /* 1 if the pairlist was rebuilt in this call */
+} gr_result;
+
+typedef struct gr_ctx gr_ctx;
+
+/* ---- context lifecycle -------------------------------------------------- */
+/* Replaces constructing gromos-rs `Forcefield::new` (forcefield.rs:119-167). */
+gr_status gr_ctx_create(int device, gr_ctx** out);
+gr_status gr_ctx_destroy(gr_ctx* ctx);
+const char* gr_last_error(void);
+/* CUDA stream used by the context (cudaStream_t as void*), for graph capture / interop. */
+void* gr_ctx_stream(gr_ctx* ctx);
+
+/* ---- system set-up ------------------------------------------------------ */
+/* Topology upload: `Forcefield::init` (forcefield.rs:210-223) + LJ matrix
+ * conversion (forcefield.rs:173-178) + build_pert_info (:146-170). */
+gr_status gr_system_upload(gr_ctx* ctx, const gr_topology* topo);
+/* CRFParameters::new + PairlistContainer::new + NSNB (md.rs:326-330, 815, 836-841). */
+gr_status gr_set_params(gr_ctx* ctx, const gr_nb_params* params);
+/* Periodicity refresh from the box (forcefield.rs:243-265); box = 3 edge lengths. */
+gr_status gr_set_box(gr_ctx* ctx, const double box[3]);
+/* conf.current().pos -> device (host buffer, n_atoms*3 FP64). */
+gr_status gr_positions_upload(gr_ctx* ctx, const double* xyz);
+/* Device pointer to the FP64 positions (n_atoms*3), for device-resident MD. */
+gr_status gr_positions_device(gr_ctx* ctx, double** dev_xyz);
+
+/* ---- pairlist ----------------------------------------------------------- */
+/* PairlistAlgorithm::update (pairlist.rs:828-839): rebuild now, reset counter. */
+gr_status gr_pairlist_build(gr_ctx* ctx);
+/* Sizes of the four lists in the reference's atom-pair form:
+ * counts[0] solute_short, [1] solute_long, [2] solvent_short (first-atom
+ * sentinel pairs), [3] solvent_long (PairlistContainer, pairlist.rs:59-70). */
+gr_status gr_pairlist_counts(gr_ctx* ctx, int64_t counts[4]);
+/* The four lists, each as (i, j) int32 pairs sorted ascending; the caller
+ * passes buffers of 2*counts[k] int32 (any may be NULL). */
+gr_status gr_pairlist_download(gr_ctx* ctx, int32_t* solute_short, int32_t* solute_long,
+                               int32_t* solvent_short, int32_t* solvent_long);
+/* Charge-group pair set: (cg1 < cg2, range) with range 0 short / 1 long,
+ * sorted; *n_pairs in/out (capacity in, count out). */
+gr_status gr_pairlist_cg_pairs(gr_ctx* ctx, int32_t* cg_pairs_3xn, int64_t* n_pairs);
+
+/* ---- evaluation --------------------------------------------------------- */
+/* One `Forcefield::apply` nonbonded evaluation (forcefield.rs:226-1020):
+ * rebuild when NSNB says so, short range every call, twin-range long range
+ * refreshed at rebuilds and reused in between, RF excluded + self terms,
+ * 1-4 pairs, soft-core FEP corrections.  Positions must be current. */
+gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out);
+/* Device pointer to the last evaluation's FP64 forces (n_atoms*3). */
+gr_status gr_forces_device(gr_ctx* ctx, const double** dev_forces);
+/* Read back the last evaluation (for GR_EVAL_NO_DOWNLOAD). */
+gr_status gr_result_download(gr_ctx* ctx, gr_result* out);
+/* Device-event timing of the last evaluation's stages in ms:
+ * [0] pairlist build, [1] short-range force kernels, [2] long-range force
+ * kernels, [3] excluded/1-4/FEP terms, [4] total. */
+gr_status gr_last_timings(gr_ctx* ctx, float ms[5]);
+
+/* ---- measurement utilities (no counterpart in gromos-rs) ---------------- */
+/* Kernels launched by this context since creation (for launch accounting). */
+gr_status gr_ctx_launches(gr_ctx* ctx, int64_t* n);
+/* FP32 FMA issue rate of `device`, measured with an FFMA-chain kernel; one
+ * FFMA counts as one operation (the force kernel's operation convention). */
+gr_status gr_ffma_peak(int device, double* ops_per_s);
+
+/* ---- reference FFI stub replacement ------------------------------------ */
+/* Replaces `rust_lj_crf_innerloop` (crates/gromos-core/src/ffi.rs:55-103):
+ * lj_crf_innerloop over an explicit atom-pair list with per-atom nearest
+ * image (innerloops.rs:169-210), evaluated on device 0.  lj_params holds
+ * (c6, c12) per type pair; q_i*q_j is scaled by four_pi_eps_i = 138.9354
+ * (crates/gromos-core/src/units.rs:53); boundary_type 0 vacuum, 1
+ * rectangular (2 = triclinic is rejected).  Outputs are overwritten.
+ * Returns GR_OK or an error (the stub returned void). */
+gr_status gr_lj_crf_innerloop(const float* positions, const float* charges, const uint32_t* iac,
+                              uint32_t n_atoms, const uint32_t* pairlist, uint32_t n_pairs,
+                              const double* lj_params, uint32_t n_types, const double* box_data,
+                              uint32_t boundary_type, double crf_cut, double crf_2cut3i,
+                              double crf_cut3i, float* forces, double* energies, double* virial);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GROMOS_NB_H */

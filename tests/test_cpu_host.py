@@ -1,0 +1,96 @@
+"""CPU-only checks of the host side: the C-ABI library loads and exports every
+declared entry point, calls fail cleanly without a GPU, and the host helpers
+(GROMOS readers, generators, CRF parameters) agree with the oracle."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle_binding as ob
+from gromos_nb import _lib, generators
+from gromos_nb.nonbonded import CRFParameters
+
+
+def _have_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="module")
+def libnb():
+    if not os.path.exists(_lib.LIB_PATH):
+        _lib.build()
+    return _lib.lib()
+
+
+def test_library_exports_every_declared_symbol(libnb):
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    declared = _lib.declared_symbols()
+    assert declared, "no declarations found"
+    missing = [s for s in declared if s not in exported]
+    assert not missing, missing
+
+
+def test_build_targets_sm100a():
+    assert "arch=compute_100a,code=sm_100a" in _lib.NVCC_FLAGS
+
+
+@pytest.mark.skipif(_have_gpu(), reason="checks the no-device error path")
+def test_no_device_is_an_error(libnb):
+    h = C.c_void_p()
+    st = libnb.gr_ctx_create(0, C.byref(h))
+    assert st == _lib.GR_ERR_NO_DEVICE
+    assert b"no CUDA device" in libnb.gr_last_error()
+
+
+def test_null_context_is_rejected(libnb):
+    assert libnb.gr_set_box(None, None) == _lib.GR_ERR_INVALID
+    assert libnb.gr_forces_eval(None, 0, None) == _lib.GR_ERR_INVALID
+
+
+def test_crf_parameters_match_oracle():
+    for rc, eps_rf, kappa in [(1.4, 61.0, 0.0), (0.9, 62.0, 0.0), (1.4, 78.5, 0.0), (1.2, 66.0, 0.5)]:
+        py = CRFParameters.new(rc, 1.0, eps_rf, kappa)
+        orc = ob.crf_params(rc, 1.0, eps_rf, kappa)
+        assert (py.crf_cut, py.crf_2cut3i, py.crf_cut3i, py.cutoff_sq) == tuple(orc)
+
+
+def test_spc_generator_geometry_and_contacts():
+    s = generators.config1_spc1000()
+    pos = s.pos.reshape(-1, 3, 3)
+    oh = np.linalg.norm(pos[:, 1] - pos[:, 0], axis=1)
+    assert np.allclose(oh, 0.1, atol=1e-12)
+    ang = np.degrees(np.arccos(np.einsum("ij,ij->i", pos[:, 1] - pos[:, 0], pos[:, 2] - pos[:, 0]) / 0.01))
+    assert np.allclose(ang, 109.47, atol=1e-9)
+    from scipy.spatial import cKDTree
+    t = cKDTree(np.mod(s.pos, 3.104), boxsize=3.104)
+    pairs = t.query_pairs(0.15, output_type="ndarray")
+    mol = np.repeat(np.arange(1000), 3)
+    assert not np.any(mol[pairs[:, 0]] != mol[pairs[:, 1]])
+    # seeded: same seed, same positions
+    assert np.array_equal(s.pos, generators.config1_spc1000().pos)
+
+
+def test_solute_generator_neutral_charge_groups():
+    s = generators.solvated_solute_system(400, 60, seed=3, perturbed=True)
+    t = s.topo
+    for c in range(t.n_solute_cg):
+        a, b = t.cg_offsets[c], t.cg_offsets[c + 1]
+        assert 3 <= b - a <= 5
+        assert abs(t.charge[a:b].sum()) < 1e-12
+        assert abs(t.pert_b_q[a:b].sum()) < 1e-12
+    assert t.n_atoms == 60 + 3 * 400
+
+
+def test_gromos_reader_roundtrip_fixture():
+    from golden_loader import load_fixture
+    s, ex = load_fixture("ch4_water_fep")
+    assert s.topo.n_atoms == 2998 and s.topo.n_solute_cg == 1 and s.topo.n_egroups == 2
+    assert s.params.rcutp == 0.8 and s.params.rcutl == 1.4 and s.params.nsnb == 1
+    assert s.topo.pert_idx[0] == 0 and s.topo.pert_alpha_lj[0] == 0.25  # 0.5 * ALPHLJ 0.5

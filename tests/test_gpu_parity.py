@@ -1,0 +1,198 @@
+"""GPU parity: the CUDA path through the C ABI against the FP64 oracle.
+
+* Pairlist: the four reference lists (solute_short, solute_long,
+  solvent_short, solvent_long) must be IDENTICAL as sorted atom-pair sets
+  (bit-exact; the reference's own cell-list-vs-standard check,
+  pairlist.rs:1121-1302, compares the same sets).
+* Forces: RMS relative error sqrt(sum|dF|^2 / sum|F|^2) <= 1e-5 for the
+  fixed-point kernel (BASELINE target), <= 1e-4 for the plain FP32 kernel;
+  max relative error max|dF_i| / max(|F_i|, 1e-3 RMS|F|) <= 1e-3.
+* Energies (per group and totals) and the virial: relative 1e-5 of the
+  largest magnitude in the set (FP32 pair arithmetic).
+* dH/dlambda: relative 1e-5 (FP64 perturbation kernels).
+"""
+import numpy as np
+import pytest
+
+import oracle_binding as ob
+from golden_loader import load_fixture
+from gromos_nb import generators
+from gromos_nb.nonbonded import Forcefield
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = ["water_216_box", "water_1000_spc_gridcell", "ch4_water_fep", "nacl_water_box",
+            "water_3_box_twinrange", "water_10_box", "nacl_3water_box", "nacl_pair_box"]
+
+
+def sorted_pairs(a):
+    a = np.asarray(a, dtype=np.int64).reshape(-1, 2)
+    if a.size == 0:
+        return a
+    return a[np.lexsort((a[:, 1], a[:, 0]))]
+
+
+def force_errors(f, ref):
+    df = f - ref
+    rms = float(np.sqrt((df * df).sum() / max((ref * ref).sum(), 1e-300)))
+    mag = np.linalg.norm(ref, axis=1)
+    floor = 1e-3 * np.sqrt((mag ** 2).mean())
+    mx = float((np.linalg.norm(df, axis=1) / np.maximum(mag, floor)).max())
+    return rms, mx
+
+
+def rel(a, b, scale=None):
+    s = scale if scale is not None else max(abs(b), 1e-12)
+    return abs(a - b) / s
+
+
+def check_pairlist(s):
+    ff = Forcefield(s, kernel="fixed")
+    ff.upload_positions(s.pos)
+    ff.build_pairlist()
+    got = ff.pairlist_lists()
+    ref = ob.pairlist(s, algorithm=0 if s.topo.n_atoms < 4000 else 2)
+    for k in range(4):
+        g, r = sorted_pairs(got[k]), sorted_pairs(ref[k])
+        assert g.shape == r.shape, (s.name, k, g.shape, r.shape)
+        assert np.array_equal(g, r), (s.name, k)
+    ff.close()
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_pairlist_bit_exact_fixtures(name):
+    s, _ = load_fixture(name)
+    check_pairlist(s)
+
+
+def test_pairlist_bit_exact_spc1000():
+    check_pairlist(generators.config1_spc1000())
+
+
+def test_pairlist_bit_exact_solute_small_box():
+    # box < 2 * cutoff: one cell per axis, per-atom images for solute pairs
+    check_pairlist(generators.solvated_solute_system(500, 200, seed=1003, rc=1.4))
+
+
+def test_pairlist_bit_exact_spc30000_twin_range():
+    check_pairlist(generators.config2_spc30000())
+
+
+def compare_eval(s, kernel="fixed", steps=1, tol_rms=1e-5, tol_e=1e-5, move=0.0, seed=0):
+    ff = Forcefield(s, kernel=kernel)
+    orc = ob.OracleForcefield(s)
+    rng = np.random.default_rng(seed)
+    pos = s.pos.copy()
+    worst = 0.0
+    for step in range(steps):
+        r = ff.apply(pos)
+        o = orc.apply(pos)
+        rms, mx = force_errors(r["forces"], o["forces"])
+        worst = max(worst, rms)
+        assert rms <= tol_rms, (s.name, kernel, step, rms)
+        assert mx <= 1e-3 if kernel == "fixed" else mx <= 1e-2, (s.name, kernel, step, mx)
+        escale = max(abs(o["e_lj"]), abs(o["e_crf"]), 1e-9)
+        assert rel(r["e_lj"], o["e_lj"], escale) <= tol_e, (s.name, step, r["e_lj"], o["e_lj"])
+        assert rel(r["e_crf"], o["e_crf"], escale) <= tol_e, (s.name, step, r["e_crf"], o["e_crf"])
+        vscale = max(np.abs(o["virial"]).max(), 1e-9)
+        assert np.abs(r["virial"] - o["virial"]).max() <= tol_e * 10 * vscale, (s.name, step)
+        if kernel == "fixed":
+            gscale = max(np.abs(o["egroup_lj"]).max(), np.abs(o["egroup_crf"]).max(), 1e-9)
+            assert np.abs(r["egroup_lj"] - o["egroup_lj"]).max() <= tol_e * gscale
+            assert np.abs(r["egroup_crf"] - o["egroup_crf"]).max() <= tol_e * gscale
+        if abs(o["dhdl"]) > 0:
+            assert rel(r["dhdl"], o["dhdl"], max(abs(o["dhdl"]), 1.0)) <= 1e-5, (r["dhdl"], o["dhdl"])
+        if move:
+            pos = pos + rng.normal(0.0, move, size=pos.shape)
+    ff.close()
+    orc.close()
+    return worst
+
+
+@pytest.mark.parametrize("name", FIXTURES + ["pair_lj", "pair_lj_mixed", "nacl_pair"])
+def test_forces_fixtures_fixed(name):
+    s, _ = load_fixture(name)
+    compare_eval(s, "fixed")
+
+
+@pytest.mark.parametrize("name", ["water_216_box", "ch4_water_fep", "nacl_water_box"])
+def test_forces_fixtures_plain(name):
+    s, _ = load_fixture(name)
+    compare_eval(s, "plain", tol_rms=1e-4, tol_e=1e-4)
+
+
+def test_spc1000_fixed_and_plain():
+    s = generators.config1_spc1000()
+    compare_eval(s, "fixed")
+    compare_eval(s, "plain", tol_rms=1e-4, tol_e=1e-4)
+
+
+def test_twin_range_cache_over_steps():
+    """Short range every step, long range refreshed every NSNB steps (forcefield.rs:620-697)."""
+    s = generators.spc_water_system(2000, box=generators.box_for_waters(2000), seed=21, rcutp=0.8, rcutl=1.4,
+                                    nsnb=3)
+    compare_eval(s, "fixed", steps=7, move=0.002, seed=5)
+
+
+def test_fep_synthetic_windows():
+    for lam in (0.0, 0.35, 1.0):
+        s = generators.solvated_solute_system(700, 30, seed=1004, perturbed=True, lam=lam, rc=1.4)
+        s.params.lam = lam
+        compare_eval(s, "fixed")
+
+
+def test_solute_small_box_per_atom_images():
+    s = generators.solvated_solute_system(500, 200, seed=1003, rc=1.4)
+    compare_eval(s, "fixed", steps=3, move=0.002)
+
+
+def test_deterministic_bits():
+    s = generators.config1_spc1000()
+    ff = Forcefield(s, kernel="fixed")
+    a = ff.apply(s.pos, force_rebuild=True)
+    b = ff.apply(s.pos, force_rebuild=True)
+    assert np.array_equal(a["forces"], b["forces"])
+    assert a["e_lj"] == b["e_lj"] and a["e_crf"] == b["e_crf"]
+    assert np.array_equal(a["virial"], b["virial"])
+    ff.close()
+
+
+def test_pair_counts_match_oracle_lists():
+    s = generators.config1_spc1000()
+    ff = Forcefield(s, kernel="fixed")
+    r = ff.apply(s.pos)
+    lists = ob.pairlist(s)
+    n_expected = len(lists[0]) + len(lists[1]) + 9 * len(lists[2]) + len(lists[3])
+    assert r["n_pairs_short"] + r["n_pairs_long"] == n_expected
+    ff.close()
+
+
+def test_innerloop_stub_replacement():
+    """gr_lj_crf_innerloop (ffi.rs:55-103 with a body) against the FP64 inner loop."""
+    from gromos_nb.nonbonded import CRFParameters, lj_crf_innerloop
+    s, _ = load_fixture("nacl_water_box")
+    lists = ob.pairlist(s, algorithm=0)
+    pairs = np.concatenate([lists[0], lists[1], lists[3]])
+    crf = CRFParameters.new(s.params.rcutl, 1.0, s.params.epsrf, 0.0)
+    lj = s.topo.lj[:, :, :2].copy()
+    f, elj, ecrf, vir = lj_crf_innerloop(s.pos, s.topo.charge, s.topo.iac, pairs, lj, crf, box=s.box)
+    # FP64 reference over the same explicit pairs
+    fpe = 138.9354
+    ref = np.zeros_like(s.pos)
+    e1 = e2 = 0.0
+    for i, j in pairs:
+        r = s.pos[i] - s.pos[j]
+        r -= s.box * np.round(r / s.box)
+        r2 = r @ r
+        c6, c12 = s.topo.lj[s.topo.iac[i], s.topo.iac[j], :2]
+        q = s.topo.charge[i] * s.topo.charge[j] * fpe
+        ir2 = 1 / r2
+        ir6 = ir2 ** 3
+        e1 += (c12 * ir6 - c6) * ir6
+        e2 += q * (np.sqrt(ir2) - crf.crf_2cut3i * r2 - crf.crf_cut)
+        fs = (12 * c12 * ir6 - 6 * c6) * ir6 * ir2 + q * (np.sqrt(ir2) * ir2 + crf.crf_cut3i)
+        ref[i] += r * fs
+        ref[j] -= r * fs
+    rms, _ = force_errors(f.astype(np.float64), ref)
+    assert rms < 1e-4
+    assert rel(ecrf, e2) < 1e-4 and rel(elj, e1) < 1e-3
