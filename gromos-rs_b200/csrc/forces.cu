@@ -366,7 +366,11 @@ __global__ void __launch_bounds__(128) k_solute_force(const SysDev* __restrict__
                                        y, z);
                     const float r2 = fmaf(x, x, fmaf(y, y, z * z));
                     if (r2 < 1e-10f) continue;
-                    const float ri = rsqrtf(r2), ri2 = ri * ri, ri6 = ri2 * ri2 * ri2;
+                    // one Newton step on the hardware reciprocal square root removes its
+                    // bias from the (cancelling) CRF energy sums of solute pairs
+                    float ri = rsqrtf(r2);
+                    ri = fmaf(0.5f * ri, fmaf(-r2 * ri, ri, 1.0f), ri);
+                    const float ri2 = ri * ri, ri6 = ri2 * ri2 * ri2;
                     const float2 lj = s.lj32[s.iac[ai] * s.n_types + tj];
                     const float q = float(s.charge[ai] * s.fpe) * qj;
                     const float el = fmaf(lj.y, ri6, -lj.x) * ri6;

@@ -8,7 +8,7 @@ orientation.  Orientations that bring an H of one molecule within 0.15 nm of
 an atom of another are re-drawn (seeded) until no such contact remains.
 
 Solute (REMD / FEP / serving workloads): charge groups of 3-5 atoms within
-0.15 nm of a CG centre, placed in a cavity (waters whose O is within 0.35 nm
+0.15 nm of a CG centre (centres >= 0.55 nm apart), placed in a cavity (waters whose O is within 0.35 nm
 of a solute atom are removed); charges ~ N(0, 0.3 e) shifted to zero net
 charge per CG; C6/C12 = SPC O values x U[0.5, 2] combined by geometric mean;
 all intra-CG pairs excluded.
@@ -135,24 +135,41 @@ def solvated_solute_system(n_waters: int, n_solute_atoms: int, seed: int, rc: fl
         left -= s
     sizes.append(left)
     ncg = len(sizes)
-    # CG centres in a compact blob near the box centre
-    spread = max(0.35, 0.3 * ncg ** (1.0 / 3.0))
-    cg_centres = box / 2 + rng.uniform(-spread, spread, size=(ncg, 3))
+    # CG centres near the box centre, at least 0.55 nm apart (seeded rejection),
+    # so atoms of different CGs stay >= 0.25 nm apart
+    spread = max(0.35, 0.42 * ncg ** (1.0 / 3.0))
+    cg_centres = []
+    tries = 0
+    while len(cg_centres) < ncg:
+        c = box / 2 + rng.uniform(-spread, spread, size=3)
+        if all(np.linalg.norm(c - d) >= 0.55 for d in cg_centres):
+            cg_centres.append(c)
+        tries += 1
+        if tries > 200 * ncg:
+            spread *= 1.1
+            tries = 0
+    cg_centres = np.asarray(cg_centres)
     sol_pos = []
     for c, s in zip(cg_centres, sizes):
         d = rng.normal(size=(s, 3))
         d /= np.linalg.norm(d, axis=1, keepdims=True)
         sol_pos.append(c + d * rng.uniform(0.05, 0.15, size=(s, 1)))
     sol_pos = np.concatenate(sol_pos)
-    # waters: generate a full box and carve a cavity
-    wpos = spc_positions(n_waters + 4 * n_solute_atoms, box, seed + 7919).reshape(-1, 3, 3)
+    # waters: fill the box at liquid density, carve a cavity around the solute,
+    # grow the box (seeded, 2% steps) until n_waters remain, keep a seeded subset
     from scipy.spatial import cKDTree
 
-    tree = cKDTree(np.mod(sol_pos, box), boxsize=box)
-    d, _ = tree.query(np.mod(wpos[:, 0, :], box))
-    keep = np.nonzero(d > 0.35)[0][:n_waters]
-    if keep.size < n_waters:
-        raise ValueError("box too small for the requested number of waters")
+    while True:
+        n_fill = int(round(33.4 * box ** 3))
+        wpos = spc_positions(max(n_fill, n_waters), box, seed + 7919).reshape(-1, 3, 3)
+        tree = cKDTree(np.mod(sol_pos, box), boxsize=box)
+        d, _ = tree.query(np.mod(wpos[:, 0, :], box))
+        ok = np.nonzero(d > 0.35)[0]
+        if ok.size >= n_waters:
+            break
+        box *= 1.02
+        sol_pos = sol_pos - (box / 1.02) / 2 + box / 2
+    keep = np.sort(rng.permutation(ok)[:n_waters])
     wpos = wpos[keep].reshape(-1, 3)
     nsa = sol_pos.shape[0]
     nat = nsa + 3 * n_waters
