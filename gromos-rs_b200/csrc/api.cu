@@ -637,13 +637,15 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     const int sm = sm_count();
     const size_t shg = size_t(2 * G * G) * sizeof(unsigned long long);
     if (prm.kernel == GR_KERNEL_FIXED) {
+        WaterParams wp;
         if (NCG > NSCG) {
+            wp = water_params();
             (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
             unsigned grid = unsigned(sm * water_blocks_per_sm);
             if (h.water_lj00_only)
-                (++launches, k_water_force<4, true, false><<<grid, 128, 0, s>>>(d_sys));
+                (++launches, k_water_force<true, false><<<grid, 128, 0, s>>>(d_sys, wp));
             else
-                (++launches, k_water_force<4, false, false><<<grid, 128, 0, s>>>(d_sys));
+                (++launches, k_water_force<false, false><<<grid, 128, 0, s>>>(d_sys, wp));
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
         if (record_events) GR_CUDA(cudaEventRecord(ev[2], s));
@@ -651,11 +653,12 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             GR_CUDA(cudaMemsetAsync(h.f_long, 0, size_t(N) * 3 * sizeof(long long), s));
             GR_CUDA(cudaMemsetAsync(h.acc_long, 0, size_t(NA) * sizeof(long long), s));
             if (NCG > NSCG) {
+                WaterParams wpl = water_params(true);
                 unsigned grid = unsigned(sm * water_blocks_per_sm);
                 if (h.water_lj00_only)
-                    (++launches, k_water_force<4, true, true><<<grid, 128, 0, s>>>(d_sys));
+                    (++launches, k_water_force<true, true><<<grid, 128, 0, s>>>(d_sys, wpl));
                 else
-                    (++launches, k_water_force<4, false, true><<<grid, 128, 0, s>>>(d_sys));
+                    (++launches, k_water_force<false, true><<<grid, 128, 0, s>>>(d_sys, wpl));
             }
             if (NSCG > 0) (++launches, k_solute_force<true><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
             lr_computed = true;
@@ -688,6 +691,30 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     GR_CUDA(cudaGetLastError());
     last_long = do_long;
     return GR_OK;
+}
+
+// Per-launch constants of the water kernel.  `lim` keeps the FP32 image
+// decision away from half a box edge: 1e-4 nm covers the FP32 rounding of the
+// first-atom vector (short list); per-atom images (long list) also need room
+// for both molecules' extents (0.6 nm covers any 3-site water geometry).
+WaterParams NbSystem::water_params(bool long_range) const {
+    WaterParams wp;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            wp.qq[a * 3 + b] = h.w_qq[a * 4 + b];
+            wp.c6[a * 3 + b] = h.w_c6[a * 4 + b];
+            wp.c12[a * 3 + b] = h.w_c12[a * 4 + b];
+        }
+    wp.crf2 = h.crf_2cut3i_f;
+    wp.crfc = h.crf_cut_f;
+    wp.crf3 = h.crf_cut3i_f;
+    const float margin = long_range ? 0.6f : 1e-4f;
+    for (int k = 0; k < 3; ++k) wp.lim[k] = h.boundary ? h.half_boxf[k] - margin : 3.0e38f;
+    wp.boundary = h.boundary;
+    wp.G = G;
+    const int gs = solvent_group < 0 ? 0 : solvent_group;
+    wp.slot = gs * G + gs;
+    return wp;
 }
 
 int NbSystem::sm_count() {

@@ -18,8 +18,7 @@
 //
 // Kernels:
 //   k_water_prep        per step: FP64 first-atom position + FP32 offsets, slot order
-//   k_water_force<W,..> water-water clusters: warp per i-cluster of W waters,
-//                       lane per j-water, forces in 64-bit fixed point
+//   (water-water clusters: water.cu)
 //   k_solute_force<..>  solute CG pairs (any CG size <= 8, LJ type table)
 //   k_plain_force       baseline: thread per CG pair, absolute FP32, FP32 atomics
 //   k_excluded_14       FP64 RF excluded / self terms (excluded.rs:25-112) and
@@ -67,218 +66,6 @@ __device__ __forceinline__ void block_flush(long long (&acc)[NV], long long* __r
     __syncthreads();
     for (int v = threadIdx.x; v < NV; v += blockDim.x)
         if (sh[v]) atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx[v]), sh[v]);
-}
-
-// Exact per-CG-pair (or per-atom, LONG) pair vectors for the rare pairs whose
-// FP32 vector is too close to half a box edge to decide the image in FP32.
-template <bool LONG>
-__device__ __noinline__ void water_slow_vectors(const SysDev& s, int islot, int jslot, float* rx,
-                                                float* ry, float* rz) {
-    int ci = s.slot_cg[islot], cj = s.slot_cg[jslot];
-    int ai = s.cg_off[ci], aj = s.cg_off[cj];
-    if (!LONG) {
-        double dx, dy, dz;
-        nearest_image_exact(s, s.pos[3 * ai], s.pos[3 * ai + 1], s.pos[3 * ai + 2], s.pos[3 * aj],
-                            s.pos[3 * aj + 1], s.pos[3 * aj + 2], dx, dy, dz);
-        // t = image - (x_i0 - x_j0); r_ab = (x_ia + t) - x_jb  (innerloops.rs:264-282)
-        double tx = dx - s.pos[3 * ai] + s.pos[3 * aj];
-        double ty = dy - s.pos[3 * ai + 1] + s.pos[3 * aj + 1];
-        double tz = dz - s.pos[3 * ai + 2] + s.pos[3 * aj + 2];
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) {
-                rx[a * 3 + b] = float(s.pos[3 * (ai + a)] + tx - s.pos[3 * (aj + b)]);
-                ry[a * 3 + b] = float(s.pos[3 * (ai + a) + 1] + ty - s.pos[3 * (aj + b) + 1]);
-                rz[a * 3 + b] = float(s.pos[3 * (ai + a) + 2] + tz - s.pos[3 * (aj + b) + 2]);
-            }
-    } else {
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) {
-                double dx, dy, dz;
-                nearest_image_exact(s, s.pos[3 * (ai + a)], s.pos[3 * (ai + a) + 1], s.pos[3 * (ai + a) + 2],
-                                    s.pos[3 * (aj + b)], s.pos[3 * (aj + b) + 1], s.pos[3 * (aj + b) + 2], dx,
-                                    dy, dz);
-                rx[a * 3 + b] = float(dx);
-                ry[a * 3 + b] = float(dy);
-                rz[a * 3 + b] = float(dz);
-            }
-    }
-}
-
-// Water-water forces.  One warp per i-cluster of W three-site waters (kept in
-// registers as FP32 offsets from the cluster's first oxygen), one lane per
-// j-water of the cluster's list; bit k of an entry's mask selects the pair
-// (i_k, j).  i-forces accumulate in registers over the whole list and are
-// warp-reduced once per cluster; j-forces are added once per (cluster, j).
-// LJ00: the solvent LJ table is non-zero only between sites 0 and 0 (SPC).
-template <int W, bool LJ00, bool LONG>
-__global__ void __launch_bounds__(128) k_water_force(const SysDev* __restrict__ sys) {
-    const SysDev& s = sys[blockIdx.y];
-    const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
-    const int nclus = s.n_clusters[0];
-    long long* __restrict__ F = LONG ? s.f_long : s.f_short;
-    // |r00| must stay this far inside half a box edge for the FP32 image to
-    // be certain; per-atom images (LONG) need room for both molecules' extents.
-    const float margin = LONG ? 0.6f : 1e-4f;
-    const float limx = s.boundary ? s.half_boxf[0] - margin : 3.0e38f;
-    const float limy = s.boundary ? s.half_boxf[1] - margin : 3.0e38f;
-    const float limz = s.boundary ? s.half_boxf[2] - margin : 3.0e38f;
-    const float crf2 = s.crf_2cut3i_f, crfc = s.crf_cut_f, crf3 = s.crf_cut3i_f;
-    float qq[9], c6[9], c12[9];
-#pragma unroll
-    for (int t = 0; t < 9; ++t) {
-        qq[t] = s.w_qq[(t / 3) * 4 + t % 3];
-        c6[t] = s.w_c6[(t / 3) * 4 + t % 3];
-        c12[t] = s.w_c12[(t / 3) * 4 + t % 3];
-    }
-    long long acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // lj, crf, vxx, vxy, vxz, vyy, vyz, vzz
-    const uint32_t* __restrict__ wl = LONG ? s.wl_l : s.wl_s;
-    const int* __restrict__ wn = LONG ? s.wn_l : s.wn_s;
-
-    for (int ci = blockIdx.x * wpb + (threadIdx.x >> 5); ci < nclus; ci += gridDim.x * wpb) {
-        const int n = s.clus_n[ci];
-        const int base = ci * W;
-        const double x00 = s.wfirst[3 * base], y00 = s.wfirst[3 * base + 1], z00 = s.wfirst[3 * base + 2];
-        float px[W][3], py[W][3], pz[W][3];
-        float fx[W][3], fy[W][3], fz[W][3];
-#pragma unroll
-        for (int k = 0; k < W; ++k) {
-            float ex = 0.f, ey = 0.f, ez = 0.f;
-            if (k < n) {
-                ex = float(s.wfirst[3 * (base + k)] - x00);
-                ey = float(s.wfirst[3 * (base + k) + 1] - y00);
-                ez = float(s.wfirst[3 * (base + k) + 2] - z00);
-            }
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                float4 d = k < n ? s.wdel[(base + k) * 3 + a] : make_float4(0.f, 0.f, 0.f, 0.f);
-                px[k][a] = ex + d.x;
-                py[k][a] = ey + d.y;
-                pz[k][a] = ez + d.z;
-                fx[k][a] = fy[k][a] = fz[k][a] = 0.f;
-            }
-        }
-        float elj = 0.f, ecrf = 0.f, vxx = 0.f, vxy = 0.f, vxz = 0.f, vyy = 0.f, vyz = 0.f, vzz = 0.f;
-        const int cnt = wn[ci];
-        const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * s.wcap;
-        for (int e0 = 0; e0 < cnt; e0 += 32) {
-            const int e = e0 + lane;
-            const uint32_t ent = e < cnt ? list[e] : 0u;
-            const unsigned mask = ent & 0xffu;
-            const int js = static_cast<int>(ent >> 8);
-            float qx[3], qy[3], qz[3];
-            float gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
-            if (mask) {
-                double dx = x00 - s.wfirst[3 * js], dy = y00 - s.wfirst[3 * js + 1], dz = z00 - s.wfirst[3 * js + 2];
-                if (s.boundary) {
-                    dx -= s.box[0] * rint(dx * s.inv_box[0]);
-                    dy -= s.box[1] * rint(dy * s.inv_box[1]);
-                    dz -= s.box[2] * rint(dz * s.inv_box[2]);
-                }
-                const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    float4 d = s.wdel[js * 3 + b];
-                    qx[b] = d.x - Dx;
-                    qy[b] = d.y - Dy;
-                    qz[b] = d.z - Dz;
-                }
-            } else {
-#pragma unroll
-                for (int b = 0; b < 3; ++b) qx[b] = qy[b] = qz[b] = 0.f;
-            }
-#pragma unroll
-            for (int k = 0; k < W; ++k) {
-                const bool act = (mask >> k) & 1u;
-                if (!__any_sync(0xffffffffu, act)) continue;
-                if (!act) continue;
-                float rx[9], ry[9], rz[9];
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-#pragma unroll
-                    for (int b = 0; b < 3; ++b) {
-                        rx[a * 3 + b] = px[k][a] - qx[b];
-                        ry[a * 3 + b] = py[k][a] - qy[b];
-                        rz[a * 3 + b] = pz[k][a] - qz[b];
-                    }
-                if (!(fabsf(rx[0]) < limx && fabsf(ry[0]) < limy && fabsf(rz[0]) < limz))
-                    water_slow_vectors<LONG>(s, base + k, js, rx, ry, rz);
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-#pragma unroll
-                    for (int b = 0; b < 3; ++b) {
-                        const int t = a * 3 + b;
-                        const float x = rx[t], y = ry[t], z = rz[t];
-                        const float r2 = fmaf(x, x, fmaf(y, y, z * z));
-                        float ri = rsqrtf(r2);
-                        ri = r2 < 1e-10f ? 0.f : ri;
-                        const float ri2 = ri * ri;
-                        const float q = qq[t];
-                        ecrf = fmaf(q, fmaf(-crf2, r2, ri) - crfc, ecrf);
-                        float fs = q * fmaf(ri, ri2, crf3);
-                        if (!LJ00 || t == 0) {
-                            const float ri6 = ri2 * ri2 * ri2;
-                            elj = fmaf(fmaf(c12[t], ri6, -c6[t]), ri6, elj);
-                            fs = fmaf(fmaf(12.f * c12[t], ri6, -6.f * c6[t]), ri6 * ri2, fs);
-                        }
-                        const float fxx = x * fs, fyy = y * fs, fzz = z * fs;
-                        fx[k][a] += fxx;
-                        fy[k][a] += fyy;
-                        fz[k][a] += fzz;
-                        gx[b] -= fxx;
-                        gy[b] -= fyy;
-                        gz[b] -= fzz;
-                        vxx = fmaf(x, fxx, vxx);
-                        vxy = fmaf(x, fyy, vxy);
-                        vxz = fmaf(x, fzz, vxz);
-                        vyy = fmaf(y, fyy, vyy);
-                        vyz = fmaf(y, fzz, vyz);
-                        vzz = fmaf(z, fzz, vzz);
-                    }
-            }
-            if (mask) {
-                const int cgj = s.slot_cg[js];
-                const int aj = s.cg_off[cgj];
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    red_add(&F[3 * (aj + b)], to_fixed_f(gx[b], kF));
-                    red_add(&F[3 * (aj + b) + 1], to_fixed_f(gy[b], kF));
-                    red_add(&F[3 * (aj + b) + 2], to_fixed_f(gz[b], kF));
-                }
-            }
-        }
-        // i-forces: warp reduction, one lane per atom component writes
-#pragma unroll
-        for (int k = 0; k < W; ++k)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                float vx = warp_sum(fx[k][a]), vy = warp_sum(fy[k][a]), vz = warp_sum(fz[k][a]);
-                if (k < n && lane == ((k * 3 + a) & 31)) {
-                    const int at = s.cg_off[s.slot_cg[base + k]] + a;
-                    red_add(&F[3 * at], to_fixed_f(vx, kF));
-                    red_add(&F[3 * at + 1], to_fixed_f(vy, kF));
-                    red_add(&F[3 * at + 2], to_fixed_f(vz, kF));
-                }
-            }
-        float ev[8] = {elj, ecrf, vxx, vxy, vxz, vyy, vyz, vzz};
-#pragma unroll
-        for (int v = 0; v < 8; ++v) {
-            float t = warp_sum(ev[v]);
-            if (lane == 0) acc[v] += to_fixed_f(t, kE);
-        }
-    }
-    // flush energies / virial: group slot of the solvent, symmetric virial
-    const int G = s.n_egroups;
-    const int gs = s.solvent_group < 0 ? 0 : s.solvent_group;
-    const int slot = group_slot(G, gs, gs);
-    const int vb = 2 * G * G;
-    int idx[8] = {slot, G * G + slot, vb + 0, vb + 1, vb + 2, vb + 4, vb + 5, vb + 8};
-    long long* dst = LONG ? s.acc_long : s.acc_short;
-    block_flush<8>(acc, dst, idx);
-    // the symmetric lower triangle of the virial (yx, zx, zy)
-    long long acc2[3] = {acc[3], acc[4], acc[6]};
-    int idx2[3] = {vb + 3, vb + 6, vb + 7};
-    block_flush<3>(acc2, dst, idx2);
 }
 
 // ---------------------------------------------------------------------------
@@ -897,10 +684,6 @@ __global__ void k_finalize_plain_energies(const SysDev* __restrict__ sys) {
 }
 
 // Explicit instantiations used by the host runtime.
-template __global__ void k_water_force<4, true, false>(const SysDev*);
-template __global__ void k_water_force<4, true, true>(const SysDev*);
-template __global__ void k_water_force<4, false, false>(const SysDev*);
-template __global__ void k_water_force<4, false, true>(const SysDev*);
 template __global__ void k_solute_force<false>(const SysDev*);
 template __global__ void k_solute_force<true>(const SysDev*);
 

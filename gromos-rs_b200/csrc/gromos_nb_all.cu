@@ -2,4 +2,5 @@
 // launch sites are compiled together (whole-program CUDA compilation).
 #include "pairlist.cu"
 #include "forces.cu"
+#include "water.cu"
 #include "api.cu"

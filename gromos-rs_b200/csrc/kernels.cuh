@@ -17,8 +17,9 @@ __global__ void k_pert_pairs(const SysDev* __restrict__ sys);
 __global__ void k_expand_cgpairs(const SysDev* __restrict__ sys, int long_range);
 
 __global__ void k_water_prep(const SysDev* __restrict__ sys);
-template <int W, bool LJ00, bool LONG>
-__global__ void k_water_force(const SysDev* __restrict__ sys);
+struct WaterParams;
+template <bool LJ00, bool LONG>
+__global__ void k_water_force(const SysDev* __restrict__ sys, const WaterParams wp);
 template <bool LONG>
 __global__ void k_solute_force(const SysDev* __restrict__ sys);
 __global__ void k_pos32(const SysDev* __restrict__ sys);

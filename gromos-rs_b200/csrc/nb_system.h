@@ -11,6 +11,7 @@
 
 namespace gnb {
 
+struct WaterParams;
 void set_error(const std::string& m);
 void crf_params(double cutoff, double epsilon, double rf_epsilon, double rf_kappa, double out[4]);
 void lambda_params(double lam, int n, double lp[17]);
@@ -29,6 +30,7 @@ class NbSystem {
     gr_status pair_counts(cudaStream_t s, long long* n_short, long long* n_long);
     gr_status push_descriptor(cudaStream_t s);
     int sm_count();
+    WaterParams water_params(bool long_range = false) const;
 
     // sizes
     int N = 0, NCG = 0, NSCG = 0, NSA = 0, NT = 0, G = 1, aps = 3, W = 4;

@@ -1,0 +1,329 @@
+// water.cu -- water-water LJ + reaction-field forces (the hot kernel).
+//
+// Physics per atom pair: lj_crf_interaction
+// (crates/gromos-forces/src/nonbonded/innerloops.rs:21-55) with the solvent
+// parameter table of process_solvent_pairs (innerloops.rs:241-255); one
+// image per CG pair taken from the first atoms (innerloops.rs:264-267) for
+// the short list, per-atom images for the long list (innerloops.rs:186).
+//
+// Layout: one warp per i-cluster of W waters; the cluster's atoms live in
+// registers as FP32 offsets from the cluster's first oxygen; one lane per
+// j-water entry of the cluster's list; bit k of the entry mask selects the
+// pair (i_k, j).  The CG-pair image comes from an FP64 difference of first
+// oxygens; FP32 arithmetic for the pairs; forces are accumulated in 64-bit
+// fixed point (2^32 per kJ mol^-1 nm^-1): i-forces in registers over the
+// whole list, reduced once per cluster, j-forces once per (cluster, j).
+// A CG pair whose first-atom vector lies within `margin` of half a box edge
+// is redone with exact FP64 images (water_slow_pair), so image choices are
+// always those of the reference.
+#include "nb_common.cuh"
+
+namespace gnb {
+
+// Per-launch constants (kernel parameters live in the constant bank, so the
+// FP32 instructions read them without registers).
+struct WaterParams {
+    float qq[9];            // q_a q_b fpe of the first solvent molecule
+    float c6[9], c12[9];    // solvent LJ table
+    float crf2, crfc, crf3; // crf_2cut3i, crf_cut, crf_cut3i
+    float lim[3];           // half box edge - margin: FP32 image certain below this
+    int boundary;
+    int slot;               // energy-group slot of solvent-solvent pairs
+    int G;
+};
+
+__device__ __forceinline__ float rsqrt_fast(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+struct PairAcc {
+    float fi[9];  // i-water atoms a*3 + comp
+    float fj[9];  // j-water atoms b*3 + comp
+    float elj, ecrf, v[6];
+};
+
+// One CG pair (i water in slot islot, j water in slot jslot) with the
+// reference's exact FP64 images: the first-atom shift (short list) or
+// per-atom images (long list).  Used only for pairs near half a box edge.
+template <bool LJ00, bool LONG>
+__device__ __noinline__ PairAcc water_slow_pair(const SysDev& s, const WaterParams& wp, int islot, int jslot) {
+    PairAcc o;
+    for (int k = 0; k < 9; ++k) o.fi[k] = o.fj[k] = 0.f;
+    o.elj = o.ecrf = 0.f;
+    for (int k = 0; k < 6; ++k) o.v[k] = 0.f;
+    const int ai = s.cg_off[s.slot_cg[islot]], aj = s.cg_off[s.slot_cg[jslot]];
+    double tx = 0, ty = 0, tz = 0;
+    if (!LONG) {
+        double dx, dy, dz;
+        nearest_image_exact(s, s.pos[3 * ai], s.pos[3 * ai + 1], s.pos[3 * ai + 2], s.pos[3 * aj],
+                            s.pos[3 * aj + 1], s.pos[3 * aj + 2], dx, dy, dz);
+        tx = dx - s.pos[3 * ai] + s.pos[3 * aj];
+        ty = dy - s.pos[3 * ai + 1] + s.pos[3 * aj + 1];
+        tz = dz - s.pos[3 * ai + 2] + s.pos[3 * aj + 2];
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            const int t = a * 3 + b;
+            double dx, dy, dz;
+            if (LONG) {
+                nearest_image_exact(s, s.pos[3 * (ai + a)], s.pos[3 * (ai + a) + 1], s.pos[3 * (ai + a) + 2],
+                                    s.pos[3 * (aj + b)], s.pos[3 * (aj + b) + 1], s.pos[3 * (aj + b) + 2], dx, dy,
+                                    dz);
+            } else {
+                dx = s.pos[3 * (ai + a)] + tx - s.pos[3 * (aj + b)];
+                dy = s.pos[3 * (ai + a) + 1] + ty - s.pos[3 * (aj + b) + 1];
+                dz = s.pos[3 * (ai + a) + 2] + tz - s.pos[3 * (aj + b) + 2];
+            }
+            const float x = float(dx), y = float(dy), z = float(dz);
+            const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+            if (r2 < 1e-10f) continue;
+            const float ri = rsqrt_fast(r2), ri2 = ri * ri;
+            const float q = wp.qq[t];
+            o.ecrf = fmaf(q, fmaf(-wp.crf2, r2, ri) - wp.crfc, o.ecrf);
+            float fs = q * fmaf(ri, ri2, wp.crf3);
+            if (!LJ00 || t == 0) {
+                const float ri6 = ri2 * ri2 * ri2;
+                o.elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, o.elj);
+                fs = fmaf(fmaf(12.f * wp.c12[t], ri6, -6.f * wp.c6[t]), ri6 * ri2, fs);
+            }
+            const float fx = x * fs, fy = y * fs, fz = z * fs;
+            o.fi[a * 3] += fx;
+            o.fi[a * 3 + 1] += fy;
+            o.fi[a * 3 + 2] += fz;
+            o.fj[b * 3] -= fx;
+            o.fj[b * 3 + 1] -= fy;
+            o.fj[b * 3 + 2] -= fz;
+            o.v[0] = fmaf(x, fx, o.v[0]);
+            o.v[1] = fmaf(x, fy, o.v[1]);
+            o.v[2] = fmaf(x, fz, o.v[2]);
+            o.v[3] = fmaf(y, fy, o.v[3]);
+            o.v[4] = fmaf(y, fz, o.v[4]);
+            o.v[5] = fmaf(z, fz, o.v[5]);
+        }
+    return o;
+}
+
+// Reduce-scatter of a per-lane array of 36 = 4 waters x 9 components over the
+// warp: afterwards lane l (with (l & 7) == 0) holds the warp sum of the 9
+// components of water l >> 3 in out[0..8].
+__device__ __forceinline__ void reduce_scatter_36(const float (&v)[36], float (&out)[9], int lane) {
+    float w[18];
+    const bool h16 = lane & 16;
+#pragma unroll
+    for (int i = 0; i < 18; ++i) {
+        const float keep = h16 ? v[i + 18] : v[i];
+        const float send = h16 ? v[i] : v[i + 18];
+        w[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    const bool h8 = lane & 8;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const float keep = h8 ? w[i + 9] : w[i];
+        const float send = h8 ? w[i] : w[i + 9];
+        out[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        out[i] += __shfl_xor_sync(0xffffffffu, out[i], 4);
+        out[i] += __shfl_xor_sync(0xffffffffu, out[i], 2);
+        out[i] += __shfl_xor_sync(0xffffffffu, out[i], 1);
+    }
+}
+
+template <bool LJ00, bool LONG>
+__global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict__ sys, const WaterParams wp) {
+    constexpr int W = 4;
+    const SysDev& s = sys[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int nclus = s.n_clusters[0];
+    long long* __restrict__ F = LONG ? s.f_long : s.f_short;
+    const uint32_t* __restrict__ wl = LONG ? s.wl_l : s.wl_s;
+    const int* __restrict__ wn = LONG ? s.wn_l : s.wn_s;
+    const double* __restrict__ wfirst = s.wfirst;
+    const float4* __restrict__ wdel = s.wdel;
+    // per-lane fixed-point (2^24) accumulators of lj, crf, xx, xy, xz, yy, yz, zz:
+    // kept in shared memory (one slot per lane, no atomics) to free registers
+    __shared__ long long accs[128 * 8];
+    __shared__ float4 sp_all[4 * W * 3];
+    long long* __restrict__ my = accs + threadIdx.x * 8;
+#pragma unroll
+    for (int v = 0; v < 8; ++v) my[v] = 0;
+
+    for (int ci = blockIdx.x * wpb + (threadIdx.x >> 5); ci < nclus; ci += gridDim.x * wpb) {
+        const int n = s.clus_n[ci];
+        const int base = ci * W;
+        const double x00 = wfirst[3 * base], y00 = wfirst[3 * base + 1], z00 = wfirst[3 * base + 2];
+        // i-cluster atoms: FP32 offsets from the first oxygen, broadcast from shared memory
+        float4* __restrict__ sp = sp_all + (threadIdx.x >> 5) * (W * 3);
+        if (lane < W * 3) {
+            const int k = lane / 3, a = lane % 3;
+            float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < n) {
+                const float4 d = wdel[(base + k) * 3 + a];
+                p.x = float(wfirst[3 * (base + k)] - x00) + d.x;
+                p.y = float(wfirst[3 * (base + k) + 1] - y00) + d.y;
+                p.z = float(wfirst[3 * (base + k) + 2] - z00) + d.z;
+            }
+            sp[lane] = p;
+        }
+        __syncwarp();
+        float fi[36];
+#pragma unroll
+        for (int i = 0; i < 36; ++i) fi[i] = 0.f;
+        float elj = 0.f, ecrf = 0.f, v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f, v4 = 0.f, v5 = 0.f;
+        const int cnt = wn[ci];
+        const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * s.wcap;
+        for (int e0 = 0; e0 < cnt; e0 += 32) {
+            const int e = e0 + lane;
+            const uint32_t ent = e < cnt ? __ldg(list + e) : 0u;
+            const unsigned mask = ent & 0xffu;
+            const int js = static_cast<int>(ent >> 8);
+            float qx[3], qy[3], qz[3];
+            float gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
+            if (mask) {
+                double dx = x00 - wfirst[3 * js], dy = y00 - wfirst[3 * js + 1], dz = z00 - wfirst[3 * js + 2];
+                if (wp.boundary) {
+                    dx -= s.box[0] * rint(dx * s.inv_box[0]);
+                    dy -= s.box[1] * rint(dy * s.inv_box[1]);
+                    dz -= s.box[2] * rint(dz * s.inv_box[2]);
+                }
+                const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    const float4 d = wdel[js * 3 + b];
+                    qx[b] = d.x - Dx;
+                    qy[b] = d.y - Dy;
+                    qz[b] = d.z - Dz;
+                }
+            } else {
+#pragma unroll
+                for (int b = 0; b < 3; ++b) qx[b] = qy[b] = qz[b] = 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const bool act = (mask >> k) & 1u;
+                if (!__any_sync(0xffffffffu, act)) continue;
+                if (!act) continue;
+                const float4 p0 = sp[k * 3], p1 = sp[k * 3 + 1], p2 = sp[k * 3 + 2];
+                const float pxk[3] = {p0.x, p1.x, p2.x}, pyk[3] = {p0.y, p1.y, p2.y}, pzk[3] = {p0.z, p1.z, p2.z};
+                // first-atom vector: decides whether the FP32 image is certain
+                const float r0x = pxk[0] - qx[0], r0y = pyk[0] - qy[0], r0z = pzk[0] - qz[0];
+                if (!(fabsf(r0x) < wp.lim[0] && fabsf(r0y) < wp.lim[1] && fabsf(r0z) < wp.lim[2])) {
+                    const PairAcc o = water_slow_pair<LJ00, LONG>(s, wp, base + k, js);
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) {
+                        fi[k * 9 + c] += o.fi[c];
+                    }
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        gx[b] += o.fj[b * 3];
+                        gy[b] += o.fj[b * 3 + 1];
+                        gz[b] += o.fj[b * 3 + 2];
+                    }
+                    elj += o.elj;
+                    ecrf += o.ecrf;
+                    v0 += o.v[0];
+                    v1 += o.v[1];
+                    v2 += o.v[2];
+                    v3 += o.v[3];
+                    v4 += o.v[4];
+                    v5 += o.v[5];
+                    continue;
+                }
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        const int t = a * 3 + b;
+                        const float x = (a == 0 && b == 0) ? r0x : pxk[a] - qx[b];
+                        const float y = (a == 0 && b == 0) ? r0y : pyk[a] - qy[b];
+                        const float z = (a == 0 && b == 0) ? r0z : pzk[a] - qz[b];
+                        const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+                        const float ri = r2 < 1e-10f ? 0.f : rsqrt_fast(r2);
+                        const float ri2 = ri * ri;
+                        const float q = wp.qq[t];
+                        ecrf = fmaf(q, fmaf(-wp.crf2, r2, ri) - wp.crfc, ecrf);
+                        float fs = q * fmaf(ri, ri2, wp.crf3);
+                        if (!LJ00 || t == 0) {
+                            const float ri6 = ri2 * ri2 * ri2;
+                            elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, elj);
+                            fs = fmaf(fmaf(12.f * wp.c12[t], ri6, -6.f * wp.c6[t]), ri6 * ri2, fs);
+                        }
+                        const float fx = x * fs, fy = y * fs, fz = z * fs;
+                        fi[k * 9 + a * 3] += fx;
+                        fi[k * 9 + a * 3 + 1] += fy;
+                        fi[k * 9 + a * 3 + 2] += fz;
+                        gx[b] -= fx;
+                        gy[b] -= fy;
+                        gz[b] -= fz;
+                        v0 = fmaf(x, fx, v0);
+                        v1 = fmaf(x, fy, v1);
+                        v2 = fmaf(x, fz, v2);
+                        v3 = fmaf(y, fy, v3);
+                        v4 = fmaf(y, fz, v4);
+                        v5 = fmaf(z, fz, v5);
+                    }
+            }
+            if (mask) {
+                const int aj = s.cg_off[s.slot_cg[js]];
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    red_add(&F[3 * (aj + b)], to_fixed_f(gx[b], 4294967296.0f));
+                    red_add(&F[3 * (aj + b) + 1], to_fixed_f(gy[b], 4294967296.0f));
+                    red_add(&F[3 * (aj + b) + 2], to_fixed_f(gz[b], 4294967296.0f));
+                }
+            }
+        }
+        float red[9];
+        reduce_scatter_36(fi, red, lane);
+        __syncwarp();  // sp is rewritten by the next cluster
+        const int k = lane >> 3;
+        if ((lane & 7) == 0 && k < n) {
+            const int at = s.cg_off[s.slot_cg[base + k]];
+#pragma unroll
+            for (int c = 0; c < 9; ++c) red_add(&F[3 * at + c], to_fixed_f(red[c], 4294967296.0f));
+        }
+        my[0] += to_fixed_f(elj, 16777216.0f);
+        my[1] += to_fixed_f(ecrf, 16777216.0f);
+        my[2] += to_fixed_f(v0, 16777216.0f);
+        my[3] += to_fixed_f(v1, 16777216.0f);
+        my[4] += to_fixed_f(v2, 16777216.0f);
+        my[5] += to_fixed_f(v3, 16777216.0f);
+        my[6] += to_fixed_f(v4, 16777216.0f);
+        my[7] += to_fixed_f(v5, 16777216.0f);
+    }
+    long long acc[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) acc[v] = my[v];
+    // warp sums of the per-lane fixed-point accumulators, then one atomic per
+    // block and quantity (virial written to both symmetric slots)
+#pragma unroll
+    for (int v = 0; v < 8; ++v) acc[v] = warp_sum_ll(acc[v]);
+    __shared__ unsigned long long sh[8];
+    if (threadIdx.x < 8) sh[threadIdx.x] = 0ull;
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+            if (acc[v]) atomicAdd(&sh[v], static_cast<unsigned long long>(acc[v]));
+    __syncthreads();
+    if (threadIdx.x < 8 && sh[threadIdx.x]) {
+        long long* dst = LONG ? s.acc_long : s.acc_short;
+        const int G = wp.G, vb = 2 * G * G;
+        const int v = threadIdx.x;
+        const int idx0[8] = {wp.slot, G * G + wp.slot, vb + 0, vb + 1, vb + 2, vb + 4, vb + 5, vb + 8};
+        const int idx1[8] = {-1, -1, -1, vb + 3, vb + 6, -1, vb + 7, -1};
+        atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx0[v]), sh[v]);
+        if (idx1[v] >= 0) atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx1[v]), sh[v]);
+    }
+}
+
+template __global__ void k_water_force<true, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_force<true, true>(const SysDev*, const WaterParams);
+template __global__ void k_water_force<false, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_force<false, true>(const SysDev*, const WaterParams);
+
+}  // namespace gnb
