@@ -230,12 +230,13 @@ def run_gpu(args, rank, world, local_rank):
     ms_per_step = total_ms / args.steps
     # end to end through the public API: host positions in, host forces out
     pinned = torch.from_numpy(np.ascontiguousarray(s.pos)).pin_memory().numpy()
+    fout = torch.empty((s.topo.n_atoms, 3), dtype=torch.float64).pin_memory().numpy()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_pairs = 0
     for k in range(args.steps):
         rebuild = (evals_done % s.params.nsnb) == 0
-        ff.apply(pinned, count_pairs=False)
+        ff.apply(pinned, count_pairs=False, out=fout)
         evals_done += 1
         e2e_pairs += n_short + (n_long if rebuild else 0)
     torch.cuda.synchronize()

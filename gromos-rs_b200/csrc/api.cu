@@ -98,6 +98,11 @@ void NbSystem::release() {
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : ev) e = nullptr;
+    if (ev_err) cudaEventDestroy(ev_err);
+    ev_err = nullptr;
+    if (err_host) cudaFreeHost(err_host);
+    err_host = nullptr;
+    pending_check = false;
 }
 
 // (Re)allocates *p; a previous allocation made through alloc() is freed.
@@ -312,6 +317,24 @@ gr_status NbSystem::upload(const gr_topology* t) {
     h.pert_q = pq_d;
     h.pert_alpha = pa_d;
     h.pp = pp_d;
+    // solvent exclusions exactly the other atoms of the molecule and no 1-4
+    // pairs (Topology::solvate, topology.rs:1240-1262): then the energy-only
+    // solvent excluded terms are computed with the per-step water data
+    solvent_excl_intra = NSA < N;
+    for (int c = NSCG; c < NCG && solvent_excl_intra; ++c)
+        for (int a = h_cg_off[c]; a < h_cg_off[c + 1] && solvent_excl_intra; ++a) {
+            int k = h_excl_off[a];
+            for (int b = h_cg_off[c]; b < h_cg_off[c + 1]; ++b) {
+                if (b == a) continue;
+                if (k >= h_excl_off[a + 1] || h_excl[k] != b) {
+                    solvent_excl_intra = false;
+                    break;
+                }
+                ++k;
+            }
+            if (k != h_excl_off[a + 1] || h_o14_off[a + 1] != h_o14_off[a]) solvent_excl_intra = false;
+        }
+    h.excl_atoms = solvent_excl_intra ? NSA : N;
     // solvent parameter table from the first solvent molecule (innerloops.rs:241-255)
     h.water_lj00_only = 1;
     if (NSA < N) {
@@ -356,6 +379,11 @@ gr_status NbSystem::upload(const gr_topology* t) {
     GR_CUDA(cudaMemset(h.e64_long, 0, 16 * sizeof(double)));
     GR_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_sys), sizeof(SysDev)));
     for (auto& e : ev) GR_CUDA(cudaEventCreate(&e));
+    GR_CUDA(cudaEventCreateWithFlags(&ev_err, cudaEventDisableTiming));
+    if (!err_host) GR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&err_host), 4 * sizeof(int)));
+    err_host[0] = 0;
+    pending_check = false;
+    ever_built = false;
     // list capacities are sized at the first build (need the box)
     cells_alloc = 0;
     clus_alloc = 0;
@@ -449,6 +477,7 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.cell_start, size_t(n) + 1))) return st;
         if ((st = alloc(&h.cell_nsolute, size_t(n)))) return st;
         if ((st = alloc(&h.cell_nclus, size_t(n) + 1))) return st;
+        if ((st = alloc(&h.cell_part, size_t(n) + 1))) return st;
         cells_alloc = n;
     }
     int nsolv = NCG - NSCG;
@@ -548,8 +577,35 @@ gr_status NbSystem::check_errors(cudaStream_t s, bool* retry) {
     return GR_OK;
 }
 
+// Reads the overflow flags of the last asynchronous rebuild.  On overflow the
+// list capacities are grown and the next evaluation rebuilds; *overflowed
+// tells the caller that the evaluation based on that rebuild is invalid.
+gr_status NbSystem::resolve_pending(bool* overflowed) {
+    *overflowed = false;
+    if (!pending_check) return GR_OK;
+    GR_CUDA(cudaEventSynchronize(ev_err));
+    pending_check = false;
+    if (err_host[0] == 0) return GR_OK;
+    const int e = err_host[0];
+    GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
+    if (e & ERR_CELL_TOO_DENSE) {
+        set_error("pairlist: a grid cell holds more than 2048 charge groups");
+        return GR_ERR_UNSUPPORTED;
+    }
+    if (e & ERR_CG_TOO_LARGE) {
+        set_error("pairlist: solute charge group larger than 8 atoms");
+        return GR_ERR_UNSUPPORTED;
+    }
+    if (e & ERR_WLIST_OVERFLOW) wcap_want = std::max(wcap_want, wcap_alloc) * 2;
+    if (e & ERR_SLIST_OVERFLOW) scap_want = std::max(scap_want, scap_alloc) * 2;
+    if (e & ERR_PERT_OVERFLOW) pcap_want = std::max(pcap_want, pcap_alloc) * 2;
+    built = false;  // the next evaluation rebuilds with the grown capacities
+    *overflowed = true;
+    return GR_OK;
+}
+
 // PairlistAlgorithm::update (pairlist.rs:828-839) on the device.
-gr_status NbSystem::build_pairlist(cudaStream_t s) {
+gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
     if (!uploaded || !params_set || !box_set) {
         set_error("pairlist build before gr_system_upload / gr_set_params / gr_set_box");
         return GR_ERR_STATE;
@@ -567,13 +623,22 @@ gr_status NbSystem::build_pairlist(cudaStream_t s) {
         (++launches, k_cell_sort<<<h.n_cells, 1024, 0, s>>>(d_sys));
         (++launches, k_scan_clusters<<<1, 1024, 0, s>>>(d_sys));
         (++launches, k_cluster_setup<<<blocks_for(h.n_cells, 8), 256, 0, s>>>(d_sys));
-        if (NCG > NSCG) (++launches, k_cluster_search<4><<<blocks_for(h.max_clusters, 4), 128, 0, s>>>(d_sys));
+        if (NCG > NSCG)
+            (++launches, k_water_search<<<unsigned(h.max_clusters / kSearchWarps + h.n_cells + 1), kSearchWarps * 32, 0, s>>>(d_sys));
         if (NSCG > 0) (++launches, k_solute_search<<<blocks_for(NSCG, 4), 128, 0, s>>>(d_sys));
         if (n_pert > 0 && NSCG > 0) {
             GR_CUDA(cudaMemsetAsync(h.n_pert_pairs, 0, sizeof(int), s));
             (++launches, k_pert_pairs<<<blocks_for((long long)NSCG * h.scap, 256), 256, 0, s>>>(d_sys));
         }
         GR_CUDA(cudaGetLastError());
+        if (!sync) {
+            // overflow flags are read back asynchronously and resolved by the next
+            // call that synchronises (resolve_pending)
+            GR_CUDA(cudaMemcpyAsync(err_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+            GR_CUDA(cudaEventRecord(ev_err, s));
+            pending_check = true;
+            break;
+        }
         bool retry = false;
         if ((st = check_errors(s, &retry))) return st;
         if (!retry) break;
@@ -618,10 +683,15 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         return GR_ERR_STATE;
     }
     gr_status st;
+    bool overflowed = false;
+    if ((st = resolve_pending(&overflowed))) return st;
+    if (overflowed) lr_computed = false;
     bool rebuild = !built || steps_since_update >= prm.nsnb || (flags & GR_EVAL_FORCE_REBUILD);
     if (record_events) GR_CUDA(cudaEventRecord(ev[0], s));
     if (rebuild) {
-        if ((st = build_pairlist(s))) return st;
+        // the first build of a system synchronises to size the list capacities
+        if ((st = build_pairlist(s, !ever_built))) return st;
+        ever_built = true;
         if (prm.kernel == GR_KERNEL_PLAIN)
             if ((st = expand_cg_pairs(s))) return st;
     } else if ((st = push_descriptor(s))) {
@@ -680,7 +750,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     }
     if (record_events) GR_CUDA(cudaEventRecord(ev[3], s));
     const size_t sha = size_t(NA) * sizeof(unsigned long long);
-    (++launches, k_excluded_14<<<blocks_for(N, 128), 128, sha, s>>>(d_sys));
+    if (h.excl_atoms > 0) (++launches, k_excluded_14<<<blocks_for(h.excl_atoms, 128), 128, sha, s>>>(d_sys));
     if (n_pert > 0) {
         if (NSCG > 0) (++launches, k_pert_pairs_force<<<blocks_for(std::max(pcap_alloc, 1), 128), 128, sha, s>>>(d_sys));
         (++launches, k_pert_terms<<<blocks_for(std::max(N, h.n_pp), 128), 128, sha, s>>>(d_sys));
@@ -912,8 +982,9 @@ gr_status gr_pairlist_build(gr_ctx* ctx) {
         set_error("gr_pairlist_build before positions are set");
         return GR_ERR_STATE;
     }
-    gr_status st = ctx->sys.build_pairlist(ctx->stream);
+    gr_status st = ctx->sys.build_pairlist(ctx->stream, true);
     if (st) return st;
+    ctx->sys.ever_built = true;
     ctx->sys.pair_count_valid = false;
     return ctx->sys.expand_cg_pairs(ctx->stream);
 }
@@ -1038,18 +1109,30 @@ gr_status gr_pairlist_cg_pairs(gr_ctx* ctx, int32_t* out, int64_t* n_pairs) {
 gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out) {
     CTX_GUARD(ctx);
     NbSystem& S = ctx->sys;
-    gr_status st = S.eval(ctx->stream, flags, true);
-    if (st) return st;
-    if (S.last_rebuilt) S.pair_count_valid = false;
-    if (out && !(flags & GR_EVAL_NO_DOWNLOAD)) {
+    const bool download = out && !(flags & GR_EVAL_NO_DOWNLOAD);
+    gr_status st;
+    for (int attempt = 0;; ++attempt) {
+        const bool had_pending = S.pending_check;
+        st = S.eval(ctx->stream, flags, true);
+        if (st) return st;
+        if (!download) return GR_OK;  // overflow (if any) is reported by the next call
         if ((st = S.download(ctx->stream, out))) return st;
-        long long ns = 0, nl = 0;
-        if (out->n_pairs_short >= 0) {  // caller may pass -1 to skip the count
-            if ((st = S.pair_counts(ctx->stream, &ns, &nl))) return st;
+        bool overflowed = false;
+        if ((st = S.resolve_pending(&overflowed))) return st;
+        if (!overflowed) break;
+        if (attempt >= 8) {
+            set_error("pairlist: list capacity could not be grown far enough");
+            return GR_ERR_OVERFLOW;
         }
-        out->n_pairs_short = ns;
-        out->n_pairs_long = S.last_long ? nl : 0;
+        (void)had_pending;  // re-run this evaluation with the grown lists
     }
+    if (S.last_rebuilt) S.pair_count_valid = false;
+    long long ns = 0, nl = 0;
+    if (out->n_pairs_short >= 0) {  // caller may pass -1 to skip the count
+        if ((st = S.pair_counts(ctx->stream, &ns, &nl))) return st;
+    }
+    out->n_pairs_short = ns;
+    out->n_pairs_long = S.last_long ? nl : 0;
     return GR_OK;
 }
 

@@ -36,19 +36,45 @@ constexpr float kE = 16777216.0f;     // energy / virial fixed-point scale (2^24
 // ---------------------------------------------------------------------------
 __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
-    int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= s.n_clusters[0] * s.W) return;
-    int cg = s.slot_cg[slot];
-    if (cg < 0) return;
-    int a0 = s.cg_off[cg];
-    double x0 = s.pos[3 * a0], y0 = s.pos[3 * a0 + 1], z0 = s.pos[3 * a0 + 2];
-    s.wfirst[3 * slot] = x0;
-    s.wfirst[3 * slot + 1] = y0;
-    s.wfirst[3 * slot + 2] = z0;
-    for (int a = 0; a < s.aps; ++a) {
-        int at = a0 + a;
-        s.wdel[slot * s.aps + a] = make_float4(float(s.pos[3 * at] - x0), float(s.pos[3 * at + 1] - y0),
-                                               float(s.pos[3 * at + 2] - z0), 0.f);
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    double e_excl = 0.0;
+    if (slot < s.n_clusters[0] * s.W) {
+        const int cg = s.slot_cg[slot];
+        if (cg >= 0) {
+            const int a0 = s.cg_off[cg];
+            const double x0 = s.pos[3 * a0], y0 = s.pos[3 * a0 + 1], z0 = s.pos[3 * a0 + 2];
+            s.wfirst[3 * slot] = x0;
+            s.wfirst[3 * slot + 1] = y0;
+            s.wfirst[3 * slot + 2] = z0;
+            for (int a = 0; a < s.aps; ++a) {
+                const int at = a0 + a;
+                s.wdel[slot * s.aps + a] = make_float4(float(s.pos[3 * at] - x0), float(s.pos[3 * at + 1] - y0),
+                                                       float(s.pos[3 * at + 2] - z0), 0.f);
+            }
+            // solvent excluded pairs: energy only, -q_i q_j fpe crf_2cut3i r^2
+            // (rf_excluded_interactions, excluded.rs:81-96)
+            if (s.excl_atoms < s.n_atoms)
+                for (int a = 0; a < s.aps; ++a)
+                    for (int b = a + 1; b < s.aps; ++b) {
+                        const int i = a0 + a, j = a0 + b;
+                        double rx, ry, rz;
+                        nearest_image_exact(s, s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], s.pos[3 * j],
+                                            s.pos[3 * j + 1], s.pos[3 * j + 2], rx, ry, rz);
+                        e_excl += -s.charge[i] * s.charge[j] * s.fpe * s.crf_2cut3i * len2_exact(rx, ry, rz);
+                    }
+        }
+    }
+    if (s.excl_atoms < s.n_atoms) {
+        long long v = warp_sum_ll(to_fixed_d(e_excl, kEnergyScale));
+        __shared__ unsigned long long sh;
+        if (threadIdx.x == 0) sh = 0ull;
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh, static_cast<unsigned long long>(v));
+        __syncthreads();
+        if (threadIdx.x == 0 && sh) {
+            const int G = s.n_egroups, gs = s.solvent_group < 0 ? 0 : s.solvent_group;
+            atomicAdd(reinterpret_cast<unsigned long long*>(s.acc_short + G * G + gs * G + gs), sh);
+        }
     }
 }
 
@@ -332,7 +358,7 @@ __global__ void k_excluded_14(const SysDev* __restrict__ sys) {
     __syncthreads();
     const int vb = 2 * G * G;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < s.n_atoms) {
+    if (i < s.excl_atoms) {
         const double qi = s.charge[i];
         const double xi = s.pos[3 * i], yi = s.pos[3 * i + 1], zi = s.pos[3 * i + 2];
         const int gi = s.egroup[i];

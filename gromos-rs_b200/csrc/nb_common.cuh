@@ -25,6 +25,7 @@ constexpr int kMaxGroups = 16;        // energy groups
 constexpr double kForceScale = 4294967296.0;   // 2^32: force fixed point
 constexpr double kEnergyScale = 16777216.0;    // 2^24: energy / virial fixed point
 constexpr int kMaxCellCGs = 2048;     // bitonic per-cell sort capacity
+constexpr int kSearchWarps = 8;       // clusters (warps) per block of the water search
 
 // Error flags (bitwise OR into SysDev::err[0]).
 enum : int {
@@ -46,6 +47,8 @@ struct SysDev {
     int has_pert;
     int water_lj00_only; // solvent LJ only between site 0 and site 0
     int solvent_group;   // energy group of all solvent atoms (-1 = mixed)
+    int excl_atoms;      // atoms [0, excl_atoms) go through k_excluded_14; the
+                         // intra-molecular solvent exclusions are done in k_water_prep
     // ---- geometry (FP64, exact reference semantics)
     double box[3], inv_box[3];
     double c2s, c2l;     // (rcutp+skin)^2, (rcutl+skin)^2 (pairlist.rs:192-193)
@@ -90,6 +93,7 @@ struct SysDev {
     int* cell_start;           // n_cells+1
     int* cell_nsolute;         // n_cells
     int* cell_nclus;           // n_cells+1 (scanned in place -> cluster start)
+    int* cell_part;            // n_cells+1 (groups of 8 clusters per cell, scanned in place)
     int* sorted_cg;            // n_cg: sorted position -> CG
     int* cg_spos;              // n_cg: CG -> sorted position
     int* clus_cell;            // cluster -> cell

@@ -23,7 +23,8 @@ class NbSystem {
     gr_status upload(const gr_topology* t);
     gr_status set_params(const gr_nb_params* p);
     gr_status set_box(const double box[3]);
-    gr_status build_pairlist(cudaStream_t s);
+    gr_status build_pairlist(cudaStream_t s, bool sync);
+    gr_status resolve_pending(bool* overflowed);
     gr_status expand_cg_pairs(cudaStream_t s);
     gr_status eval(cudaStream_t s, int flags, bool record_events);
     gr_status download(cudaStream_t s, gr_result* out);
@@ -59,6 +60,10 @@ class NbSystem {
     int regrow_count = 0;
     size_t bytes = 0;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_err = nullptr;
+    int* err_host = nullptr;  // pinned copy of the device error flags
+    bool pending_check = false, ever_built = false;
+    bool solvent_excl_intra = false;  // solvent exclusions are exactly the molecule's other atoms
 
    private:
     template <class T>

@@ -14,7 +14,7 @@
 // Stages: k_refpos (reference positions, cell keys) -> k_scan_cells ->
 // k_scatter -> k_cell_sort (bitonic, per cell, deterministic) ->
 // k_scan_clusters -> k_cluster_setup (solvent i-clusters of W CGs) ->
-// k_cluster_search (water-water j-lists with W-bit masks) and
+// k_water_search (water-water j-lists with W-bit masks) and
 // k_solute_search (per solute CG j-lists with exclusion masks) ->
 // k_pert_pairs (explicit perturbed atom pairs for the FEP correction).
 #include "nb_common.cuh"
@@ -190,12 +190,15 @@ __global__ void k_cell_sort(const SysDev* __restrict__ sys) {
         s.cell_nsolute[cell] = nsol;
         int nsolv = n - nsol;
         s.cell_nclus[cell] = (nsolv + s.W - 1) / s.W;
+        s.cell_part[cell] = (s.cell_nclus[cell] + kSearchWarps - 1) / kSearchWarps;
     }
 }
 
 __global__ void k_scan_clusters(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
     __shared__ int total;
+    block_exclusive_scan(s.cell_part, s.cell_part, s.n_cells, nullptr);
+    __syncthreads();
     block_exclusive_scan(s.cell_nclus, s.cell_nclus, s.n_cells, &total);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -255,102 +258,203 @@ __device__ __forceinline__ int axis_offsets(int g, int* off) {
     return 1;
 }
 
-// Water-water search: one warp per solvent i-cluster.  Candidate j = solvent
-// CG in a neighbour cell; pair {i_k, j} belongs to this cluster iff j's sorted
-// position is after i_k's, so every unordered CG pair is listed once.  Bit k
-// of the short (long) mask is set when the exact reference test puts
-// (i_k, j) in the short (long) range; the solvent reference point is the
-// first atom for both CGs (pairlist.rs:359-368).
-template <int W>
-__global__ void k_cluster_search(const SysDev* __restrict__ sys) {
-    const SysDev& s = sys[blockIdx.y];
-    const int lane = threadIdx.x & 31;
-    const int ci = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (ci >= s.n_clusters[0]) return;
-    const int cell = s.clus_cell[ci], first = s.clus_first[ci], n = s.clus_n[ci];
-    double xi[W], yi[W], zi[W];
+// Water-water search, tiled by cell.  One block per group of up to
+// kSearchWarps clusters of one cell, one warp per cluster; the solvent CGs of
+// each neighbour cell are staged in shared memory in tiles of kTile and every
+// warp tests its cluster against the tile.  Pair {i_k, j} belongs to this
+// cluster iff j's sorted position is after i_k's, so every unordered CG pair
+// is listed once.  Bit k of the short (long) mask is set when the reference
+// test puts (i_k, j) in the short (long) range; the solvent reference point
+// is the first atom for both CGs (pairlist.rs:359-368).
+//
+// The test runs in FP32 on cluster-relative coordinates (FP64 differences
+// rounded once); a squared distance within a relative 1e-5 of either cutoff,
+// or a vector near half a box edge (image not certain in FP32), is decided by
+// the exact FP64 test (nearest_image_exact + len2_exact).  The FP32 error is
+// below 1e-6 relative, so the set is exactly the reference's.
+//
+// Each cluster's entries are collected in shared memory and written out
+// sorted by mask value, so warp chunks of the force kernel see similar masks.
+constexpr int kTile = 256;
+constexpr int kEntBuf = 640;
+
+__device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ buf, int nbuf,
+                                                   uint32_t* __restrict__ out, int lane) {
+    int off[16];
+    int hist[16];
 #pragma unroll
-    for (int k = 0; k < W; ++k) {
-        if (k < n) {
-            int a0 = s.cg_off[s.sorted_cg[first + k]];
-            xi[k] = s.pos[3 * a0];
-            yi[k] = s.pos[3 * a0 + 1];
-            zi[k] = s.pos[3 * a0 + 2];
-        } else {
-            xi[k] = yi[k] = zi[k] = 0.0;
+    for (int v = 0; v < 16; ++v) hist[v] = 0;
+    for (int c = 0; c < nbuf; c += 32) {
+        const int e = c + lane;
+        const unsigned m = e < nbuf ? (buf[e] & 0xfu) : 0u;
+#pragma unroll
+        for (int v = 1; v < 16; ++v) hist[v] += __popc(__ballot_sync(0xffffffffu, m == unsigned(v)));
+    }
+    off[0] = 0;
+#pragma unroll
+    for (int v = 1; v < 16; ++v) off[v] = off[v - 1] + hist[v - 1];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int c = 0; c < nbuf; c += 32) {
+        const int e = c + lane;
+        const uint32_t ent = e < nbuf ? buf[e] : 0u;
+        const unsigned m = ent & 0xfu;
+#pragma unroll
+        for (int v = 1; v < 16; ++v) {
+            const unsigned b = __ballot_sync(0xffffffffu, m == unsigned(v));
+            if (m == unsigned(v)) out[off[v] + __popc(b & lt)] = ent;
+            off[v] += __popc(b);
         }
     }
-    // bounding sphere around the first CG for the conservative FP32 prefilter
+}
+
+__global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev* __restrict__ sys) {
+    constexpr int W = 4;
+    const SysDev& s = sys[blockIdx.y];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b = blockIdx.x;
+    if (b >= s.cell_part[s.n_cells]) return;  // the whole block leaves together
+    int lo = 0, hi = s.n_cells - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s.cell_part[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int cell = lo;
+    const int ci = s.cell_nclus[cell] + (b - s.cell_part[cell]) * kSearchWarps + warp;
+    const bool active = ci < s.cell_nclus[cell + 1];
+
+    __shared__ double tx[kTile], ty[kTile], tz[kTile];
+    __shared__ uint32_t ebuf_s[kSearchWarps][kEntBuf], ebuf_l[kSearchWarps][kEntBuf];
+
+    int n = 0, first = 0;
+    double xi[W], yi[W], zi[W];
+    float ex[W], ey[W], ez[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) xi[k] = yi[k] = zi[k] = 0.0;
+    if (active) {
+        n = s.clus_n[ci];
+        first = s.clus_first[ci];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            if (k < n) {
+                const int cg = s.sorted_cg[first + k];
+                xi[k] = s.ref[3 * cg];
+                yi[k] = s.ref[3 * cg + 1];
+                zi[k] = s.ref[3 * cg + 2];
+            }
+    }
     float rad = 0.f;
 #pragma unroll
-    for (int k = 1; k < W; ++k)
-        if (k < n) {
-            float dx = float(xi[k] - xi[0]), dy = float(yi[k] - yi[0]), dz = float(zi[k] - zi[0]);
-            rad = fmaxf(rad, sqrtf(dx * dx + dy * dy + dz * dz));
-        }
+    for (int k = 0; k < W; ++k) {
+        ex[k] = float(xi[k] - xi[0]);
+        ey[k] = float(yi[k] - yi[0]);
+        ez[k] = float(zi[k] - zi[0]);
+        if (k < n) rad = fmaxf(rad, sqrtf(ex[k] * ex[k] + ey[k] * ey[k] + ez[k] * ez[k]));
+    }
     const float reach = sqrtf(float(s.c2l)) + rad + 1e-3f;
     const float reach2 = reach * reach;
-    int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
-    int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
+    const float c2s = float(s.c2s), c2l = float(s.c2l);
+    const float s_lo = c2s * (1.f - 1e-5f), s_hi = c2s * (1.f + 1e-5f);
+    const float l_lo = c2l * (1.f - 1e-5f), l_hi = c2l * (1.f + 1e-5f);
+    const float limx = s.boundary ? s.half_boxf[0] - 1e-4f : 3e38f;
+    const float limy = s.boundary ? s.half_boxf[1] - 1e-4f : 3e38f;
+    const float limz = s.boundary ? s.half_boxf[2] - 1e-4f : 3e38f;
+    const int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
+    const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
     int ox[3], oy[3], oz[3];
-    int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
-    uint32_t* outs = s.wl_s + static_cast<size_t>(ci) * s.wcap;
-    uint32_t* outl = s.wl_l + static_cast<size_t>(ci) * s.wcap;
+    const int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
+    uint32_t* outs = s.wl_s + static_cast<size_t>(active ? ci : 0) * s.wcap;
+    uint32_t* outl = s.wl_l + static_cast<size_t>(active ? ci : 0) * s.wcap;
     int cnt_s = 0, cnt_l = 0;
+    const unsigned below = (1u << lane) - 1u;
     for (int iz = 0; iz < nz; ++iz)
         for (int iy = 0; iy < ny; ++iy)
             for (int ix = 0; ix < nx; ++ix) {
-                int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
-                if (nc < cell) continue;
-                int j0 = s.cell_start[nc] + s.cell_nsolute[nc], j1 = s.cell_start[nc + 1];
-                if (nc == cell) j0 = max(j0, first + 1);
-                for (int base = j0; base < j1; base += 32) {
-                    int sp = base + lane;
-                    unsigned ms = 0, ml = 0;
-                    int slot = 0;
-                    if (sp < j1) {
-                        int cgj = s.sorted_cg[sp];
-                        slot = s.cg_slot[cgj];
-                        int a0 = s.cg_off[cgj];
-                        double xj = s.pos[3 * a0], yj = s.pos[3 * a0 + 1], zj = s.pos[3 * a0 + 2];
-                        float dx = float(xi[0] - xj), dy = float(yi[0] - yj), dz = float(zi[0] - zj);
-                        if (s.boundary == 1) {
-                            dx -= s.boxf[0] * rintf(dx * s.inv_boxf[0]);
-                            dy -= s.boxf[1] * rintf(dy * s.inv_boxf[1]);
-                            dz -= s.boxf[2] * rintf(dz * s.inv_boxf[2]);
-                        }
-                        if (dx * dx + dy * dy + dz * dz <= reach2) {
+                const int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
+                if (nc < cell) continue;  // uniform over the block
+                const int j0 = s.cell_start[nc] + s.cell_nsolute[nc], j1 = s.cell_start[nc + 1];
+                const int slot0 = s.cell_nclus[nc] * W;
+                for (int t0 = j0; t0 < j1; t0 += kTile) {
+                    const int tn = min(kTile, j1 - t0);
+                    __syncthreads();
+                    for (int t = threadIdx.x; t < tn; t += blockDim.x) {
+                        const int cg = s.sorted_cg[t0 + t];
+                        tx[t] = s.ref[3 * cg];
+                        ty[t] = s.ref[3 * cg + 1];
+                        tz[t] = s.ref[3 * cg + 2];
+                    }
+                    __syncthreads();
+                    if (!active) continue;
+                    for (int base = 0; base < tn; base += 32) {
+                        const int t = base + lane;
+                        const int sp = t0 + t;
+                        unsigned ms = 0, ml = 0;
+                        if (t < tn && sp > first) {
+                            double dx = xi[0] - tx[t], dy = yi[0] - ty[t], dz = zi[0] - tz[t];
+                            if (s.boundary) {
+                                dx -= s.box[0] * rint(dx * s.inv_box[0]);
+                                dy -= s.box[1] * rint(dy * s.inv_box[1]);
+                                dz -= s.box[2] * rint(dz * s.inv_box[2]);
+                            }
+                            const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
+                            if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
 #pragma unroll
-                            for (int k = 0; k < W; ++k) {
-                                if (k < n && sp > first + k) {
-                                    double rx, ry, rz;
-                                    nearest_image_exact(s, xi[k], yi[k], zi[k], xj, yj, zj, rx, ry, rz);
-                                    double d2 = len2_exact(rx, ry, rz);
-                                    if (!(d2 > s.c2l)) {
-                                        if (d2 > s.c2s)
-                                            ml |= 1u << k;
-                                        else
-                                            ms |= 1u << k;
+                                for (int k = 0; k < W; ++k) {
+                                    if (k >= n || sp <= first + k) continue;
+                                    const float kx = ex[k] + Dx, ky = ey[k] + Dy, kz = ez[k] + Dz;
+                                    const float d2 = kx * kx + ky * ky + kz * kz;
+                                    int cls;  // 0 none, 1 short, 2 long, 3 undecided
+                                    if (!(fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz))
+                                        cls = 3;
+                                    else if (d2 > l_hi)
+                                        cls = 0;
+                                    else if (d2 < s_lo)
+                                        cls = 1;
+                                    else if (d2 > s_hi && d2 < l_lo)
+                                        cls = 2;
+                                    else
+                                        cls = 3;
+                                    if (cls == 3) {
+                                        double rx, ry, rz;
+                                        nearest_image_exact(s, xi[k], yi[k], zi[k], tx[t], ty[t], tz[t], rx, ry, rz);
+                                        const double e2 = len2_exact(rx, ry, rz);
+                                        cls = e2 > s.c2l ? 0 : (e2 > s.c2s ? 2 : 1);
                                     }
+                                    if (cls == 1) ms |= 1u << k;
+                                    if (cls == 2) ml |= 1u << k;
                                 }
                             }
                         }
+                        const uint32_t slot = static_cast<uint32_t>(slot0 + (sp - j0));
+                        const unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
+                        const unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
+                        if (ms) {
+                            const int p = cnt_s + __popc(bs & below);
+                            const uint32_t ent = (slot << 8) | ms;
+                            if (p < kEntBuf)
+                                ebuf_s[warp][p] = ent;
+                            else if (p < s.wcap)
+                                outs[p] = ent;
+                        }
+                        if (ml) {
+                            const int p = cnt_l + __popc(bl & below);
+                            const uint32_t ent = (slot << 8) | ml;
+                            if (p < kEntBuf)
+                                ebuf_l[warp][p] = ent;
+                            else if (p < s.wcap)
+                                outl[p] = ent;
+                        }
+                        cnt_s += __popc(bs);
+                        cnt_l += __popc(bl);
                     }
-                    unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
-                    unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
-                    unsigned below = (1u << lane) - 1u;
-                    if (ms) {
-                        int p = cnt_s + __popc(bs & below);
-                        if (p < s.wcap) outs[p] = (static_cast<uint32_t>(slot) << 8) | ms;
-                    }
-                    if (ml) {
-                        int p = cnt_l + __popc(bl & below);
-                        if (p < s.wcap) outl[p] = (static_cast<uint32_t>(slot) << 8) | ml;
-                    }
-                    cnt_s += __popc(bs);
-                    cnt_l += __popc(bl);
                 }
             }
+    if (!active) return;
+    __syncwarp();
+    sort_write_entries(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
+    sort_write_entries(ebuf_l[warp], min(cnt_l, kEntBuf), outl, lane);
     if (lane == 0) {
         if (cnt_s > s.wcap || cnt_l > s.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
         s.wn_s[ci] = min(cnt_s, s.wcap);
@@ -546,6 +650,4 @@ __global__ void k_expand_cgpairs(const SysDev* __restrict__ sys, int long_range)
 }  // namespace gnb
 
 namespace gnb {
-template __global__ void k_cluster_search<4>(const SysDev*);
-template __global__ void k_cluster_search<8>(const SysDev*);
 }  // namespace gnb

@@ -151,11 +151,18 @@ class Forcefield:
 
     # ---- evaluation
     def apply(self, pos=None, virial: bool = True, force_rebuild: bool = False, count_pairs: bool = True,
-              download_forces: bool = True) -> Dict:
+              download_forces: bool = True, out: Optional[np.ndarray] = None) -> Dict:
+        """One Forcefield::apply.  ``out`` (n_atoms, 3) float64, ideally in
+        pinned memory, receives the forces without a per-call allocation."""
         if pos is not None:
             self.upload_positions(pos)
         flags = (_lib.GR_EVAL_VIRIAL if virial else 0) | (_lib.GR_EVAL_FORCE_REBUILD if force_rebuild else 0)
-        f = np.zeros((self.n_atoms, 3)) if download_forces else None
+        if out is not None:
+            if out.shape != (self.n_atoms, 3) or out.dtype != np.float64 or not out.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous float64 (n_atoms, 3) array")
+            f = out
+        else:
+            f = np.zeros((self.n_atoms, 3)) if download_forces else None
         glj = np.zeros((self.G, self.G))
         gcrf = np.zeros((self.G, self.G))
         r = _lib.GrResult()
