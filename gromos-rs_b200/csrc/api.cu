@@ -354,6 +354,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&d_cg_key, size_t(NCG)))) return st;
     if ((st = alloc(&h.cg_cell, size_t(NCG)))) return st;
     if ((st = alloc(&h.sorted_cg, size_t(NCG)))) return st;
+    if ((st = alloc(&h.sref, 3 * (size_t(NCG) + 2)))) return st;
     if ((st = alloc(&h.cg_spos, size_t(NCG)))) return st;
     if ((st = alloc(&h.cg_slot, size_t(NCG)))) return st;
     if ((st = alloc(&h.n_clusters, 1))) return st;
@@ -734,6 +735,8 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             lr_computed = true;
         }
     } else {
+        if (NCG > NSCG)  // per-step water data incl. the solvent excluded energies
+            (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
         (++launches, k_pos32<<<blocks_for(N, 256), 256, 0, s>>>(d_sys));
         GR_CUDA(cudaMemsetAsync(h.f32, 0, size_t(N) * 3 * sizeof(float), s));
         GR_CUDA(cudaMemsetAsync(h.e64, 0, 16 * sizeof(double), s));

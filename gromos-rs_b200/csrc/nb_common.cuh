@@ -95,6 +95,7 @@ struct SysDev {
     int* cell_nclus;           // n_cells+1 (scanned in place -> cluster start)
     int* cell_part;            // n_cells+1 (groups of 8 clusters per cell, scanned in place)
     int* sorted_cg;            // n_cg: sorted position -> CG
+    double* sref;              // [3][n_cg + 2] sorted reference positions (x, y, z planes)
     int* cg_spos;              // n_cg: CG -> sorted position
     int* clus_cell;            // cluster -> cell
     int* clus_first;           // cluster -> first sorted position

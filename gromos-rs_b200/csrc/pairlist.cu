@@ -182,6 +182,10 @@ __global__ void k_cell_sort(const SysDev* __restrict__ sys) {
         s.keys[start + i] = key;
         s.sorted_cg[start + i] = cg;
         s.cg_spos[cg] = start + i;
+        const int stride = s.n_cg + 2;
+        s.sref[start + i] = s.ref[3 * cg];
+        s.sref[stride + start + i] = s.ref[3 * cg + 1];
+        s.sref[2 * stride + start + i] = s.ref[3 * cg + 2];
         if (((key >> 41) & 1ull) == 0ull) ++local;
     }
     atomicAdd(&nsol, local);
@@ -369,88 +373,140 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
     uint32_t* outl = s.wl_l + static_cast<size_t>(active ? ci : 0) * s.wcap;
     int cnt_s = 0, cnt_l = 0;
     const unsigned below = (1u << lane) - 1u;
-    for (int iz = 0; iz < nz; ++iz)
-        for (int iy = 0; iy < ny; ++iy)
-            for (int ix = 0; ix < nx; ++ix) {
-                const int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
-                if (nc < cell) continue;  // uniform over the block
-                const int j0 = s.cell_start[nc] + s.cell_nsolute[nc], j1 = s.cell_start[nc + 1];
-                const int slot0 = s.cell_nclus[nc] * W;
-                for (int t0 = j0; t0 < j1; t0 += kTile) {
-                    const int tn = min(kTile, j1 - t0);
-                    __syncthreads();
-                    for (int t = threadIdx.x; t < tn; t += blockDim.x) {
-                        const int cg = s.sorted_cg[t0 + t];
-                        tx[t] = s.ref[3 * cg];
-                        ty[t] = s.ref[3 * cg + 1];
-                        tz[t] = s.ref[3 * cg + 2];
+    // neighbour cells at or after this one (block-uniform), then the tiles of
+    // their solvent CGs; the next tile is prefetched into registers while the
+    // current one is processed
+    __shared__ int ncell[27];
+    __shared__ int n_nc;
+    if (threadIdx.x == 0) {
+        int m = 0;
+        for (int iz = 0; iz < nz; ++iz)
+            for (int iy = 0; iy < ny; ++iy)
+                for (int ix = 0; ix < nx; ++ix) {
+                    const int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
+                    if (nc >= cell) ncell[m++] = nc;
+                }
+        n_nc = m;
+    }
+    __syncthreads();
+    const int stride = s.n_cg + 2;
+    int ic = 0, t0 = 0;  // current tile: neighbour index ic, offset t0 into its solvent range
+    auto tile_range = [&](int icc, int& j0, int& j1) {
+        const int nc = ncell[icc];
+        j0 = s.cell_start[nc] + s.cell_nsolute[nc];
+        j1 = s.cell_start[nc + 1];
+    };
+    // skip empty neighbour ranges
+    int j0 = 0, j1 = 0;
+    while (ic < n_nc) {
+        tile_range(ic, j0, j1);
+        if (j1 > j0) break;
+        ++ic;
+    }
+    double px = 0, py = 0, pz = 0;
+    if (ic < n_nc && threadIdx.x < min(kTile, j1 - j0)) {
+        px = s.sref[j0 + threadIdx.x];
+        py = s.sref[stride + j0 + threadIdx.x];
+        pz = s.sref[2 * stride + j0 + threadIdx.x];
+    }
+    while (ic < n_nc) {
+        const int nc = ncell[ic];
+        const int tbeg = j0 + t0;
+        const int tn = min(kTile, j1 - tbeg);
+        const int slot0 = s.cell_nclus[nc] * W;
+        __syncthreads();
+        if (threadIdx.x < tn) {
+            tx[threadIdx.x] = px;
+            ty[threadIdx.x] = py;
+            tz[threadIdx.x] = pz;
+        }
+        __syncthreads();
+        // advance to the next tile and prefetch it
+        int nic = ic, nt0 = t0 + kTile, nj0 = j0, nj1 = j1;
+        if (nj0 + nt0 >= nj1) {
+            nt0 = 0;
+            ++nic;
+            while (nic < n_nc) {
+                tile_range(nic, nj0, nj1);
+                if (nj1 > nj0) break;
+                ++nic;
+            }
+        }
+        if (nic < n_nc && threadIdx.x < min(kTile, nj1 - (nj0 + nt0))) {
+            const int q = nj0 + nt0 + threadIdx.x;
+            px = s.sref[q];
+            py = s.sref[stride + q];
+            pz = s.sref[2 * stride + q];
+        }
+        if (active) {
+            for (int base = 0; base < tn; base += 32) {
+                const int t = base + lane;
+                const int sp = tbeg + t;
+                unsigned ms = 0, ml = 0;
+                if (t < tn && sp > first) {
+                    double dx = xi[0] - tx[t], dy = yi[0] - ty[t], dz = zi[0] - tz[t];
+                    if (s.boundary) {
+                        dx -= s.box[0] * rint(dx * s.inv_box[0]);
+                        dy -= s.box[1] * rint(dy * s.inv_box[1]);
+                        dz -= s.box[2] * rint(dz * s.inv_box[2]);
                     }
-                    __syncthreads();
-                    if (!active) continue;
-                    for (int base = 0; base < tn; base += 32) {
-                        const int t = base + lane;
-                        const int sp = t0 + t;
-                        unsigned ms = 0, ml = 0;
-                        if (t < tn && sp > first) {
-                            double dx = xi[0] - tx[t], dy = yi[0] - ty[t], dz = zi[0] - tz[t];
-                            if (s.boundary) {
-                                dx -= s.box[0] * rint(dx * s.inv_box[0]);
-                                dy -= s.box[1] * rint(dy * s.inv_box[1]);
-                                dz -= s.box[2] * rint(dz * s.inv_box[2]);
-                            }
-                            const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
-                            if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
+                    const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
+                    if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
 #pragma unroll
-                                for (int k = 0; k < W; ++k) {
-                                    if (k >= n || sp <= first + k) continue;
-                                    const float kx = ex[k] + Dx, ky = ey[k] + Dy, kz = ez[k] + Dz;
-                                    const float d2 = kx * kx + ky * ky + kz * kz;
-                                    int cls;  // 0 none, 1 short, 2 long, 3 undecided
-                                    if (!(fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz))
-                                        cls = 3;
-                                    else if (d2 > l_hi)
-                                        cls = 0;
-                                    else if (d2 < s_lo)
-                                        cls = 1;
-                                    else if (d2 > s_hi && d2 < l_lo)
-                                        cls = 2;
-                                    else
-                                        cls = 3;
-                                    if (cls == 3) {
-                                        double rx, ry, rz;
-                                        nearest_image_exact(s, xi[k], yi[k], zi[k], tx[t], ty[t], tz[t], rx, ry, rz);
-                                        const double e2 = len2_exact(rx, ry, rz);
-                                        cls = e2 > s.c2l ? 0 : (e2 > s.c2s ? 2 : 1);
-                                    }
-                                    if (cls == 1) ms |= 1u << k;
-                                    if (cls == 2) ml |= 1u << k;
-                                }
+                        for (int k = 0; k < W; ++k) {
+                            if (k >= n || sp <= first + k) continue;
+                            const float kx = ex[k] + Dx, ky = ey[k] + Dy, kz = ez[k] + Dz;
+                            const float d2 = kx * kx + ky * ky + kz * kz;
+                            int cls;  // 0 none, 1 short, 2 long, 3 undecided
+                            if (!(fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz))
+                                cls = 3;
+                            else if (d2 > l_hi)
+                                cls = 0;
+                            else if (d2 < s_lo)
+                                cls = 1;
+                            else if (d2 > s_hi && d2 < l_lo)
+                                cls = 2;
+                            else
+                                cls = 3;
+                            if (cls == 3) {
+                                double rx, ry, rz;
+                                nearest_image_exact(s, xi[k], yi[k], zi[k], tx[t], ty[t], tz[t], rx, ry, rz);
+                                const double e2 = len2_exact(rx, ry, rz);
+                                cls = e2 > s.c2l ? 0 : (e2 > s.c2s ? 2 : 1);
                             }
+                            if (cls == 1) ms |= 1u << k;
+                            if (cls == 2) ml |= 1u << k;
                         }
-                        const uint32_t slot = static_cast<uint32_t>(slot0 + (sp - j0));
-                        const unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
-                        const unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
-                        if (ms) {
-                            const int p = cnt_s + __popc(bs & below);
-                            const uint32_t ent = (slot << 8) | ms;
-                            if (p < kEntBuf)
-                                ebuf_s[warp][p] = ent;
-                            else if (p < s.wcap)
-                                outs[p] = ent;
-                        }
-                        if (ml) {
-                            const int p = cnt_l + __popc(bl & below);
-                            const uint32_t ent = (slot << 8) | ml;
-                            if (p < kEntBuf)
-                                ebuf_l[warp][p] = ent;
-                            else if (p < s.wcap)
-                                outl[p] = ent;
-                        }
-                        cnt_s += __popc(bs);
-                        cnt_l += __popc(bl);
                     }
                 }
+                const uint32_t slot = static_cast<uint32_t>(slot0 + (sp - j0));
+                const unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
+                const unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
+                if (ms) {
+                    const int p = cnt_s + __popc(bs & below);
+                    const uint32_t ent = (slot << 8) | ms;
+                    if (p < kEntBuf)
+                        ebuf_s[warp][p] = ent;
+                    else if (p < s.wcap)
+                        outs[p] = ent;
+                }
+                if (ml) {
+                    const int p = cnt_l + __popc(bl & below);
+                    const uint32_t ent = (slot << 8) | ml;
+                    if (p < kEntBuf)
+                        ebuf_l[warp][p] = ent;
+                    else if (p < s.wcap)
+                        outl[p] = ent;
+                }
+                cnt_s += __popc(bs);
+                cnt_l += __popc(bl);
             }
+        }
+        ic = nic;
+        t0 = nt0;
+        j0 = nj0;
+        j1 = nj1;
+    }
     if (!active) return;
     __syncwarp();
     sort_write_entries(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
