@@ -490,8 +490,10 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.slot_cg, size_t(maxc) * W))) return st;
         if ((st = alloc(&h.wn_s, size_t(maxc)))) return st;
         if ((st = alloc(&h.wn_l, size_t(maxc)))) return st;
-        if ((st = alloc(&h.wfirst, size_t(maxc) * W * 3))) return st;
-        if ((st = alloc(&h.wdel, size_t(maxc) * W * aps))) return st;
+        if ((st = alloc(&h.wrec, size_t(maxc) * W))) return st;
+        if ((st = alloc(&h.fs_short, size_t(maxc) * W * 9))) return st;
+        if ((st = alloc(&h.fs_long, size_t(maxc) * W * 9))) return st;
+        fs_long_zeroed = false;
         clus_alloc = maxc;
         wcap_alloc = 0;  // lists must be re-sized with the cluster count
     }
@@ -704,6 +706,12 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     const int NA = acc_size(G);
     GR_CUDA(cudaMemsetAsync(h.f_short, 0, size_t(N) * 3 * sizeof(long long), s));
     GR_CUDA(cudaMemsetAsync(h.acc_short, 0, size_t(NA) * sizeof(long long), s));
+    if (NCG > NSCG) GR_CUDA(cudaMemsetAsync(h.fs_short, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
+    if (NCG > NSCG && !fs_long_zeroed) {
+        // the slot layout changes at rebuilds; keep the long cache consistent
+        GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
+        fs_long_zeroed = true;
+    }
     bool do_long = h.twin && (rebuild || !lr_computed);
     const int sm = sm_count();
     const size_t shg = size_t(2 * G * G) * sizeof(unsigned long long);
@@ -723,6 +731,8 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         if (do_long) {
             GR_CUDA(cudaMemsetAsync(h.f_long, 0, size_t(N) * 3 * sizeof(long long), s));
             GR_CUDA(cudaMemsetAsync(h.acc_long, 0, size_t(NA) * sizeof(long long), s));
+            if (NCG > NSCG)
+                GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
             if (NCG > NSCG) {
                 WaterParams wpl = water_params(true);
                 unsigned grid = unsigned(sm * water_blocks_per_sm);

@@ -43,14 +43,17 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
         if (cg >= 0) {
             const int a0 = s.cg_off[cg];
             const double x0 = s.pos[3 * a0], y0 = s.pos[3 * a0 + 1], z0 = s.pos[3 * a0 + 2];
-            s.wfirst[3 * slot] = x0;
-            s.wfirst[3 * slot + 1] = y0;
-            s.wfirst[3 * slot + 2] = z0;
-            for (int a = 0; a < s.aps; ++a) {
-                const int at = a0 + a;
-                s.wdel[slot * s.aps + a] = make_float4(float(s.pos[3 * at] - x0), float(s.pos[3 * at + 1] - y0),
-                                                       float(s.pos[3 * at + 2] - z0), 0.f);
-            }
+            WaterRec w;
+            w.x0 = x0;
+            w.y0 = y0;
+            w.z0 = z0;
+            w.h1x = float(s.pos[3 * a0 + 3] - x0);
+            w.h1y = float(s.pos[3 * a0 + 4] - y0);
+            w.h1z = float(s.pos[3 * a0 + 5] - z0);
+            w.h2x = float(s.pos[3 * a0 + 6] - x0);
+            w.h2y = float(s.pos[3 * a0 + 7] - y0);
+            w.h2z = float(s.pos[3 * a0 + 8] - z0);
+            s.wrec[slot] = w;
             // solvent excluded pairs: energy only, -q_i q_j fpe crf_2cut3i r^2
             // (rf_excluded_interactions, excluded.rs:81-96)
             if (s.excl_atoms < s.n_atoms)
@@ -677,8 +680,18 @@ __global__ void k_finalize(const SysDev* __restrict__ sys, int plain) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double inv = 1.0 / kForceScale;
     if (i < 3 * s.n_atoms) {
-        double v = double(s.f_short[i]) * inv;
-        if (s.twin) v += double(s.f_long[i]) * inv;
+        long long fx = s.f_short[i];
+        if (s.twin) fx += s.f_long[i];
+        const int a = i / 3;
+        if (a >= s.n_solute_atoms && s.wrec != nullptr && !plain) {
+            // water atoms: forces accumulated per cluster slot
+            const int cg = s.atom_cg[a];
+            const int slot = s.cg_slot[cg];
+            const int k = (a - s.cg_off[cg]) * 3 + (i - 3 * a);
+            fx += s.fs_short[slot * 9 + k];
+            if (s.twin) fx += s.fs_long[slot * 9 + k];
+        }
+        double v = double(fx) * inv;
         if (plain) {
             v += double(s.f32[i]);
             if (s.twin) v += double(s.f32_long[i]);

@@ -37,6 +37,15 @@ enum : int {
     ERR_CGPAIR_OVERFLOW = 32,
 };
 
+// One water per slot, 48 bytes, read with three 16-byte loads: the FP64
+// position of the first atom and the FP32 offsets of atoms 1 and 2 from it.
+struct __align__(16) WaterRec {
+    double x0, y0;
+    double z0;
+    float h1x, h1y;
+    float h1z, h2x, h2y, h2z;
+};
+
 struct SysDev {
     // ---- sizes and flags
     int n_atoms, n_cg, n_solute_cg, n_solute_atoms, aps, n_types, n_egroups;
@@ -117,8 +126,9 @@ struct SysDev {
     int* n_pert_pairs;         // [1]
     int pcap;
     // ---- per-step water data in slot order
-    double* wfirst;            // [max_clusters*W*3] FP64 first-atom position
-    float4* wdel;              // [max_clusters*W*aps] FP32 offset from first atom
+    struct WaterRec* wrec;     // [max_clusters*W] per-slot FP64 first atom + FP32 offsets
+    long long* fs_short;       // [max_clusters*W*9] water forces per slot (fixed 2^32)
+    long long* fs_long;        // same, long-range cache
     // ---- plain-kernel data
     float4* pos32;             // n_atoms (x, y, z, q)
     int* cgp;                  // [cgp_cap*3] explicit CG pairs (i_cg, j_cg, long)

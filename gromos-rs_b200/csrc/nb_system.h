@@ -63,7 +63,8 @@ class NbSystem {
     cudaEvent_t ev_err = nullptr;
     int* err_host = nullptr;  // pinned copy of the device error flags
     bool pending_check = false, ever_built = false;
-    bool solvent_excl_intra = false;  // solvent exclusions are exactly the molecule's other atoms
+    bool solvent_excl_intra = false;
+    bool fs_long_zeroed = false;  // solvent exclusions are exactly the molecule's other atoms
 
    private:
     template <class T>

@@ -271,8 +271,11 @@ __device__ __forceinline__ int axis_offsets(int g, int* off) {
 // test puts (i_k, j) in the short (long) range; the solvent reference point
 // is the first atom for both CGs (pairlist.rs:359-368).
 //
-// The test runs in FP32 on cluster-relative coordinates (FP64 differences
-// rounded once); a squared distance within a relative 1e-5 of either cutoff,
+// Candidates are staged with FP64 positions and FP32 min-image offsets from
+// the centre of their chunk of 32; a warp skips a chunk whose bounding sphere
+// is out of reach of its cluster.  The test runs in FP32 on
+// cluster-to-chunk vectors (FP64 image, rounded once) minus the offsets; a
+// squared distance within a relative 1e-5 of either cutoff,
 // or a vector near half a box edge (image not certain in FP32), is decided by
 // the exact FP64 test (nearest_image_exact + len2_exact).  The FP32 error is
 // below 1e-6 relative, so the set is exactly the reference's.
@@ -280,7 +283,7 @@ __device__ __forceinline__ int axis_offsets(int g, int* off) {
 // Each cluster's entries are collected in shared memory and written out
 // sorted by mask value, so warp chunks of the force kernel see similar masks.
 constexpr int kTile = 256;
-constexpr int kEntBuf = 640;
+constexpr int kEntBuf = 512;
 
 __device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ buf, int nbuf,
                                                    uint32_t* __restrict__ out, int lane) {
@@ -330,6 +333,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
     const bool active = ci < s.cell_nclus[cell + 1];
 
     __shared__ double tx[kTile], ty[kTile], tz[kTile];
+    __shared__ float fx[kTile], fy[kTile], fz[kTile];       // offsets from the chunk centre (min image)
+    __shared__ double chx[kTile / 32], chy[kTile / 32], chz[kTile / 32];  // chunk centres
+    __shared__ float chr[kTile / 32];                        // chunk radii
     __shared__ uint32_t ebuf_s[kSearchWarps][kEntBuf], ebuf_l[kSearchWarps][kEntBuf];
 
     int n = 0, first = 0;
@@ -420,6 +426,37 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
             ty[threadIdx.x] = py;
             tz[threadIdx.x] = pz;
         }
+        // chunk of 32 candidates per warp: centre = first member, FP32 min-image
+        // offsets of the members, radius = largest offset
+        {
+            const int cbeg = warp * 32;
+            if (cbeg < tn) {
+                const double cx0 = __shfl_sync(0xffffffffu, px, 0);
+                const double cy0 = __shfl_sync(0xffffffffu, py, 0);
+                const double cz0 = __shfl_sync(0xffffffffu, pz, 0);
+                float r = 0.f;
+                if (threadIdx.x < tn) {
+                    double dx = px - cx0, dy = py - cy0, dz = pz - cz0;
+                    if (s.boundary) {
+                        dx -= s.box[0] * rint(dx * s.inv_box[0]);
+                        dy -= s.box[1] * rint(dy * s.inv_box[1]);
+                        dz -= s.box[2] * rint(dz * s.inv_box[2]);
+                    }
+                    fx[threadIdx.x] = float(dx);
+                    fy[threadIdx.x] = float(dy);
+                    fz[threadIdx.x] = float(dz);
+                    r = sqrtf(float(dx) * float(dx) + float(dy) * float(dy) + float(dz) * float(dz));
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
+                if (lane == 0) {
+                    chx[warp] = cx0;
+                    chy[warp] = cy0;
+                    chz[warp] = cz0;
+                    chr[warp] = r * (1.f + 1e-5f) + 1e-5f;
+                }
+            }
+        }
         __syncthreads();
         // advance to the next tile and prefetch it
         int nic = ic, nt0 = t0 + kTile, nj0 = j0, nj1 = j1;
@@ -440,17 +477,23 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
         }
         if (active) {
             for (int base = 0; base < tn; base += 32) {
+                // cluster-to-chunk vector (FP64 image once per chunk); skip
+                // chunks entirely out of reach (warp-uniform)
+                const int ch = base >> 5;
+                double cdx = xi[0] - chx[ch], cdy = yi[0] - chy[ch], cdz = zi[0] - chz[ch];
+                if (s.boundary) {
+                    cdx -= s.box[0] * rint(cdx * s.inv_box[0]);
+                    cdy -= s.box[1] * rint(cdy * s.inv_box[1]);
+                    cdz -= s.box[2] * rint(cdz * s.inv_box[2]);
+                }
+                const float Cx = float(cdx), Cy = float(cdy), Cz = float(cdz);
+                const float cd = sqrtf(Cx * Cx + Cy * Cy + Cz * Cz);
+                if (cd - chr[ch] > reach) continue;
                 const int t = base + lane;
                 const int sp = tbeg + t;
                 unsigned ms = 0, ml = 0;
                 if (t < tn && sp > first) {
-                    double dx = xi[0] - tx[t], dy = yi[0] - ty[t], dz = zi[0] - tz[t];
-                    if (s.boundary) {
-                        dx -= s.box[0] * rint(dx * s.inv_box[0]);
-                        dy -= s.box[1] * rint(dy * s.inv_box[1]);
-                        dz -= s.box[2] * rint(dz * s.inv_box[2]);
-                    }
-                    const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
+                    const float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
                     if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
 #pragma unroll
                         for (int k = 0; k < W; ++k) {

@@ -139,11 +139,10 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     const int nclus = s.n_clusters[0];
-    long long* __restrict__ F = LONG ? s.f_long : s.f_short;
+    long long* __restrict__ FS = LONG ? s.fs_long : s.fs_short;  // per slot: 3 atoms x 3 components
     const uint32_t* __restrict__ wl = LONG ? s.wl_l : s.wl_s;
     const int* __restrict__ wn = LONG ? s.wn_l : s.wn_s;
-    const double* __restrict__ wfirst = s.wfirst;
-    const float4* __restrict__ wdel = s.wdel;
+    const float4* __restrict__ wrec4 = reinterpret_cast<const float4*>(s.wrec);
     // per-lane fixed-point (2^24) accumulators of lj, crf, xx, xy, xz, yy, yz, zz:
     // kept in shared memory (one slot per lane, no atomics) to free registers
     __shared__ long long accs[128 * 8];
@@ -155,17 +154,21 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     for (int ci = blockIdx.x * wpb + (threadIdx.x >> 5); ci < nclus; ci += gridDim.x * wpb) {
         const int n = s.clus_n[ci];
         const int base = ci * W;
-        const double x00 = wfirst[3 * base], y00 = wfirst[3 * base + 1], z00 = wfirst[3 * base + 2];
+        const WaterRec r00 = s.wrec[base];
+        const double x00 = r00.x0, y00 = r00.y0, z00 = r00.z0;
         // i-cluster atoms: FP32 offsets from the first oxygen, broadcast from shared memory
         float4* __restrict__ sp = sp_all + (threadIdx.x >> 5) * (W * 3);
         if (lane < W * 3) {
             const int k = lane / 3, a = lane % 3;
             float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
             if (k < n) {
-                const float4 d = wdel[(base + k) * 3 + a];
-                p.x = float(wfirst[3 * (base + k)] - x00) + d.x;
-                p.y = float(wfirst[3 * (base + k) + 1] - y00) + d.y;
-                p.z = float(wfirst[3 * (base + k) + 2] - z00) + d.z;
+                const WaterRec rk = s.wrec[base + k];
+                const float dx = a == 0 ? 0.f : (a == 1 ? rk.h1x : rk.h2x);
+                const float dy = a == 0 ? 0.f : (a == 1 ? rk.h1y : rk.h2y);
+                const float dz = a == 0 ? 0.f : (a == 1 ? rk.h1z : rk.h2z);
+                p.x = float(rk.x0 - x00) + dx;
+                p.y = float(rk.y0 - y00) + dy;
+                p.z = float(rk.z0 - z00) + dz;
             }
             sp[lane] = p;
         }
@@ -184,20 +187,27 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
             float qx[3], qy[3], qz[3];
             float gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
             if (mask) {
-                double dx = x00 - wfirst[3 * js], dy = y00 - wfirst[3 * js + 1], dz = z00 - wfirst[3 * js + 2];
+                // the j water's 48-byte record: FP64 first atom, FP32 offsets of atoms 1, 2
+                const float4 v0 = __ldg(wrec4 + 3 * js), v1 = __ldg(wrec4 + 3 * js + 1), v2 = __ldg(wrec4 + 3 * js + 2);
+                const double xj = __hiloint2double(__float_as_int(v0.y), __float_as_int(v0.x));
+                const double yj = __hiloint2double(__float_as_int(v0.w), __float_as_int(v0.z));
+                const double zj = __hiloint2double(__float_as_int(v1.y), __float_as_int(v1.x));
+                double dx = x00 - xj, dy = y00 - yj, dz = z00 - zj;
                 if (wp.boundary) {
                     dx -= s.box[0] * rint(dx * s.inv_box[0]);
                     dy -= s.box[1] * rint(dy * s.inv_box[1]);
                     dz -= s.box[2] * rint(dz * s.inv_box[2]);
                 }
                 const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
-#pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    const float4 d = wdel[js * 3 + b];
-                    qx[b] = d.x - Dx;
-                    qy[b] = d.y - Dy;
-                    qz[b] = d.z - Dz;
-                }
+                qx[0] = -Dx;
+                qy[0] = -Dy;
+                qz[0] = -Dz;
+                qx[1] = v1.z - Dx;
+                qy[1] = v1.w - Dy;
+                qz[1] = v2.x - Dz;
+                qx[2] = v2.y - Dx;
+                qy[2] = v2.z - Dy;
+                qz[2] = v2.w - Dz;
             } else {
 #pragma unroll
                 for (int b = 0; b < 3; ++b) qx[b] = qy[b] = qz[b] = 0.f;
@@ -268,12 +278,12 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                     }
             }
             if (mask) {
-                const int aj = s.cg_off[s.slot_cg[js]];
+                long long* __restrict__ fj = FS + static_cast<size_t>(js) * 9;
 #pragma unroll
                 for (int b = 0; b < 3; ++b) {
-                    red_add(&F[3 * (aj + b)], to_fixed_f(gx[b], 4294967296.0f));
-                    red_add(&F[3 * (aj + b) + 1], to_fixed_f(gy[b], 4294967296.0f));
-                    red_add(&F[3 * (aj + b) + 2], to_fixed_f(gz[b], 4294967296.0f));
+                    red_add(fj + 3 * b, to_fixed_f(gx[b], 4294967296.0f));
+                    red_add(fj + 3 * b + 1, to_fixed_f(gy[b], 4294967296.0f));
+                    red_add(fj + 3 * b + 2, to_fixed_f(gz[b], 4294967296.0f));
                 }
             }
         }
@@ -282,9 +292,9 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
         __syncwarp();  // sp is rewritten by the next cluster
         const int k = lane >> 3;
         if ((lane & 7) == 0 && k < n) {
-            const int at = s.cg_off[s.slot_cg[base + k]];
+            long long* __restrict__ fi_out = FS + static_cast<size_t>(base + k) * 9;
 #pragma unroll
-            for (int c = 0; c < 9; ++c) red_add(&F[3 * at + c], to_fixed_f(red[c], 4294967296.0f));
+            for (int c = 0; c < 9; ++c) red_add(fi_out + c, to_fixed_f(red[c], 4294967296.0f));
         }
         my[0] += to_fixed_f(elj, 16777216.0f);
         my[1] += to_fixed_f(ecrf, 16777216.0f);
