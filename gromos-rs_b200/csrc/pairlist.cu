@@ -493,32 +493,42 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                 const int sp = tbeg + t;
                 unsigned ms = 0, ml = 0;
                 if (t < tn && sp > first) {
-                    const float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
+                    float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
+                    if (s.boundary) {  // the sum of two minimum images need not be one
+                        Dx -= s.boxf[0] * rintf(Dx * s.inv_boxf[0]);
+                        Dy -= s.boxf[1] * rintf(Dy * s.inv_boxf[1]);
+                        Dz -= s.boxf[2] * rintf(Dz * s.inv_boxf[2]);
+                    }
                     if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
+                        // branch-free classification of the W pairs; pairs inside a
+                        // band around a cutoff or near half a box edge are decided
+                        // by the exact FP64 test
+                        unsigned amb = 0;
 #pragma unroll
                         for (int k = 0; k < W; ++k) {
-                            if (k >= n || sp <= first + k) continue;
+                            const bool valid = k < n && sp > first + k;
                             const float kx = ex[k] + Dx, ky = ey[k] + Dy, kz = ez[k] + Dz;
                             const float d2 = kx * kx + ky * ky + kz * kz;
-                            int cls;  // 0 none, 1 short, 2 long, 3 undecided
-                            if (!(fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz))
-                                cls = 3;
-                            else if (d2 > l_hi)
-                                cls = 0;
-                            else if (d2 < s_lo)
-                                cls = 1;
-                            else if (d2 > s_hi && d2 < l_lo)
-                                cls = 2;
-                            else
-                                cls = 3;
-                            if (cls == 3) {
-                                double rx, ry, rz;
-                                nearest_image_exact(s, xi[k], yi[k], zi[k], tx[t], ty[t], tz[t], rx, ry, rz);
-                                const double e2 = len2_exact(rx, ry, rz);
-                                cls = e2 > s.c2l ? 0 : (e2 > s.c2s ? 2 : 1);
+                            const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
+                            const bool sh = d2 < s_lo;
+                            const bool lg = d2 > s_hi && d2 < l_lo;
+                            const bool far = d2 > l_hi;
+                            ms |= unsigned(valid && inbox && sh) << k;
+                            ml |= unsigned(valid && inbox && lg) << k;
+                            amb |= unsigned(valid && !(inbox && (sh || lg || far))) << k;
+                        }
+#pragma unroll
+                        for (int k = 0; k < W; ++k) {
+                            if (!((amb >> k) & 1u)) continue;
+                            double rx, ry, rz;
+                            nearest_image_exact(s, xi[k], yi[k], zi[k], tx[t], ty[t], tz[t], rx, ry, rz);
+                            const double e2 = len2_exact(rx, ry, rz);
+                            if (!(e2 > s.c2l)) {
+                                if (e2 > s.c2s)
+                                    ml |= 1u << k;
+                                else
+                                    ms |= 1u << k;
                             }
-                            if (cls == 1) ms |= 1u << k;
-                            if (cls == 2) ml |= 1u << k;
                         }
                     }
                 }

@@ -132,67 +132,111 @@ __device__ __forceinline__ void reduce_scatter_36(const float (&v)[36], float (&
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ double rec_x(float4 v) { return __hiloint2double(__float_as_int(v.y), __float_as_int(v.x)); }
+__device__ __forceinline__ double rec_y(float4 v) { return __hiloint2double(__float_as_int(v.w), __float_as_int(v.z)); }
+
+constexpr int kWaterWarps = 4;
+
+// Software pipeline per warp: the 32 j-records of chunk c+1 are copied into
+// shared memory (cp.async, double buffer) while chunk c is computed, the
+// entries are loaded two chunks ahead, and the next cluster's i-records are
+// copied while the current cluster's forces are reduced.
 template <bool LJ00, bool LONG>
 __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict__ sys, const WaterParams wp) {
     constexpr int W = 4;
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
+    const int wid = threadIdx.x >> 5;
     const int nclus = s.n_clusters[0];
     long long* __restrict__ FS = LONG ? s.fs_long : s.fs_short;  // per slot: 3 atoms x 3 components
     const uint32_t* __restrict__ wl = LONG ? s.wl_l : s.wl_s;
     const int* __restrict__ wn = LONG ? s.wn_l : s.wn_s;
     const float4* __restrict__ wrec4 = reinterpret_cast<const float4*>(s.wrec);
-    // per-lane fixed-point (2^24) accumulators of lj, crf, xx, xy, xz, yy, yz, zz:
-    // kept in shared memory (one slot per lane, no atomics) to free registers
-    __shared__ long long accs[128 * 8];
-    __shared__ float4 sp_all[4 * W * 3];
+    // per-lane fixed-point (2^24) accumulators of lj, crf, xx, xy, xz, yy, yz, zz
+    __shared__ long long accs[kWaterWarps * 32 * 8];
+    __shared__ float4 sp_all[kWaterWarps][W * 3];            // i atoms (offsets from the first oxygen)
+    __shared__ float4 ibuf[kWaterWarps][2][W * 3];           // raw i-records, two clusters
+    __shared__ float4 jbuf[kWaterWarps][2][32 * 3];          // raw j-records, two chunks
     long long* __restrict__ my = accs + threadIdx.x * 8;
 #pragma unroll
     for (int v = 0; v < 8; ++v) my[v] = 0;
+    float4* __restrict__ sp = sp_all[wid];
+    const int stride = gridDim.x * kWaterWarps;
+    int ci = blockIdx.x * kWaterWarps + wid;
+    int ib = 0;
+    // prologue: i-records of the first cluster
+    if (ci < nclus && lane < W * 3) cp_async16(&ibuf[wid][0][lane], wrec4 + 3 * (ci * W) + lane);
+    cp_async_commit();
 
-    for (int ci = blockIdx.x * wpb + (threadIdx.x >> 5); ci < nclus; ci += gridDim.x * wpb) {
+    for (; ci < nclus; ci += stride) {
         const int n = s.clus_n[ci];
         const int base = ci * W;
-        const WaterRec r00 = s.wrec[base];
-        const double x00 = r00.x0, y00 = r00.y0, z00 = r00.z0;
-        // i-cluster atoms: FP32 offsets from the first oxygen, broadcast from shared memory
-        float4* __restrict__ sp = sp_all + (threadIdx.x >> 5) * (W * 3);
+        const int cnt = wn[ci];
+        const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * s.wcap;
+        uint32_t e_cur = lane < cnt ? __ldg(list + lane) : 0u;
+        uint32_t e_nx = 32 + lane < cnt ? __ldg(list + 32 + lane) : 0u;
+        cp_async_wait<0>();  // this cluster's i-records
+        __syncwarp();
+        const double x00 = rec_x(ibuf[wid][ib][0]), y00 = rec_y(ibuf[wid][ib][0]);
+        const double z00 = rec_x(ibuf[wid][ib][1]);
         if (lane < W * 3) {
             const int k = lane / 3, a = lane % 3;
             float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
             if (k < n) {
-                const WaterRec rk = s.wrec[base + k];
-                const float dx = a == 0 ? 0.f : (a == 1 ? rk.h1x : rk.h2x);
-                const float dy = a == 0 ? 0.f : (a == 1 ? rk.h1y : rk.h2y);
-                const float dz = a == 0 ? 0.f : (a == 1 ? rk.h1z : rk.h2z);
-                p.x = float(rk.x0 - x00) + dx;
-                p.y = float(rk.y0 - y00) + dy;
-                p.z = float(rk.z0 - z00) + dz;
+                const float4 v0 = ibuf[wid][ib][3 * k], v1 = ibuf[wid][ib][3 * k + 1], v2 = ibuf[wid][ib][3 * k + 2];
+                const float dx = a == 0 ? 0.f : (a == 1 ? v1.z : v2.y);
+                const float dy = a == 0 ? 0.f : (a == 1 ? v1.w : v2.z);
+                const float dz = a == 0 ? 0.f : (a == 1 ? v2.x : v2.w);
+                p.x = float(rec_x(v0) - x00) + dx;
+                p.y = float(rec_y(v0) - y00) + dy;
+                p.z = float(rec_x(v1) - z00) + dz;
             }
             sp[lane] = p;
         }
+        // j-records of chunk 0
+        if (e_cur & 0xffu) {
+            const int js = static_cast<int>(e_cur >> 8);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][0][3 * lane + q], wrec4 + 3 * js + q);
+        }
+        cp_async_commit();
         __syncwarp();
         float fi[36];
 #pragma unroll
         for (int i = 0; i < 36; ++i) fi[i] = 0.f;
-        float elj = 0.f, ecrf = 0.f, v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f, v4 = 0.f, v5 = 0.f;
-        const int cnt = wn[ci];
-        const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * s.wcap;
-        for (int e0 = 0; e0 < cnt; e0 += 32) {
-            const int e = e0 + lane;
-            const uint32_t ent = e < cnt ? __ldg(list + e) : 0u;
+        float elj = 0.f, ecrf = 0.f, v0s = 0.f, v1s = 0.f, v2s = 0.f, v3s = 0.f, v4s = 0.f, v5s = 0.f;
+        const int nch = (cnt + 31) >> 5;
+        for (int c = 0; c < nch; ++c) {
+            const int jb = c & 1;
+            if (c + 1 < nch && (e_nx & 0xffu)) {
+                const int js = static_cast<int>(e_nx >> 8);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][jb ^ 1][3 * lane + q], wrec4 + 3 * js + q);
+            }
+            cp_async_commit();
+            const int e2 = (c + 2) * 32 + lane;
+            const uint32_t e_nn = e2 < cnt ? __ldg(list + e2) : 0u;
+            cp_async_wait<1>();  // chunk c's records
+            __syncwarp();
+            const uint32_t ent = e_cur;
             const unsigned mask = ent & 0xffu;
             const int js = static_cast<int>(ent >> 8);
             float qx[3], qy[3], qz[3];
             float gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
             if (mask) {
-                // the j water's 48-byte record: FP64 first atom, FP32 offsets of atoms 1, 2
-                const float4 v0 = __ldg(wrec4 + 3 * js), v1 = __ldg(wrec4 + 3 * js + 1), v2 = __ldg(wrec4 + 3 * js + 2);
-                const double xj = __hiloint2double(__float_as_int(v0.y), __float_as_int(v0.x));
-                const double yj = __hiloint2double(__float_as_int(v0.w), __float_as_int(v0.z));
-                const double zj = __hiloint2double(__float_as_int(v1.y), __float_as_int(v1.x));
-                double dx = x00 - xj, dy = y00 - yj, dz = z00 - zj;
+                const float4 r0 = jbuf[wid][jb][3 * lane], r1 = jbuf[wid][jb][3 * lane + 1],
+                             r2 = jbuf[wid][jb][3 * lane + 2];
+                double dx = x00 - rec_x(r0), dy = y00 - rec_y(r0), dz = z00 - rec_x(r1);
                 if (wp.boundary) {
                     dx -= s.box[0] * rint(dx * s.inv_box[0]);
                     dy -= s.box[1] * rint(dy * s.inv_box[1]);
@@ -202,12 +246,12 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                 qx[0] = -Dx;
                 qy[0] = -Dy;
                 qz[0] = -Dz;
-                qx[1] = v1.z - Dx;
-                qy[1] = v1.w - Dy;
-                qz[1] = v2.x - Dz;
-                qx[2] = v2.y - Dx;
-                qy[2] = v2.z - Dy;
-                qz[2] = v2.w - Dz;
+                qx[1] = r1.z - Dx;
+                qy[1] = r1.w - Dy;
+                qz[1] = r2.x - Dz;
+                qx[2] = r2.y - Dx;
+                qy[2] = r2.z - Dy;
+                qz[2] = r2.w - Dz;
             } else {
 #pragma unroll
                 for (int b = 0; b < 3; ++b) qx[b] = qy[b] = qz[b] = 0.f;
@@ -224,9 +268,7 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                 if (!(fabsf(r0x) < wp.lim[0] && fabsf(r0y) < wp.lim[1] && fabsf(r0z) < wp.lim[2])) {
                     const PairAcc o = water_slow_pair<LJ00, LONG>(s, wp, base + k, js);
 #pragma unroll
-                    for (int c = 0; c < 9; ++c) {
-                        fi[k * 9 + c] += o.fi[c];
-                    }
+                    for (int cc = 0; cc < 9; ++cc) fi[k * 9 + cc] += o.fi[cc];
 #pragma unroll
                     for (int b = 0; b < 3; ++b) {
                         gx[b] += o.fj[b * 3];
@@ -235,12 +277,12 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                     }
                     elj += o.elj;
                     ecrf += o.ecrf;
-                    v0 += o.v[0];
-                    v1 += o.v[1];
-                    v2 += o.v[2];
-                    v3 += o.v[3];
-                    v4 += o.v[4];
-                    v5 += o.v[5];
+                    v0s += o.v[0];
+                    v1s += o.v[1];
+                    v2s += o.v[2];
+                    v3s += o.v[3];
+                    v4s += o.v[4];
+                    v5s += o.v[5];
                     continue;
                 }
 #pragma unroll
@@ -262,19 +304,19 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                             elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, elj);
                             fs = fmaf(fmaf(12.f * wp.c12[t], ri6, -6.f * wp.c6[t]), ri6 * ri2, fs);
                         }
-                        const float fx = x * fs, fy = y * fs, fz = z * fs;
-                        fi[k * 9 + a * 3] += fx;
-                        fi[k * 9 + a * 3 + 1] += fy;
-                        fi[k * 9 + a * 3 + 2] += fz;
-                        gx[b] -= fx;
-                        gy[b] -= fy;
-                        gz[b] -= fz;
-                        v0 = fmaf(x, fx, v0);
-                        v1 = fmaf(x, fy, v1);
-                        v2 = fmaf(x, fz, v2);
-                        v3 = fmaf(y, fy, v3);
-                        v4 = fmaf(y, fz, v4);
-                        v5 = fmaf(z, fz, v5);
+                        const float fxx = x * fs, fyy = y * fs, fzz = z * fs;
+                        fi[k * 9 + a * 3] += fxx;
+                        fi[k * 9 + a * 3 + 1] += fyy;
+                        fi[k * 9 + a * 3 + 2] += fzz;
+                        gx[b] -= fxx;
+                        gy[b] -= fyy;
+                        gz[b] -= fzz;
+                        v0s = fmaf(x, fxx, v0s);
+                        v1s = fmaf(x, fyy, v1s);
+                        v2s = fmaf(x, fzz, v2s);
+                        v3s = fmaf(y, fyy, v3s);
+                        v4s = fmaf(y, fzz, v4s);
+                        v5s = fmaf(z, fzz, v5s);
                     }
             }
             if (mask) {
@@ -286,32 +328,37 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                     red_add(fj + 3 * b + 2, to_fixed_f(gz[b], 4294967296.0f));
                 }
             }
+            e_cur = e_nx;
+            e_nx = e_nn;
+            __syncwarp();  // jbuf[jb] is refilled two chunks later
         }
+        // next cluster's i-records, copied while this cluster's forces are reduced
+        const int cn = ci + stride;
+        if (cn < nclus && lane < W * 3) cp_async16(&ibuf[wid][ib ^ 1][lane], wrec4 + 3 * (cn * W) + lane);
+        cp_async_commit();
         float red[9];
         reduce_scatter_36(fi, red, lane);
-        __syncwarp();  // sp is rewritten by the next cluster
         const int k = lane >> 3;
         if ((lane & 7) == 0 && k < n) {
             long long* __restrict__ fi_out = FS + static_cast<size_t>(base + k) * 9;
 #pragma unroll
-            for (int c = 0; c < 9; ++c) red_add(fi_out + c, to_fixed_f(red[c], 4294967296.0f));
+            for (int cc = 0; cc < 9; ++cc) red_add(fi_out + cc, to_fixed_f(red[cc], 4294967296.0f));
         }
         my[0] += to_fixed_f(elj, 16777216.0f);
         my[1] += to_fixed_f(ecrf, 16777216.0f);
-        my[2] += to_fixed_f(v0, 16777216.0f);
-        my[3] += to_fixed_f(v1, 16777216.0f);
-        my[4] += to_fixed_f(v2, 16777216.0f);
-        my[5] += to_fixed_f(v3, 16777216.0f);
-        my[6] += to_fixed_f(v4, 16777216.0f);
-        my[7] += to_fixed_f(v5, 16777216.0f);
+        my[2] += to_fixed_f(v0s, 16777216.0f);
+        my[3] += to_fixed_f(v1s, 16777216.0f);
+        my[4] += to_fixed_f(v2s, 16777216.0f);
+        my[5] += to_fixed_f(v3s, 16777216.0f);
+        my[6] += to_fixed_f(v4s, 16777216.0f);
+        my[7] += to_fixed_f(v5s, 16777216.0f);
+        ib ^= 1;
+        __syncwarp();  // sp is rewritten by the next cluster
     }
+    cp_async_wait<0>();
     long long acc[8];
 #pragma unroll
-    for (int v = 0; v < 8; ++v) acc[v] = my[v];
-    // warp sums of the per-lane fixed-point accumulators, then one atomic per
-    // block and quantity (virial written to both symmetric slots)
-#pragma unroll
-    for (int v = 0; v < 8; ++v) acc[v] = warp_sum_ll(acc[v]);
+    for (int v = 0; v < 8; ++v) acc[v] = warp_sum_ll(my[v]);
     __shared__ unsigned long long sh[8];
     if (threadIdx.x < 8) sh[threadIdx.x] = 0ull;
     __syncthreads();
