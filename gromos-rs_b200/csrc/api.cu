@@ -626,8 +626,22 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
         (++launches, k_cell_sort<<<h.n_cells, 1024, 0, s>>>(d_sys));
         (++launches, k_scan_clusters<<<1, 1024, 0, s>>>(d_sys));
         (++launches, k_cluster_setup<<<blocks_for(h.n_cells, 8), 256, 0, s>>>(d_sys));
-        if (NCG > NSCG)
-            (++launches, k_water_search<<<unsigned(h.max_clusters / kSearchWarps + h.n_cells + 1), kSearchWarps * 32, 0, s>>>(d_sys));
+        if (NCG > NSCG) {
+            SearchParams P;
+            for (int k = 0; k < 3; ++k) {
+                P.box[k] = h.box[k];
+                P.inv_box[k] = h.inv_box[k];
+                P.boxf[k] = h.boxf[k];
+                P.inv_boxf[k] = h.inv_boxf[k];
+                P.half_boxf[k] = h.half_boxf[k];
+            }
+            P.c2s = h.c2s;
+            P.c2l = h.c2l;
+            P.boundary = h.boundary;
+            P.wcap = h.wcap;
+            (++launches, k_water_search<<<unsigned(h.max_clusters / kSearchWarps + h.n_cells + 1), kSearchWarps * 32, 0,
+                                          s>>>(d_sys, P));
+        }
         if (NSCG > 0) (++launches, k_solute_search<<<blocks_for(NSCG, 4), 128, 0, s>>>(d_sys));
         if (n_pert > 0 && NSCG > 0) {
             GR_CUDA(cudaMemsetAsync(h.n_pert_pairs, 0, sizeof(int), s));
@@ -792,7 +806,11 @@ WaterParams NbSystem::water_params(bool long_range) const {
     wp.crfc = h.crf_cut_f;
     wp.crf3 = h.crf_cut3i_f;
     const float margin = long_range ? 0.6f : 1e-4f;
-    for (int k = 0; k < 3; ++k) wp.lim[k] = h.boundary ? h.half_boxf[k] - margin : 3.0e38f;
+    for (int k = 0; k < 3; ++k) {
+        wp.lim[k] = h.boundary ? h.half_boxf[k] - margin : 3.0e38f;
+        wp.box[k] = h.box[k];
+        wp.inv_box[k] = h.inv_box[k];
+    }
     wp.boundary = h.boundary;
     wp.G = G;
     const int gs = solvent_group < 0 ? 0 : solvent_group;

@@ -10,7 +10,8 @@ __global__ void k_scatter(const SysDev* __restrict__ sys, const unsigned long lo
 __global__ void k_cell_sort(const SysDev* __restrict__ sys);
 __global__ void k_scan_clusters(const SysDev* __restrict__ sys);
 __global__ void k_cluster_setup(const SysDev* __restrict__ sys);
-__global__ void k_water_search(const SysDev* __restrict__ sys);
+struct SearchParams;
+__global__ void k_water_search(const SysDev* __restrict__ sys, const SearchParams P);
 __global__ void k_solute_search(const SysDev* __restrict__ sys);
 __global__ void k_pert_pairs(const SysDev* __restrict__ sys);
 __global__ void k_expand_cgpairs(const SysDev* __restrict__ sys, int long_range);

@@ -283,6 +283,15 @@ __device__ __forceinline__ int axis_offsets(int g, int* off) {
 // Each cluster's entries are collected in shared memory and written out
 // sorted by mask value, so warp chunks of the force kernel see similar masks.
 constexpr int kTile = 256;
+
+// Per-launch constants of the water search (kernel parameters, constant bank).
+struct SearchParams {
+    double box[3], inv_box[3];
+    float boxf[3], inv_boxf[3], half_boxf[3];
+    double c2s, c2l;
+    int boundary;
+    int wcap;
+};
 constexpr int kEntBuf = 512;
 
 __device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ buf, int nbuf,
@@ -314,7 +323,7 @@ __device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ 
     }
 }
 
-__global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev* __restrict__ sys) {
+__global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
     constexpr int W = 4;
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -363,20 +372,20 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
         ez[k] = float(zi[k] - zi[0]);
         if (k < n) rad = fmaxf(rad, sqrtf(ex[k] * ex[k] + ey[k] * ey[k] + ez[k] * ez[k]));
     }
-    const float reach = sqrtf(float(s.c2l)) + rad + 1e-3f;
+    const float reach = sqrtf(float(P.c2l)) + rad + 1e-3f;
     const float reach2 = reach * reach;
-    const float c2s = float(s.c2s), c2l = float(s.c2l);
+    const float c2s = float(P.c2s), c2l = float(P.c2l);
     const float s_lo = c2s * (1.f - 1e-5f), s_hi = c2s * (1.f + 1e-5f);
     const float l_lo = c2l * (1.f - 1e-5f), l_hi = c2l * (1.f + 1e-5f);
-    const float limx = s.boundary ? s.half_boxf[0] - 1e-4f : 3e38f;
-    const float limy = s.boundary ? s.half_boxf[1] - 1e-4f : 3e38f;
-    const float limz = s.boundary ? s.half_boxf[2] - 1e-4f : 3e38f;
+    const float limx = P.boundary ? P.half_boxf[0] - 1e-4f : 3e38f;
+    const float limy = P.boundary ? P.half_boxf[1] - 1e-4f : 3e38f;
+    const float limz = P.boundary ? P.half_boxf[2] - 1e-4f : 3e38f;
     const int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
     const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
     int ox[3], oy[3], oz[3];
     const int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
-    uint32_t* outs = s.wl_s + static_cast<size_t>(active ? ci : 0) * s.wcap;
-    uint32_t* outl = s.wl_l + static_cast<size_t>(active ? ci : 0) * s.wcap;
+    uint32_t* outs = s.wl_s + static_cast<size_t>(active ? ci : 0) * P.wcap;
+    uint32_t* outl = s.wl_l + static_cast<size_t>(active ? ci : 0) * P.wcap;
     int cnt_s = 0, cnt_l = 0;
     const unsigned below = (1u << lane) - 1u;
     // neighbour cells at or after this one (block-uniform), then the tiles of
@@ -437,10 +446,10 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                 float r = 0.f;
                 if (threadIdx.x < tn) {
                     double dx = px - cx0, dy = py - cy0, dz = pz - cz0;
-                    if (s.boundary) {
-                        dx -= s.box[0] * rint(dx * s.inv_box[0]);
-                        dy -= s.box[1] * rint(dy * s.inv_box[1]);
-                        dz -= s.box[2] * rint(dz * s.inv_box[2]);
+                    if (P.boundary) {
+                        dx -= P.box[0] * rint(dx * P.inv_box[0]);
+                        dy -= P.box[1] * rint(dy * P.inv_box[1]);
+                        dz -= P.box[2] * rint(dz * P.inv_box[2]);
                     }
                     fx[threadIdx.x] = float(dx);
                     fy[threadIdx.x] = float(dy);
@@ -481,10 +490,10 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                 // chunks entirely out of reach (warp-uniform)
                 const int ch = base >> 5;
                 double cdx = xi[0] - chx[ch], cdy = yi[0] - chy[ch], cdz = zi[0] - chz[ch];
-                if (s.boundary) {
-                    cdx -= s.box[0] * rint(cdx * s.inv_box[0]);
-                    cdy -= s.box[1] * rint(cdy * s.inv_box[1]);
-                    cdz -= s.box[2] * rint(cdz * s.inv_box[2]);
+                if (P.boundary) {
+                    cdx -= P.box[0] * rint(cdx * P.inv_box[0]);
+                    cdy -= P.box[1] * rint(cdy * P.inv_box[1]);
+                    cdz -= P.box[2] * rint(cdz * P.inv_box[2]);
                 }
                 const float Cx = float(cdx), Cy = float(cdy), Cz = float(cdz);
                 const float cd = sqrtf(Cx * Cx + Cy * Cy + Cz * Cz);
@@ -494,10 +503,10 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                 unsigned ms = 0, ml = 0;
                 if (t < tn && sp > first) {
                     float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
-                    if (s.boundary) {  // the sum of two minimum images need not be one
-                        Dx -= s.boxf[0] * rintf(Dx * s.inv_boxf[0]);
-                        Dy -= s.boxf[1] * rintf(Dy * s.inv_boxf[1]);
-                        Dz -= s.boxf[2] * rintf(Dz * s.inv_boxf[2]);
+                    if (P.boundary) {  // the sum of two minimum images need not be one
+                        Dx -= P.boxf[0] * rintf(Dx * P.inv_boxf[0]);
+                        Dy -= P.boxf[1] * rintf(Dy * P.inv_boxf[1]);
+                        Dz -= P.boxf[2] * rintf(Dz * P.inv_boxf[2]);
                     }
                     if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
                         // branch-free classification of the W pairs; pairs inside a
@@ -523,8 +532,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                             double rx, ry, rz;
                             nearest_image_exact(s, xi[k], yi[k], zi[k], tx[t], ty[t], tz[t], rx, ry, rz);
                             const double e2 = len2_exact(rx, ry, rz);
-                            if (!(e2 > s.c2l)) {
-                                if (e2 > s.c2s)
+                            if (!(e2 > P.c2l)) {
+                                if (e2 > P.c2s)
                                     ml |= 1u << k;
                                 else
                                     ms |= 1u << k;
@@ -540,7 +549,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                     const uint32_t ent = (slot << 8) | ms;
                     if (p < kEntBuf)
                         ebuf_s[warp][p] = ent;
-                    else if (p < s.wcap)
+                    else if (p < P.wcap)
                         outs[p] = ent;
                 }
                 if (ml) {
@@ -548,7 +557,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                     const uint32_t ent = (slot << 8) | ml;
                     if (p < kEntBuf)
                         ebuf_l[warp][p] = ent;
-                    else if (p < s.wcap)
+                    else if (p < P.wcap)
                         outl[p] = ent;
                 }
                 cnt_s += __popc(bs);
@@ -565,9 +574,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
     sort_write_entries(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
     sort_write_entries(ebuf_l[warp], min(cnt_l, kEntBuf), outl, lane);
     if (lane == 0) {
-        if (cnt_s > s.wcap || cnt_l > s.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
-        s.wn_s[ci] = min(cnt_s, s.wcap);
-        s.wn_l[ci] = min(cnt_l, s.wcap);
+        if (cnt_s > P.wcap || cnt_l > P.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
+        s.wn_s[ci] = min(cnt_s, P.wcap);
+        s.wn_l[ci] = min(cnt_l, P.wcap);
     }
 }
 

@@ -27,6 +27,7 @@ struct WaterParams {
     float c6[9], c12[9];    // solvent LJ table
     float crf2, crfc, crf3; // crf_2cut3i, crf_cut, crf_cut3i
     float lim[3];           // half box edge - margin: FP32 image certain below this
+    double box[3], inv_box[3];
     int boundary;
     int slot;               // energy-group slot of solvent-solvent pairs
     int G;
@@ -162,6 +163,8 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     const uint32_t* __restrict__ wl = LONG ? s.wl_l : s.wl_s;
     const int* __restrict__ wn = LONG ? s.wn_l : s.wn_s;
     const float4* __restrict__ wrec4 = reinterpret_cast<const float4*>(s.wrec);
+    const int* __restrict__ clus_n = s.clus_n;
+    const int wcap = s.wcap;
     // per-lane fixed-point (2^24) accumulators of lj, crf, xx, xy, xz, yy, yz, zz
     __shared__ long long accs[kWaterWarps * 32 * 8];
     __shared__ float4 sp_all[kWaterWarps][W * 3];            // i atoms (offsets from the first oxygen)
@@ -179,10 +182,10 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     cp_async_commit();
 
     for (; ci < nclus; ci += stride) {
-        const int n = s.clus_n[ci];
+        const int n = clus_n[ci];
         const int base = ci * W;
         const int cnt = wn[ci];
-        const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * s.wcap;
+        const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * wcap;
         uint32_t e_cur = lane < cnt ? __ldg(list + lane) : 0u;
         uint32_t e_nx = 32 + lane < cnt ? __ldg(list + 32 + lane) : 0u;
         cp_async_wait<0>();  // this cluster's i-records
@@ -238,9 +241,9 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                              r2 = jbuf[wid][jb][3 * lane + 2];
                 double dx = x00 - rec_x(r0), dy = y00 - rec_y(r0), dz = z00 - rec_x(r1);
                 if (wp.boundary) {
-                    dx -= s.box[0] * rint(dx * s.inv_box[0]);
-                    dy -= s.box[1] * rint(dy * s.inv_box[1]);
-                    dz -= s.box[2] * rint(dz * s.inv_box[2]);
+                    dx -= wp.box[0] * rint(dx * wp.inv_box[0]);
+                    dy -= wp.box[1] * rint(dy * wp.inv_box[1]);
+                    dz -= wp.box[2] * rint(dz * wp.inv_box[2]);
                 }
                 const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
                 qx[0] = -Dx;
