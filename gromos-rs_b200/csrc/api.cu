@@ -373,6 +373,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&h.f_out, size_t(N) * 3))) return st;
     if ((st = alloc(&h.e_out, size_t(acc_size(G))))) return st;
     if ((st = alloc(&h.err, 4))) return st;
+    if ((st = alloc(&h.n_deferred, 2))) return st;
     GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
     GR_CUDA(cudaMemset(h.f_long, 0, size_t(N) * 3 * sizeof(long long)));
     GR_CUDA(cudaMemset(h.acc_long, 0, size_t(acc_size(G)) * sizeof(long long)));
@@ -491,6 +492,8 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.wn_s, size_t(maxc)))) return st;
         if ((st = alloc(&h.wn_l, size_t(maxc)))) return st;
         if ((st = alloc(&h.wrec, size_t(maxc) * W))) return st;
+        h.defer_cap = std::max(4096, (NCG - NSCG) * 4);
+        if ((st = alloc(&h.deferred, size_t(4) * h.defer_cap))) return st;
         if ((st = alloc(&h.fs_short, size_t(maxc) * W * 9))) return st;
         if ((st = alloc(&h.fs_long, size_t(maxc) * W * 9))) return st;
         fs_long_zeroed = false;
@@ -735,10 +738,14 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             wp = water_params();
             (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
             unsigned grid = unsigned(sm * water_blocks_per_sm);
-            if (h.water_lj00_only)
+            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 2 * sizeof(int), s));
+            if (h.water_lj00_only) {
                 (++launches, k_water_force<true, false><<<grid, 128, 0, s>>>(d_sys, wp));
-            else
+                (++launches, k_water_deferred<true, false><<<sm, 128, 0, s>>>(d_sys, wp));
+            } else {
                 (++launches, k_water_force<false, false><<<grid, 128, 0, s>>>(d_sys, wp));
+                (++launches, k_water_deferred<false, false><<<sm, 128, 0, s>>>(d_sys, wp));
+            }
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
         if (record_events) GR_CUDA(cudaEventRecord(ev[2], s));
@@ -750,10 +757,13 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             if (NCG > NSCG) {
                 WaterParams wpl = water_params(true);
                 unsigned grid = unsigned(sm * water_blocks_per_sm);
-                if (h.water_lj00_only)
+                if (h.water_lj00_only) {
                     (++launches, k_water_force<true, true><<<grid, 128, 0, s>>>(d_sys, wpl));
-                else
+                    (++launches, k_water_deferred<true, true><<<sm, 128, 0, s>>>(d_sys, wpl));
+                } else {
                     (++launches, k_water_force<false, true><<<grid, 128, 0, s>>>(d_sys, wpl));
+                    (++launches, k_water_deferred<false, true><<<sm, 128, 0, s>>>(d_sys, wpl));
+                }
             }
             if (NSCG > 0) (++launches, k_solute_force<true><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
             lr_computed = true;
@@ -810,6 +820,8 @@ WaterParams NbSystem::water_params(bool long_range) const {
         wp.lim[k] = h.boundary ? h.half_boxf[k] - margin : 3.0e38f;
         wp.box[k] = h.box[k];
         wp.inv_box[k] = h.inv_box[k];
+        wp.boxf[k] = h.boxf[k];
+        wp.inv_boxf[k] = h.inv_boxf[k];
     }
     wp.boundary = h.boundary;
     wp.G = G;
@@ -1148,6 +1160,12 @@ gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out) {
         if (st) return st;
         if (!download) return GR_OK;  // overflow (if any) is reported by the next call
         if ((st = S.download(ctx->stream, out))) return st;
+        int errs[4] = {0, 0, 0, 0};
+        if (cudaMemcpy(errs, S.h.err, sizeof(errs), cudaMemcpyDeviceToHost) == cudaSuccess &&
+            (errs[0] & gnb::ERR_DEFER_OVERFLOW)) {
+            set_error("water kernel: deferred-pair list overflowed (box too small for the cutoff?)");
+            return GR_ERR_OVERFLOW;
+        }
         bool overflowed = false;
         if ((st = S.resolve_pending(&overflowed))) return st;
         if (!overflowed) break;

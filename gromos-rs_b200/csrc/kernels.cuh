@@ -20,6 +20,8 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys);
 struct WaterParams;
 template <bool LJ00, bool LONG>
 __global__ void k_water_force(const SysDev* __restrict__ sys, const WaterParams wp);
+template <bool LJ00, bool LONG>
+__global__ void k_water_deferred(const SysDev* __restrict__ sys, const WaterParams wp);
 template <bool LONG>
 __global__ void k_solute_force(const SysDev* __restrict__ sys);
 __global__ void k_pos32(const SysDev* __restrict__ sys);

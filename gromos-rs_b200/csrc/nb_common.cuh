@@ -35,6 +35,7 @@ enum : int {
     ERR_CG_TOO_LARGE = 8,
     ERR_PERT_OVERFLOW = 16,
     ERR_CGPAIR_OVERFLOW = 32,
+    ERR_DEFER_OVERFLOW = 64,
 };
 
 // One water per slot, 48 bytes, read with three 16-byte loads: the FP64
@@ -129,6 +130,9 @@ struct SysDev {
     struct WaterRec* wrec;     // [max_clusters*W] per-slot FP64 first atom + FP32 offsets
     long long* fs_short;       // [max_clusters*W*9] water forces per slot (fixed 2^32)
     long long* fs_long;        // same, long-range cache
+    int* deferred;             // [2 * 2 * defer_cap] (i slot, j slot): short, then long
+    int* n_deferred;           // [2]
+    int defer_cap;
     // ---- plain-kernel data
     float4* pos32;             // n_atoms (x, y, z, q)
     int* cgp;                  // [cgp_cap*3] explicit CG pairs (i_cg, j_cg, long)

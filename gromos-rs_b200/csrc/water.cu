@@ -13,8 +13,9 @@
 // oxygens; FP32 arithmetic for the pairs; forces are accumulated in 64-bit
 // fixed point (2^32 per kJ mol^-1 nm^-1): i-forces in registers over the
 // whole list, reduced once per cluster, j-forces once per (cluster, j).
-// A CG pair whose first-atom vector lies within `margin` of half a box edge
-// is redone with exact FP64 images (water_slow_pair), so image choices are
+// A CG pair whose first-atom vector is not certainly inside half a box edge is
+// re-imaged in FP32; if that is still not certain it is deferred to
+// k_water_deferred, which uses the exact FP64 images, so image choices are
 // always those of the reference.
 #include "nb_common.cuh"
 
@@ -28,6 +29,7 @@ struct WaterParams {
     float crf2, crfc, crf3; // crf_2cut3i, crf_cut, crf_cut3i
     float lim[3];           // half box edge - margin: FP32 image certain below this
     double box[3], inv_box[3];
+    float boxf[3], inv_boxf[3];
     int boundary;
     int slot;               // energy-group slot of solvent-solvent pairs
     int G;
@@ -49,7 +51,7 @@ struct PairAcc {
 // reference's exact FP64 images: the first-atom shift (short list) or
 // per-atom images (long list).  Used only for pairs near half a box edge.
 template <bool LJ00, bool LONG>
-__device__ __noinline__ PairAcc water_slow_pair(const SysDev& s, const WaterParams& wp, int islot, int jslot) {
+__device__ __forceinline__ PairAcc water_slow_pair(const SysDev& s, const WaterParams& wp, int islot, int jslot) {
     PairAcc o;
     for (int k = 0; k < 9; ++k) o.fi[k] = o.fj[k] = 0.f;
     o.elj = o.ecrf = 0.f;
@@ -266,36 +268,40 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                 if (!act) continue;
                 const float4 p0 = sp[k * 3], p1 = sp[k * 3 + 1], p2 = sp[k * 3 + 2];
                 const float pxk[3] = {p0.x, p1.x, p2.x}, pyk[3] = {p0.y, p1.y, p2.y}, pzk[3] = {p0.z, p1.z, p2.z};
-                // first-atom vector: decides whether the FP32 image is certain
-                const float r0x = pxk[0] - qx[0], r0y = pyk[0] - qy[0], r0z = pzk[0] - qz[0];
+                // first-atom vector: decides whether the FP32 image is certain; a
+                // pair outside the certain range is re-imaged in FP32 (one shift
+                // for the CG pair), and if still uncertain deferred to the exact
+                // FP64 kernel (k_water_deferred)
+                float r0x = pxk[0] - qx[0], r0y = pyk[0] - qy[0], r0z = pzk[0] - qz[0];
+                float shx = 0.f, shy = 0.f, shz = 0.f;
                 if (!(fabsf(r0x) < wp.lim[0] && fabsf(r0y) < wp.lim[1] && fabsf(r0z) < wp.lim[2])) {
-                    const PairAcc o = water_slow_pair<LJ00, LONG>(s, wp, base + k, js);
-#pragma unroll
-                    for (int cc = 0; cc < 9; ++cc) fi[k * 9 + cc] += o.fi[cc];
-#pragma unroll
-                    for (int b = 0; b < 3; ++b) {
-                        gx[b] += o.fj[b * 3];
-                        gy[b] += o.fj[b * 3 + 1];
-                        gz[b] += o.fj[b * 3 + 2];
+                    if (wp.boundary) {
+                        shx = -wp.boxf[0] * rintf(r0x * wp.inv_boxf[0]);
+                        shy = -wp.boxf[1] * rintf(r0y * wp.inv_boxf[1]);
+                        shz = -wp.boxf[2] * rintf(r0z * wp.inv_boxf[2]);
+                        r0x += shx;
+                        r0y += shy;
+                        r0z += shz;
                     }
-                    elj += o.elj;
-                    ecrf += o.ecrf;
-                    v0s += o.v[0];
-                    v1s += o.v[1];
-                    v2s += o.v[2];
-                    v3s += o.v[3];
-                    v4s += o.v[4];
-                    v5s += o.v[5];
-                    continue;
+                    if (!(fabsf(r0x) < wp.lim[0] && fabsf(r0y) < wp.lim[1] && fabsf(r0z) < wp.lim[2])) {
+                        const int d = atomicAdd(&s.n_deferred[LONG ? 1 : 0], 1);
+                        if (d < s.defer_cap) {
+                            s.deferred[2 * (LONG ? s.defer_cap + d : d)] = base + k;
+                            s.deferred[2 * (LONG ? s.defer_cap + d : d) + 1] = js;
+                        } else {
+                            atomicOr(&s.err[0], ERR_DEFER_OVERFLOW);
+                        }
+                        continue;
+                    }
                 }
 #pragma unroll
                 for (int a = 0; a < 3; ++a)
 #pragma unroll
                     for (int b = 0; b < 3; ++b) {
                         const int t = a * 3 + b;
-                        const float x = (a == 0 && b == 0) ? r0x : pxk[a] - qx[b];
-                        const float y = (a == 0 && b == 0) ? r0y : pyk[a] - qy[b];
-                        const float z = (a == 0 && b == 0) ? r0z : pzk[a] - qz[b];
+                        const float x = (a == 0 && b == 0) ? r0x : (pxk[a] + shx) - qx[b];
+                        const float y = (a == 0 && b == 0) ? r0y : (pyk[a] + shy) - qy[b];
+                        const float z = (a == 0 && b == 0) ? r0z : (pzk[a] + shz) - qz[b];
                         const float r2 = fmaf(x, x, fmaf(y, y, z * z));
                         const float ri = r2 < 1e-10f ? 0.f : rsqrt_fast(r2);
                         const float ri2 = ri * ri;
@@ -381,6 +387,44 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     }
 }
 
+// CG pairs the main kernel deferred: exact FP64 images (first-atom shift for
+// the short list, per-atom images for the long list), FP32 pair arithmetic.
+template <bool LJ00, bool LONG>
+__global__ void __launch_bounds__(128) k_water_deferred(const SysDev* __restrict__ sys, const WaterParams wp) {
+    const SysDev& s = sys[blockIdx.y];
+    long long* __restrict__ FS = LONG ? s.fs_long : s.fs_short;
+    const int nd = min(s.n_deferred[LONG ? 1 : 0], s.defer_cap);
+    long long acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nd; d += gridDim.x * blockDim.x) {
+        const int e = LONG ? s.defer_cap + d : d;
+        const int islot = s.deferred[2 * e], jslot = s.deferred[2 * e + 1];
+        const PairAcc o = water_slow_pair<LJ00, LONG>(s, wp, islot, jslot);
+        for (int c = 0; c < 9; ++c) {
+            red_add(FS + static_cast<size_t>(islot) * 9 + c, to_fixed_f(o.fi[c], 4294967296.0f));
+            red_add(FS + static_cast<size_t>(jslot) * 9 + c, to_fixed_f(o.fj[c], 4294967296.0f));
+        }
+        acc[0] += to_fixed_f(o.elj, 16777216.0f);
+        acc[1] += to_fixed_f(o.ecrf, 16777216.0f);
+        for (int v = 0; v < 6; ++v) acc[2 + v] += to_fixed_f(o.v[v], 16777216.0f);
+    }
+    long long* dst = LONG ? s.acc_long : s.acc_short;
+    const int G = wp.G, vb = 2 * G * G;
+    const int idx0[8] = {wp.slot, G * G + wp.slot, vb + 0, vb + 1, vb + 2, vb + 4, vb + 5, vb + 8};
+    const int idx1[8] = {-1, -1, -1, vb + 3, vb + 6, -1, vb + 7, -1};
+    for (int v = 0; v < 8; ++v) {
+        const long long t = warp_sum_ll(acc[v]);
+        if ((threadIdx.x & 31) == 0 && t) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx0[v]), static_cast<unsigned long long>(t));
+            if (idx1[v] >= 0)
+                atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx1[v]), static_cast<unsigned long long>(t));
+        }
+    }
+}
+
+template __global__ void k_water_deferred<true, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_deferred<true, true>(const SysDev*, const WaterParams);
+template __global__ void k_water_deferred<false, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_deferred<false, true>(const SysDev*, const WaterParams);
 template __global__ void k_water_force<true, false>(const SysDev*, const WaterParams);
 template __global__ void k_water_force<true, true>(const SysDev*, const WaterParams);
 template __global__ void k_water_force<false, false>(const SysDev*, const WaterParams);
