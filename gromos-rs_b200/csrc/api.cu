@@ -374,6 +374,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&h.e_out, size_t(acc_size(G))))) return st;
     if ((st = alloc(&h.err, 4))) return st;
     if ((st = alloc(&h.n_deferred, 2))) return st;
+    if ((st = alloc(&h.max_delta, 1))) return st;
     GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
     GR_CUDA(cudaMemset(h.f_long, 0, size_t(N) * 3 * sizeof(long long)));
     GR_CUDA(cudaMemset(h.acc_long, 0, size_t(acc_size(G)) * sizeof(long long)));
@@ -492,7 +493,12 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.wn_s, size_t(maxc)))) return st;
         if ((st = alloc(&h.wn_l, size_t(maxc)))) return st;
         if ((st = alloc(&h.wrec, size_t(maxc) * W))) return st;
-        h.defer_cap = std::max(4096, (NCG - NSCG) * 4);
+        // pairs near half a box edge are few unless the box is small for the cutoff
+        {
+            double half_min = std::min(std::min(h.box[0], h.box[1]), h.box[2]) * 0.5;
+            int per = (prm.rcutl + prm.skin + 0.3 > half_min) ? 64 : 4;
+            h.defer_cap = std::max(4096, std::max(defer_want, (NCG - NSCG) * per));
+        }
         if ((st = alloc(&h.deferred, size_t(4) * h.defer_cap))) return st;
         if ((st = alloc(&h.fs_short, size_t(maxc) * W * 9))) return st;
         if ((st = alloc(&h.fs_long, size_t(maxc) * W * 9))) return st;
@@ -723,7 +729,10 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     const int NA = acc_size(G);
     GR_CUDA(cudaMemsetAsync(h.f_short, 0, size_t(N) * 3 * sizeof(long long), s));
     GR_CUDA(cudaMemsetAsync(h.acc_short, 0, size_t(NA) * sizeof(long long), s));
-    if (NCG > NSCG) GR_CUDA(cudaMemsetAsync(h.fs_short, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
+    if (NCG > NSCG) {
+        GR_CUDA(cudaMemsetAsync(h.fs_short, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
+        GR_CUDA(cudaMemsetAsync(h.max_delta, 0, sizeof(float), s));
+    }
     if (NCG > NSCG && !fs_long_zeroed) {
         // the slot layout changes at rebuilds; keep the long cache consistent
         GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
@@ -815,7 +824,7 @@ WaterParams NbSystem::water_params(bool long_range) const {
     wp.crf2 = h.crf_2cut3i_f;
     wp.crfc = h.crf_cut_f;
     wp.crf3 = h.crf_cut3i_f;
-    const float margin = long_range ? 0.6f : 1e-4f;
+    const float margin = 1e-4f;  // the long list adds the measured molecule extent in the kernel
     for (int k = 0; k < 3; ++k) {
         wp.lim[k] = h.boundary ? h.half_boxf[k] - margin : 3.0e38f;
         wp.box[k] = h.box[k];
@@ -1163,8 +1172,17 @@ gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out) {
         int errs[4] = {0, 0, 0, 0};
         if (cudaMemcpy(errs, S.h.err, sizeof(errs), cudaMemcpyDeviceToHost) == cudaSuccess &&
             (errs[0] & gnb::ERR_DEFER_OVERFLOW)) {
-            set_error("water kernel: deferred-pair list overflowed (box too small for the cutoff?)");
-            return GR_ERR_OVERFLOW;
+            // grow the deferred-pair list and redo this evaluation (long range too)
+            cudaMemset(S.h.err, 0, sizeof(errs));
+            if (attempt >= 8) {
+                set_error("water kernel: deferred-pair list could not be grown far enough");
+                return GR_ERR_OVERFLOW;
+            }
+            S.defer_want = std::max(S.defer_want, S.h.defer_cap) * 4;
+            S.clus_alloc = 0;  // re-run the cluster allocation with the larger list
+            S.built = false;
+            S.lr_computed = false;
+            continue;
         }
         bool overflowed = false;
         if ((st = S.resolve_pending(&overflowed))) return st;

@@ -54,6 +54,10 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
             w.h2y = float(s.pos[3 * a0 + 7] - y0);
             w.h2z = float(s.pos[3 * a0 + 8] - z0);
             s.wrec[slot] = w;
+            // extent of the molecule (per-atom images of the long list need it)
+            float m = fmaxf(fmaxf(fabsf(w.h1x), fabsf(w.h1y)), fmaxf(fabsf(w.h1z), fabsf(w.h2x)));
+            m = fmaxf(m, fmaxf(fabsf(w.h2y), fabsf(w.h2z)));
+            atomicMax(reinterpret_cast<int*>(s.max_delta), __float_as_int(m));
             // solvent excluded pairs: energy only, -q_i q_j fpe crf_2cut3i r^2
             // (rf_excluded_interactions, excluded.rs:81-96)
             if (s.excl_atoms < s.n_atoms)

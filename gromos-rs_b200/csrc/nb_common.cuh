@@ -132,6 +132,7 @@ struct SysDev {
     long long* fs_long;        // same, long-range cache
     int* deferred;             // [2 * 2 * defer_cap] (i slot, j slot): short, then long
     int* n_deferred;           // [2]
+    float* max_delta;          // [1] largest |offset| component of a water atom from its first atom (this step)
     int defer_cap;
     // ---- plain-kernel data
     float4* pos32;             // n_atoms (x, y, z, q)

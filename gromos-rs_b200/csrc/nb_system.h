@@ -55,7 +55,7 @@ class NbSystem {
     long long launches = 0;  // kernels launched by this system
     // capacities
     int cells_alloc = 0, clus_alloc = 0, wcap_alloc = 0, scap_alloc = 0, pcap_alloc = 0, cgp_alloc = 0;
-    int wcap_want = 0, scap_want = 0, pcap_want = 0;
+    int wcap_want = 0, scap_want = 0, pcap_want = 0, defer_want = 0;
     long long cgp_want = 0;
     int regrow_count = 0;
     size_t bytes = 0;

@@ -167,6 +167,16 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     const float4* __restrict__ wrec4 = reinterpret_cast<const float4*>(s.wrec);
     const int* __restrict__ clus_n = s.clus_n;
     const int wcap = s.wcap;
+    // certain-image limits: the short list needs only the first-atom vector
+    // inside half a box edge; per-atom images (long list) also need room for
+    // both molecules' extents (measured this step by k_water_prep)
+    float limx = wp.lim[0], limy = wp.lim[1], limz = wp.lim[2];
+    if (LONG) {
+        const float m = 2.f * (*s.max_delta) * 1.0001f + 1e-4f;
+        limx -= m;
+        limy -= m;
+        limz -= m;
+    }
     // per-lane fixed-point (2^24) accumulators of lj, crf, xx, xy, xz, yy, yz, zz
     __shared__ long long accs[kWaterWarps * 32 * 8];
     __shared__ float4 sp_all[kWaterWarps][W * 3];            // i atoms (offsets from the first oxygen)
@@ -274,7 +284,7 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                 // FP64 kernel (k_water_deferred)
                 float r0x = pxk[0] - qx[0], r0y = pyk[0] - qy[0], r0z = pzk[0] - qz[0];
                 float shx = 0.f, shy = 0.f, shz = 0.f;
-                if (!(fabsf(r0x) < wp.lim[0] && fabsf(r0y) < wp.lim[1] && fabsf(r0z) < wp.lim[2])) {
+                if (!(fabsf(r0x) < limx && fabsf(r0y) < limy && fabsf(r0z) < limz)) {
                     if (wp.boundary) {
                         shx = -wp.boxf[0] * rintf(r0x * wp.inv_boxf[0]);
                         shy = -wp.boxf[1] * rintf(r0y * wp.inv_boxf[1]);
@@ -283,7 +293,7 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                         r0y += shy;
                         r0z += shz;
                     }
-                    if (!(fabsf(r0x) < wp.lim[0] && fabsf(r0y) < wp.lim[1] && fabsf(r0z) < wp.lim[2])) {
+                    if (!(fabsf(r0x) < limx && fabsf(r0y) < limy && fabsf(r0z) < limz)) {
                         const int d = atomicAdd(&s.n_deferred[LONG ? 1 : 0], 1);
                         if (d < s.defer_cap) {
                             s.deferred[2 * (LONG ? s.defer_cap + d : d)] = base + k;
