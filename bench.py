@@ -178,7 +178,8 @@ def run_gpu(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
     s = generators.config2_spc30000(seed=1002 + rank)
-    ff = Forcefield(s, kernel=args.kernel, device=local_rank)
+    ff = Forcefield(s, kernel=args.kernel, device=local_rank, cluster_size=args.cluster_size,
+                    water_layout=args.layout)
     # pair counts of this configuration (short per step, long per rebuild)
     r0 = ff.apply(s.pos, count_pairs=True)
     n_short, n_long = int(r0["n_pairs_short"]), int(r0["n_pairs_long"])
@@ -257,7 +258,8 @@ def run_gpu(args, rank, world, local_rank):
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64",
                "data": "synthetic (seeded SPC water box)",
                "config": {"workload": WORKLOAD, "n_atoms": s.topo.n_atoms, "box_nm": 9.65, "rcutp": 0.8,
-                          "rcutl": 1.4, "nsnb": 5, "kernel": args.kernel, "pairs_short_per_step": n_short,
+                          "rcutl": 1.4, "nsnb": 5, "kernel": args.kernel, "cluster_size": args.cluster_size,
+                          "water_layout": args.layout, "pairs_short_per_step": n_short,
                           "pairs_long_per_rebuild": n_long, "rebuild_steps_timed": rebuilds,
                           "l2": "flushed (256 MiB write) between steps, outside the step events",
                           "step": "force evaluation only (positions static; MD integration not timed)",
@@ -283,6 +285,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--kernel", default="fixed", choices=["fixed", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cluster-size", type=int, default=0, help="water i-cluster width 4 or 8 (0 = default)")
+    ap.add_argument("--layout", type=int, default=0, help="water kernel layout: 1 shared bits, 2 per-lane bits")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

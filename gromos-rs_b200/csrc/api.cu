@@ -415,8 +415,20 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
         return GR_ERR_INVALID;
     }
     prm = *p;
-    W = 4;  // registers hold a 4-water i-cluster; 8 needs shared-memory i-data
+    // water kernel layout: 1 = lanes share the mask bits (width 4 only),
+    // 2 = each lane iterates over its own bits (width 4 or 8)
+    layout = p->water_layout == 1 ? 1 : 2;
+    W = (layout == 2 && p->cluster_size == 4) ? 4 : (layout == 1 ? 4 : 8);
+    if (p->cluster_size != 0 && p->cluster_size != 4 && p->cluster_size != 8) {
+        set_error("gr_nb_params: cluster_size must be 0, 4 or 8");
+        return GR_ERR_INVALID;
+    }
+    if (layout == 1 && p->cluster_size == 8) {
+        set_error("gr_nb_params: the shared-bit layout supports cluster_size 4 only");
+        return GR_ERR_INVALID;
+    }
     h.W = W;
+    clus_alloc = 0;  // cluster arrays depend on W
     h.boundary = p->boundary;
     h.twin = p->rcutp < p->rcutl - 1e-10 ? 1 : 0;  // forcefield.rs:126
     double rs = p->rcutp + p->skin, rl = p->rcutl + p->skin;
@@ -648,8 +660,13 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
             P.c2l = h.c2l;
             P.boundary = h.boundary;
             P.wcap = h.wcap;
-            (++launches, k_water_search<<<unsigned(h.max_clusters / kSearchWarps + h.n_cells + 1), kSearchWarps * 32, 0,
-                                          s>>>(d_sys, P));
+            const unsigned g = unsigned(h.max_clusters / kSearchWarps + h.n_cells + 1);
+            if (layout == 1)
+                (++launches, k_water_search<4, false><<<g, kSearchWarps * 32, 0, s>>>(d_sys, P));
+            else if (W == 4)
+                (++launches, k_water_search<4, true><<<g, kSearchWarps * 32, 0, s>>>(d_sys, P));
+            else
+                (++launches, k_water_search<8, true><<<g, kSearchWarps * 32, 0, s>>>(d_sys, P));
         }
         if (NSCG > 0) (++launches, k_solute_search<<<blocks_for(NSCG, 4), 128, 0, s>>>(d_sys));
         if (n_pert > 0 && NSCG > 0) {
@@ -748,13 +765,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
             unsigned grid = unsigned(sm * water_blocks_per_sm);
             GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 2 * sizeof(int), s));
-            if (h.water_lj00_only) {
-                (++launches, k_water_force<true, false><<<grid, 128, 0, s>>>(d_sys, wp));
-                (++launches, k_water_deferred<true, false><<<sm, 128, 0, s>>>(d_sys, wp));
-            } else {
-                (++launches, k_water_force<false, false><<<grid, 128, 0, s>>>(d_sys, wp));
-                (++launches, k_water_deferred<false, false><<<sm, 128, 0, s>>>(d_sys, wp));
-            }
+            if ((st = launch_water(s, wp, false))) return st;
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
         if (record_events) GR_CUDA(cudaEventRecord(ev[2], s));
@@ -766,13 +777,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             if (NCG > NSCG) {
                 WaterParams wpl = water_params(true);
                 unsigned grid = unsigned(sm * water_blocks_per_sm);
-                if (h.water_lj00_only) {
-                    (++launches, k_water_force<true, true><<<grid, 128, 0, s>>>(d_sys, wpl));
-                    (++launches, k_water_deferred<true, true><<<sm, 128, 0, s>>>(d_sys, wpl));
-                } else {
-                    (++launches, k_water_force<false, true><<<grid, 128, 0, s>>>(d_sys, wpl));
-                    (++launches, k_water_deferred<false, true><<<sm, 128, 0, s>>>(d_sys, wpl));
-                }
+                if ((st = launch_water(s, wpl, true))) return st;
             }
             if (NSCG > 0) (++launches, k_solute_force<true><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
             lr_computed = true;
@@ -837,6 +842,56 @@ WaterParams NbSystem::water_params(bool long_range) const {
     const int gs = solvent_group < 0 ? 0 : solvent_group;
     wp.slot = gs * G + gs;
     return wp;
+}
+
+// The water force kernel of the selected layout and width, then the
+// deferred-pair kernel.
+gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr) {
+    const int sm = sm_count();
+    const unsigned grid = unsigned(sm * water_blocks_per_sm);
+    const bool lj00 = h.water_lj00_only != 0;
+#define GR_WATER_IT(WW, LJ, LL)                                                                          \
+    do {                                                                                                 \
+        const size_t smem = water_it_smem<WW>();                                                         \
+        static bool attr_set = false;                                                                    \
+        if (!attr_set) {                                                                                 \
+            GR_CUDA(cudaFuncSetAttribute(k_water_force_it<WW, LJ, LL>,                                   \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));       \
+            attr_set = true;                                                                             \
+        }                                                                                                \
+        (++launches, k_water_force_it<WW, LJ, LL><<<grid, 128, smem, s>>>(d_sys, wp));                   \
+    } while (0)
+    if (layout == 1) {
+        if (lj00) {
+            if (lr) (++launches, k_water_force<true, true><<<grid, 128, 0, s>>>(d_sys, wp));
+            else (++launches, k_water_force<true, false><<<grid, 128, 0, s>>>(d_sys, wp));
+        } else {
+            if (lr) (++launches, k_water_force<false, true><<<grid, 128, 0, s>>>(d_sys, wp));
+            else (++launches, k_water_force<false, false><<<grid, 128, 0, s>>>(d_sys, wp));
+        }
+    } else if (W == 4) {
+        if (lj00) {
+            if (lr) GR_WATER_IT(4, true, true); else GR_WATER_IT(4, true, false);
+        } else {
+            if (lr) GR_WATER_IT(4, false, true); else GR_WATER_IT(4, false, false);
+        }
+    } else {
+        if (lj00) {
+            if (lr) GR_WATER_IT(8, true, true); else GR_WATER_IT(8, true, false);
+        } else {
+            if (lr) GR_WATER_IT(8, false, true); else GR_WATER_IT(8, false, false);
+        }
+    }
+#undef GR_WATER_IT
+    if (lj00) {
+        if (lr) (++launches, k_water_deferred<true, true><<<sm, 128, 0, s>>>(d_sys, wp));
+        else (++launches, k_water_deferred<true, false><<<sm, 128, 0, s>>>(d_sys, wp));
+    } else {
+        if (lr) (++launches, k_water_deferred<false, true><<<sm, 128, 0, s>>>(d_sys, wp));
+        else (++launches, k_water_deferred<false, false><<<sm, 128, 0, s>>>(d_sys, wp));
+    }
+    GR_CUDA(cudaGetLastError());
+    return GR_OK;
 }
 
 int NbSystem::sm_count() {

@@ -11,6 +11,7 @@ __global__ void k_cell_sort(const SysDev* __restrict__ sys);
 __global__ void k_scan_clusters(const SysDev* __restrict__ sys);
 __global__ void k_cluster_setup(const SysDev* __restrict__ sys);
 struct SearchParams;
+template <int W, bool POPSORT>
 __global__ void k_water_search(const SysDev* __restrict__ sys, const SearchParams P);
 __global__ void k_solute_search(const SysDev* __restrict__ sys);
 __global__ void k_pert_pairs(const SysDev* __restrict__ sys);
@@ -22,6 +23,8 @@ template <bool LJ00, bool LONG>
 __global__ void k_water_force(const SysDev* __restrict__ sys, const WaterParams wp);
 template <bool LJ00, bool LONG>
 __global__ void k_water_deferred(const SysDev* __restrict__ sys, const WaterParams wp);
+template <int W, bool LJ00, bool LONG>
+__global__ void k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp);
 template <bool LONG>
 __global__ void k_solute_force(const SysDev* __restrict__ sys);
 __global__ void k_pos32(const SysDev* __restrict__ sys);

@@ -32,9 +32,10 @@ class NbSystem {
     gr_status push_descriptor(cudaStream_t s);
     int sm_count();
     WaterParams water_params(bool long_range = false) const;
+    gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
 
     // sizes
-    int N = 0, NCG = 0, NSCG = 0, NSA = 0, NT = 0, G = 1, aps = 3, W = 4;
+    int N = 0, NCG = 0, NSCG = 0, NSA = 0, NT = 0, G = 1, aps = 3, W = 4, layout = 2;
     int n_pert = 0, solvent_group = -1;
     double fpe = 138.9354;
     gr_nb_params prm{};

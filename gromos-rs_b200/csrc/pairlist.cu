@@ -323,8 +323,40 @@ __device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ 
     }
 }
 
+// Stable counting sort of a cluster's entries by popcount of the mask (lanes of
+// a warp chunk then iterate over the same number of bits).
+template <int W>
+__device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restrict__ buf, int nbuf,
+                                                       uint32_t* __restrict__ out, int lane) {
+    int off[W + 1];
+    int hist[W + 1];
+#pragma unroll
+    for (int v = 0; v <= W; ++v) hist[v] = 0;
+    for (int c = 0; c < nbuf; c += 32) {
+        const int e = c + lane;
+        const int m = e < nbuf ? __popc(buf[e] & 0xffu) : 0;
+#pragma unroll
+        for (int v = 1; v <= W; ++v) hist[v] += __popc(__ballot_sync(0xffffffffu, m == v));
+    }
+    off[0] = 0;
+#pragma unroll
+    for (int v = 1; v <= W; ++v) off[v] = off[v - 1] + hist[v - 1];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int c = 0; c < nbuf; c += 32) {
+        const int e = c + lane;
+        const uint32_t ent = e < nbuf ? buf[e] : 0u;
+        const int m = e < nbuf ? __popc(ent & 0xffu) : 0;
+#pragma unroll
+        for (int v = 1; v <= W; ++v) {
+            const unsigned b = __ballot_sync(0xffffffffu, m == v);
+            if (m == v) out[off[v] + __popc(b & lt)] = ent;
+            off[v] += __popc(b);
+        }
+    }
+}
+
+template <int W, bool POPSORT>
 __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
-    constexpr int W = 4;
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int b = blockIdx.x;
@@ -347,29 +379,35 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
     __shared__ float chr[kTile / 32];                        // chunk radii
     __shared__ uint32_t ebuf_s[kSearchWarps][kEntBuf], ebuf_l[kSearchWarps][kEntBuf];
 
+    // the cluster's first atoms: FP64 in shared memory (exact tests), FP32
+    // offsets from the first one in registers
+    __shared__ double cxs[kSearchWarps][3][8];
     int n = 0, first = 0;
-    double xi[W], yi[W], zi[W];
     float ex[W], ey[W], ez[W];
-#pragma unroll
-    for (int k = 0; k < W; ++k) xi[k] = yi[k] = zi[k] = 0.0;
     if (active) {
         n = s.clus_n[ci];
         first = s.clus_first[ci];
-#pragma unroll
-        for (int k = 0; k < W; ++k)
-            if (k < n) {
-                const int cg = s.sorted_cg[first + k];
-                xi[k] = s.ref[3 * cg];
-                yi[k] = s.ref[3 * cg + 1];
-                zi[k] = s.ref[3 * cg + 2];
+        if (lane < W) {
+            double x = 0, y = 0, z = 0;
+            if (lane < n) {
+                const int cg = s.sorted_cg[first + lane];
+                x = s.ref[3 * cg];
+                y = s.ref[3 * cg + 1];
+                z = s.ref[3 * cg + 2];
             }
+            cxs[warp][0][lane] = x;
+            cxs[warp][1][lane] = y;
+            cxs[warp][2][lane] = z;
+        }
     }
+    __syncwarp();
+    const double x0 = cxs[warp][0][0], y0 = cxs[warp][1][0], z0 = cxs[warp][2][0];
     float rad = 0.f;
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-        ex[k] = float(xi[k] - xi[0]);
-        ey[k] = float(yi[k] - yi[0]);
-        ez[k] = float(zi[k] - zi[0]);
+        ex[k] = k < n ? float(cxs[warp][0][k] - x0) : 0.f;
+        ey[k] = k < n ? float(cxs[warp][1][k] - y0) : 0.f;
+        ez[k] = k < n ? float(cxs[warp][2][k] - z0) : 0.f;
         if (k < n) rad = fmaxf(rad, sqrtf(ex[k] * ex[k] + ey[k] * ey[k] + ez[k] * ez[k]));
     }
     const float reach = sqrtf(float(P.c2l)) + rad + 1e-3f;
@@ -489,7 +527,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                 // cluster-to-chunk vector (FP64 image once per chunk); skip
                 // chunks entirely out of reach (warp-uniform)
                 const int ch = base >> 5;
-                double cdx = xi[0] - chx[ch], cdy = yi[0] - chy[ch], cdz = zi[0] - chz[ch];
+                double cdx = x0 - chx[ch], cdy = y0 - chy[ch], cdz = z0 - chz[ch];
                 if (P.boundary) {
                     cdx -= P.box[0] * rint(cdx * P.inv_box[0]);
                     cdy -= P.box[1] * rint(cdy * P.inv_box[1]);
@@ -530,7 +568,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                         for (int k = 0; k < W; ++k) {
                             if (!((amb >> k) & 1u)) continue;
                             double rx, ry, rz;
-                            nearest_image_exact(s, xi[k], yi[k], zi[k], tx[t], ty[t], tz[t], rx, ry, rz);
+                            nearest_image_exact(s, cxs[warp][0][k], cxs[warp][1][k], cxs[warp][2][k], tx[t], ty[t],
+                                                tz[t], rx, ry, rz);
                             const double e2 = len2_exact(rx, ry, rz);
                             if (!(e2 > P.c2l)) {
                                 if (e2 > P.c2s)
@@ -571,8 +610,13 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
     }
     if (!active) return;
     __syncwarp();
-    sort_write_entries(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
-    sort_write_entries(ebuf_l[warp], min(cnt_l, kEntBuf), outl, lane);
+    if (POPSORT) {
+        sort_write_entries_pop<W>(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
+        sort_write_entries_pop<W>(ebuf_l[warp], min(cnt_l, kEntBuf), outl, lane);
+    } else {
+        sort_write_entries(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
+        sort_write_entries(ebuf_l[warp], min(cnt_l, kEntBuf), outl, lane);
+    }
     if (lane == 0) {
         if (cnt_s > P.wcap || cnt_l > P.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
         s.wn_s[ci] = min(cnt_s, P.wcap);
@@ -768,4 +812,10 @@ __global__ void k_expand_cgpairs(const SysDev* __restrict__ sys, int long_range)
 }  // namespace gnb
 
 namespace gnb {
+}  // namespace gnb
+
+namespace gnb {
+template __global__ void k_water_search<4, false>(const SysDev*, const SearchParams);
+template __global__ void k_water_search<4, true>(const SysDev*, const SearchParams);
+template __global__ void k_water_search<8, true>(const SysDev*, const SearchParams);
 }  // namespace gnb

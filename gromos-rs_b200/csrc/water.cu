@@ -397,6 +397,260 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     }
 }
 
+// Bit-iterating layout: one warp per i-cluster of W waters, one lane per
+// j-water entry; each lane loops over the set bits of its own mask only, so
+// no lane idles on another lane's bits (entries are sorted by popcount, so
+// the lanes of a chunk run the same number of iterations).  The i atoms are
+// read from shared memory by bit index; i-forces accumulate in a lane-private
+// shared-memory row (no atomics, so the result does not depend on the order
+// of lanes) and the rows are summed once per cluster.
+template <int W, bool LJ00, bool LONG>
+__global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp) {
+    constexpr int ROW = W * 3 + 1;  // float4 per lane row (+1 keeps 8 consecutive lanes on distinct banks)
+    const SysDev& s = sys[blockIdx.y];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int nclus = s.n_clusters[0];
+    long long* __restrict__ FS = LONG ? s.fs_long : s.fs_short;
+    const uint32_t* __restrict__ wl = LONG ? s.wl_l : s.wl_s;
+    const int* __restrict__ wn = LONG ? s.wn_l : s.wn_s;
+    const float4* __restrict__ wrec4 = reinterpret_cast<const float4*>(s.wrec);
+    const int* __restrict__ clus_n = s.clus_n;
+    const int wcap = s.wcap;
+    float limx = wp.lim[0], limy = wp.lim[1], limz = wp.lim[2];
+    if (LONG) {
+        const float m = 2.f * (*s.max_delta) * 1.0001f + 1e-4f;
+        limx -= m;
+        limy -= m;
+        limz -= m;
+    }
+    extern __shared__ float4 dyn[];
+    float4* __restrict__ fis = dyn + static_cast<size_t>(wid) * 32 * ROW;  // [32][ROW]
+    float4* __restrict__ myrow = fis + lane * ROW;
+    __shared__ float4 sp_all[kWaterWarps][W * 3];
+    __shared__ float4 ibuf[kWaterWarps][2][W * 3];
+    __shared__ float4 jbuf[kWaterWarps][2][32 * 3];
+    float4* __restrict__ sp = sp_all[wid];
+#pragma unroll
+    for (int c = 0; c < W * 3; ++c) myrow[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    long long acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int stride = gridDim.x * kWaterWarps;
+    int ci = blockIdx.x * kWaterWarps + wid;
+    int ib = 0;
+    if (ci < nclus && lane < W * 3) cp_async16(&ibuf[wid][0][lane], wrec4 + 3 * (ci * W) + lane);
+    cp_async_commit();
+
+    for (; ci < nclus; ci += stride) {
+        const int n = clus_n[ci];
+        const int base = ci * W;
+        const int cnt = wn[ci];
+        const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * wcap;
+        uint32_t e_cur = lane < cnt ? __ldg(list + lane) : 0u;
+        uint32_t e_nx = 32 + lane < cnt ? __ldg(list + 32 + lane) : 0u;
+        cp_async_wait<0>();
+        __syncwarp();
+        const double x00 = rec_x(ibuf[wid][ib][0]), y00 = rec_y(ibuf[wid][ib][0]);
+        const double z00 = rec_x(ibuf[wid][ib][1]);
+        if (lane < W * 3) {
+            const int k = lane / 3, a = lane % 3;
+            float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < n) {
+                const float4 v0 = ibuf[wid][ib][3 * k], v1 = ibuf[wid][ib][3 * k + 1], v2 = ibuf[wid][ib][3 * k + 2];
+                const float dx = a == 0 ? 0.f : (a == 1 ? v1.z : v2.y);
+                const float dy = a == 0 ? 0.f : (a == 1 ? v1.w : v2.z);
+                const float dz = a == 0 ? 0.f : (a == 1 ? v2.x : v2.w);
+                p.x = float(rec_x(v0) - x00) + dx;
+                p.y = float(rec_y(v0) - y00) + dy;
+                p.z = float(rec_x(v1) - z00) + dz;
+            }
+            sp[lane] = p;
+        }
+        if (e_cur & 0xffu) {
+            const int js = static_cast<int>(e_cur >> 8);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][0][3 * lane + q], wrec4 + 3 * js + q);
+        }
+        cp_async_commit();
+        __syncwarp();
+        float elj = 0.f, ecrf = 0.f, v0s = 0.f, v1s = 0.f, v2s = 0.f, v3s = 0.f, v4s = 0.f, v5s = 0.f;
+        const int nch = (cnt + 31) >> 5;
+        for (int c = 0; c < nch; ++c) {
+            const int jb = c & 1;
+            if (c + 1 < nch && (e_nx & 0xffu)) {
+                const int js = static_cast<int>(e_nx >> 8);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][jb ^ 1][3 * lane + q], wrec4 + 3 * js + q);
+            }
+            cp_async_commit();
+            const int e2 = (c + 2) * 32 + lane;
+            const uint32_t e_nn = e2 < cnt ? __ldg(list + e2) : 0u;
+            cp_async_wait<1>();
+            __syncwarp();
+            unsigned mask = e_cur & 0xffu;
+            const int js = static_cast<int>(e_cur >> 8);
+            if (mask) {
+                const float4 r0 = jbuf[wid][jb][3 * lane], r1 = jbuf[wid][jb][3 * lane + 1], r2 = jbuf[wid][jb][3 * lane + 2];
+                double dx = x00 - rec_x(r0), dy = y00 - rec_y(r0), dz = z00 - rec_x(r1);
+                if (wp.boundary) {
+                    dx -= wp.box[0] * rint(dx * wp.inv_box[0]);
+                    dy -= wp.box[1] * rint(dy * wp.inv_box[1]);
+                    dz -= wp.box[2] * rint(dz * wp.inv_box[2]);
+                }
+                const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
+                const float qx[3] = {-Dx, r1.z - Dx, r2.y - Dx};
+                const float qy[3] = {-Dy, r1.w - Dy, r2.z - Dy};
+                const float qz[3] = {-Dz, r2.x - Dz, r2.w - Dz};
+                float gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
+                while (mask) {
+                    const int k = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const float4 p0 = sp[k * 3], p1 = sp[k * 3 + 1], p2 = sp[k * 3 + 2];
+                    float pxk[3] = {p0.x, p1.x, p2.x}, pyk[3] = {p0.y, p1.y, p2.y}, pzk[3] = {p0.z, p1.z, p2.z};
+                    float r0x = pxk[0] - qx[0], r0y = pyk[0] - qy[0], r0z = pzk[0] - qz[0];
+                    if (!(fabsf(r0x) < limx && fabsf(r0y) < limy && fabsf(r0z) < limz)) {
+                        float shx = 0.f, shy = 0.f, shz = 0.f;
+                        if (wp.boundary) {
+                            shx = -wp.boxf[0] * rintf(r0x * wp.inv_boxf[0]);
+                            shy = -wp.boxf[1] * rintf(r0y * wp.inv_boxf[1]);
+                            shz = -wp.boxf[2] * rintf(r0z * wp.inv_boxf[2]);
+                        }
+                        r0x += shx;
+                        r0y += shy;
+                        r0z += shz;
+                        if (!(fabsf(r0x) < limx && fabsf(r0y) < limy && fabsf(r0z) < limz)) {
+                            const int d = atomicAdd(&s.n_deferred[LONG ? 1 : 0], 1);
+                            if (d < s.defer_cap) {
+                                s.deferred[2 * (LONG ? s.defer_cap + d : d)] = base + k;
+                                s.deferred[2 * (LONG ? s.defer_cap + d : d) + 1] = js;
+                            } else {
+                                atomicOr(&s.err[0], ERR_DEFER_OVERFLOW);
+                            }
+                            continue;
+                        }
+#pragma unroll
+                        for (int a = 1; a < 3; ++a) {
+                            pxk[a] += shx;
+                            pyk[a] += shy;
+                            pzk[a] += shz;
+                        }
+                    }
+                    float fx[3] = {0.f, 0.f, 0.f}, fy[3] = {0.f, 0.f, 0.f}, fz[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+#pragma unroll
+                        for (int b = 0; b < 3; ++b) {
+                            const int t = a * 3 + b;
+                            const float x = (a == 0 && b == 0) ? r0x : pxk[a] - qx[b];
+                            const float y = (a == 0 && b == 0) ? r0y : pyk[a] - qy[b];
+                            const float z = (a == 0 && b == 0) ? r0z : pzk[a] - qz[b];
+                            const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+                            const float ri = r2 < 1e-10f ? 0.f : rsqrt_fast(r2);
+                            const float ri2 = ri * ri;
+                            const float q = wp.qq[t];
+                            ecrf = fmaf(q, fmaf(-wp.crf2, r2, ri) - wp.crfc, ecrf);
+                            float fs = q * fmaf(ri, ri2, wp.crf3);
+                            if (!LJ00 || t == 0) {
+                                const float ri6 = ri2 * ri2 * ri2;
+                                elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, elj);
+                                fs = fmaf(fmaf(12.f * wp.c12[t], ri6, -6.f * wp.c6[t]), ri6 * ri2, fs);
+                            }
+                            const float fxx = x * fs, fyy = y * fs, fzz = z * fs;
+                            fx[a] += fxx;
+                            fy[a] += fyy;
+                            fz[a] += fzz;
+                            gx[b] -= fxx;
+                            gy[b] -= fyy;
+                            gz[b] -= fzz;
+                            v0s = fmaf(x, fxx, v0s);
+                            v1s = fmaf(x, fyy, v1s);
+                            v2s = fmaf(x, fzz, v2s);
+                            v3s = fmaf(y, fyy, v3s);
+                            v4s = fmaf(y, fzz, v4s);
+                            v5s = fmaf(z, fzz, v5s);
+                        }
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        float4 f = myrow[k * 3 + a];
+                        f.x += fx[a];
+                        f.y += fy[a];
+                        f.z += fz[a];
+                        myrow[k * 3 + a] = f;
+                    }
+                }
+                long long* __restrict__ fj = FS + static_cast<size_t>(js) * 9;
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    red_add(fj + 3 * b, to_fixed_f(gx[b], 4294967296.0f));
+                    red_add(fj + 3 * b + 1, to_fixed_f(gy[b], 4294967296.0f));
+                    red_add(fj + 3 * b + 2, to_fixed_f(gz[b], 4294967296.0f));
+                }
+            }
+            e_cur = e_nx;
+            e_nx = e_nn;
+            __syncwarp();
+        }
+        const int cn = ci + stride;
+        if (cn < nclus && lane < W * 3) cp_async16(&ibuf[wid][ib ^ 1][lane], wrec4 + 3 * (cn * W) + lane);
+        cp_async_commit();
+        __syncwarp();
+        // column sums of the lane rows: lane c < 3W owns i atom c (water c / 3)
+        if (lane < W * 3) {
+            float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll 8
+            for (int r = 0; r < 32; ++r) {
+                const float4 f = fis[r * ROW + lane];
+                sx += f.x;
+                sy += f.y;
+                sz += f.z;
+            }
+            if (lane / 3 < n) {
+                long long* __restrict__ fo = FS + static_cast<size_t>(base) * 9 + 3 * lane;
+                red_add(fo, to_fixed_f(sx, 4294967296.0f));
+                red_add(fo + 1, to_fixed_f(sy, 4294967296.0f));
+                red_add(fo + 2, to_fixed_f(sz, 4294967296.0f));
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int cc = 0; cc < W * 3; ++cc) myrow[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
+        acc[0] += to_fixed_f(elj, 16777216.0f);
+        acc[1] += to_fixed_f(ecrf, 16777216.0f);
+        acc[2] += to_fixed_f(v0s, 16777216.0f);
+        acc[3] += to_fixed_f(v1s, 16777216.0f);
+        acc[4] += to_fixed_f(v2s, 16777216.0f);
+        acc[5] += to_fixed_f(v3s, 16777216.0f);
+        acc[6] += to_fixed_f(v4s, 16777216.0f);
+        acc[7] += to_fixed_f(v5s, 16777216.0f);
+        ib ^= 1;
+        __syncwarp();
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) acc[v] = warp_sum_ll(acc[v]);
+    __shared__ unsigned long long sh[8];
+    if (threadIdx.x < 8) sh[threadIdx.x] = 0ull;
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+            if (acc[v]) atomicAdd(&sh[v], static_cast<unsigned long long>(acc[v]));
+    __syncthreads();
+    if (threadIdx.x < 8 && sh[threadIdx.x]) {
+        long long* dst = LONG ? s.acc_long : s.acc_short;
+        const int G = wp.G, vb = 2 * G * G;
+        const int v = threadIdx.x;
+        const int i0 = v == 0 ? wp.slot : v == 1 ? G * G + wp.slot : vb + (v == 2 ? 0 : v == 3 ? 1 : v == 4 ? 2 : v == 5 ? 4 : v == 6 ? 5 : 8);
+        const int i1 = v == 3 ? vb + 3 : v == 4 ? vb + 6 : v == 6 ? vb + 7 : -1;
+        atomicAdd(reinterpret_cast<unsigned long long*>(dst + i0), sh[v]);
+        if (i1 >= 0) atomicAdd(reinterpret_cast<unsigned long long*>(dst + i1), sh[v]);
+    }
+}
+
+template <int W>
+constexpr size_t water_it_smem() {
+    return size_t(kWaterWarps) * 32 * (W * 3 + 1) * sizeof(float4);
+}
+
 // CG pairs the main kernel deferred: exact FP64 images (first-atom shift for
 // the short list, per-atom images for the long list), FP32 pair arithmetic.
 template <bool LJ00, bool LONG>
@@ -440,4 +694,15 @@ template __global__ void k_water_force<true, true>(const SysDev*, const WaterPar
 template __global__ void k_water_force<false, false>(const SysDev*, const WaterParams);
 template __global__ void k_water_force<false, true>(const SysDev*, const WaterParams);
 
+}  // namespace gnb
+
+namespace gnb {
+template __global__ void k_water_force_it<4, true, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<4, true, true>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<4, false, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<4, false, true>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<8, true, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<8, true, true>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<8, false, false>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<8, false, true>(const SysDev*, const WaterParams);
 }  // namespace gnb

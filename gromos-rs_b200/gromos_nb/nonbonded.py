@@ -100,13 +100,15 @@ class _TopologyStruct:
         self.struct = s
 
 
-def make_params(p: NonbondedParams, kernel: str = "fixed") -> _lib.GrNbParams:
+def make_params(p: NonbondedParams, kernel: str = "fixed", cluster_size: int = 0,
+                water_layout: int = 0) -> _lib.GrNbParams:
     q = _lib.GrNbParams()
     q.rcutp, q.rcutl, q.skin = p.rcutp, p.rcutl, p.skin
     q.epsilon, q.epsrf, q.kappa = p.epsilon, p.epsrf, p.kappa
     q.nsnb, q.boundary, q.lam, q.nlam = p.nsnb, p.boundary, p.lam, p.nlam
     q.kernel = KERNELS[kernel]
-    q.cluster_size = 0
+    q.cluster_size = cluster_size
+    q.water_layout = water_layout
     return q
 
 
@@ -118,7 +120,8 @@ class Forcefield:
     first step), later calls rebuild it every ``nsnb`` calls.
     """
 
-    def __init__(self, system: System, kernel: str = "fixed", device: int = 0):
+    def __init__(self, system: System, kernel: str = "fixed", device: int = 0, cluster_size: int = 0,
+                 water_layout: int = 0):
         L = _lib.lib()
         self._L = L
         self.system = system
@@ -128,7 +131,7 @@ class Forcefield:
         self._h = h
         self._topo = _TopologyStruct(system.topo)
         check(L.gr_system_upload(h, C.byref(self._topo.struct)))
-        self._params = make_params(system.params, kernel)
+        self._params = make_params(system.params, kernel, cluster_size, water_layout)
         check(L.gr_set_params(h, C.byref(self._params)))
         self.set_box(system.box)
         self.n_atoms = system.topo.n_atoms
