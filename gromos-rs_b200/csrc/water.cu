@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                             continue;
                         }
 #pragma unroll
-                        for (int a = 1; a < 3; ++a) {
+                        for (int a = 0; a < 3; ++a) {  // r0 already carries the shift
                             pxk[a] += shx;
                             pyk[a] += shy;
                             pzk[a] += shz;
