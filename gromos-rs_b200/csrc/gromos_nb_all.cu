@@ -4,3 +4,4 @@
 #include "forces.cu"
 #include "water.cu"
 #include "api.cu"
+#include "noalloc.cu"

@@ -95,6 +95,10 @@ _SIGNATURES = {
     "gr_last_timings": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
     "gr_ctx_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_ffma_peak": (C.c_int32, [C.c_int, C.POINTER(C.c_double)]),
+    "gr_lj_crf_innerloop_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                                C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                                C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_void_p]),
 }
 
 

@@ -198,6 +198,31 @@ gr_status gr_lj_crf_innerloop(const float* positions, const float* charges, cons
                               uint32_t boundary_type, double crf_cut, double crf_2cut3i,
                               double crf_cut3i, float* forces, double* energies, double* virial);
 
+/* ---- allocation-free variant (no counterpart in gromos-rs) -------------- */
+/* gr_lj_crf_innerloop on DEVICE buffers, enqueued on `stream` (a
+ * cudaStream_t; NULL = legacy default stream) of the calling thread's current
+ * device, without allocating device memory: for callers that cannot call
+ * cudaMalloc while forces are computed (an integrator recorded into a CUDA
+ * graph, a loop that must not wait on the allocator, a host program whose
+ * device memory belongs to another allocator).  All inputs and outputs are
+ * device pointers with the meaning of gr_lj_crf_innerloop (lj_params is the
+ * double (c6, c12) table), except box_data: 3 doubles of host memory, read
+ * during the call and passed to the kernel by value.  Its scratch (the FP32 table and the energy /
+ * virial accumulators) is one static device array per GPU, sized for at most
+ * 64 atom types: n_types > 64 returns GR_ERR_INVALID.  The first call on a
+ * device looks the array's address up (cudaGetSymbolAddress) and must come
+ * before any stream capture on that device.  forces are cleared by the call;
+ * energies[2] and virial[9] are overwritten.  Pair indices (< n_atoms) and
+ * iac values (< n_types) are the caller's to guarantee: they stay on the
+ * device and are not checked.  Calls whose work may overlap on the GPU share
+ * the scratch and race: order them on one stream. */
+gr_status gr_lj_crf_innerloop_noalloc(const float* positions, const float* charges, const uint32_t* iac,
+                                      uint32_t n_atoms, const uint32_t* pairlist, uint32_t n_pairs,
+                                      const double* lj_params, uint32_t n_types, const double* box_data,
+                                      uint32_t boundary_type, double crf_cut, double crf_2cut3i,
+                                      double crf_cut3i, float* forces, double* energies, double* virial,
+                                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif
