@@ -39,6 +39,10 @@ DT_PS = 0.002
 OPS_PER_PAIR = 37          # FP32 pipe ops per atom pair, energies + virial step
 METRIC = "pair-int/s"
 WORKLOAD = "spc30000_twinrange_0.8_1.4_nsnb5"
+# DRAM bytes (read + write) of one short-range water-kernel launch on this
+# workload, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum;
+# profiles/water_force_it_spc30000_short.md)
+SHORT_KERNEL_DRAM_BYTES = 6.75e6
 
 
 def ns_per_day(ms_per_step: float) -> float:
@@ -265,9 +269,10 @@ def run_gpu(args, rank, world, local_rank):
                           "step": "force evaluation only (positions static; MD integration not timed)",
                           "parallelism": "replicas" if world > 1 else "single system"},
                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-               "roofline": {"bound": "fp32", "kernel": "k_water_force (short range) + k_water_prep",
+               "roofline": {"bound": "fp32",
+                            "kernel": "short-range window: k_water_prep + k_water_force_it + k_water_deferred",
                             "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s (FP32 pipe)",
-                            "frac": achieved / peak, "traffic": None,
+                            "frac": achieved / peak, "traffic": SHORT_KERNEL_DRAM_BYTES,
                             "peak_source": "measured FFMA-chain kernel (gr_ffma_peak), one FFMA = one op",
                             "ops_per_pair": OPS_PER_PAIR, "short_kernel_ms": t_short,
                             "long_kernel_ms": statistics.median(long_ms) if long_ms else None},

@@ -418,7 +418,7 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
     // water kernel layout: 1 = lanes share the mask bits (width 4 only),
     // 2 = each lane iterates over its own bits (width 4 or 8)
     layout = p->water_layout == 1 ? 1 : 2;
-    W = (layout == 2 && p->cluster_size == 4) ? 4 : (layout == 1 ? 4 : 8);
+    W = (layout == 2 && p->cluster_size == 8) ? 8 : 4;
     if (p->cluster_size != 0 && p->cluster_size != 4 && p->cluster_size != 8) {
         set_error("gr_nb_params: cluster_size must be 0, 4 or 8");
         return GR_ERR_INVALID;
@@ -763,7 +763,6 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         if (NCG > NSCG) {
             wp = water_params();
             (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
-            unsigned grid = unsigned(sm * water_blocks_per_sm);
             GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 2 * sizeof(int), s));
             if ((st = launch_water(s, wp, false))) return st;
         }
@@ -776,7 +775,6 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
                 GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
             if (NCG > NSCG) {
                 WaterParams wpl = water_params(true);
-                unsigned grid = unsigned(sm * water_blocks_per_sm);
                 if ((st = launch_water(s, wpl, true))) return st;
             }
             if (NSCG > 0) (++launches, k_solute_force<true><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
@@ -848,26 +846,37 @@ WaterParams NbSystem::water_params(bool long_range) const {
 // deferred-pair kernel.
 gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr) {
     const int sm = sm_count();
-    const unsigned grid = unsigned(sm * water_blocks_per_sm);
     const bool lj00 = h.water_lj00_only != 0;
+    // The water kernels are persistent (grid-stride over i-clusters): the grid
+    // is exactly one wave, SMs x resident blocks per SM, so that no block
+    // starts after the first ones have finished their share.
 #define GR_WATER_IT(WW, LJ, LL)                                                                          \
     do {                                                                                                 \
         const size_t smem = water_it_smem<WW>();                                                         \
-        static bool attr_set = false;                                                                    \
-        if (!attr_set) {                                                                                 \
+        static int occ = 0;                                                                              \
+        if (!occ) {                                                                                      \
             GR_CUDA(cudaFuncSetAttribute(k_water_force_it<WW, LJ, LL>,                                   \
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));       \
-            attr_set = true;                                                                             \
+            GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_water_force_it<WW, LJ, LL>,    \
+                                                                  128, smem));                           \
+            if (occ < 1) occ = 1;                                                                        \
         }                                                                                                \
-        (++launches, k_water_force_it<WW, LJ, LL><<<grid, 128, smem, s>>>(d_sys, wp));                   \
+        (++launches, k_water_force_it<WW, LJ, LL><<<unsigned(sm * occ), 128, smem, s>>>(d_sys, wp));     \
+    } while (0)
+#define GR_WATER_SHARED(LJ, LL)                                                                          \
+    do {                                                                                                 \
+        static int occ = 0;                                                                              \
+        if (!occ) {                                                                                      \
+            GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_water_force<LJ, LL>, 128, 0)); \
+            if (occ < 1) occ = 1;                                                                        \
+        }                                                                                                \
+        (++launches, k_water_force<LJ, LL><<<unsigned(sm * occ), 128, 0, s>>>(d_sys, wp));               \
     } while (0)
     if (layout == 1) {
         if (lj00) {
-            if (lr) (++launches, k_water_force<true, true><<<grid, 128, 0, s>>>(d_sys, wp));
-            else (++launches, k_water_force<true, false><<<grid, 128, 0, s>>>(d_sys, wp));
+            if (lr) GR_WATER_SHARED(true, true); else GR_WATER_SHARED(true, false);
         } else {
-            if (lr) (++launches, k_water_force<false, true><<<grid, 128, 0, s>>>(d_sys, wp));
-            else (++launches, k_water_force<false, false><<<grid, 128, 0, s>>>(d_sys, wp));
+            if (lr) GR_WATER_SHARED(false, true); else GR_WATER_SHARED(false, false);
         }
     } else if (W == 4) {
         if (lj00) {
@@ -883,6 +892,7 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
         }
     }
 #undef GR_WATER_IT
+#undef GR_WATER_SHARED
     if (lj00) {
         if (lr) (++launches, k_water_deferred<true, true><<<sm, 128, 0, s>>>(d_sys, wp));
         else (++launches, k_water_deferred<true, false><<<sm, 128, 0, s>>>(d_sys, wp));

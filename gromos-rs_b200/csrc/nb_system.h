@@ -52,7 +52,6 @@ class NbSystem {
     int steps_since_update = 0;
     int n_cgp_host[2] = {0, 0};
     long long pairs_short = 0, pairs_long = 0;
-    int water_blocks_per_sm = 4;
     long long launches = 0;  // kernels launched by this system
     // capacities
     int cells_alloc = 0, clus_alloc = 0, wcap_alloc = 0, scap_alloc = 0, pcap_alloc = 0, cgp_alloc = 0;

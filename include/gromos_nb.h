@@ -107,7 +107,7 @@ typedef struct {
     double lambda;               /* RLAM */
     int32_t nlam;                /* NLAM */
     int32_t kernel;              /* GR_KERNEL_* */
-    int32_t cluster_size;        /* solvent i-cluster width 4 or 8 (0 = default) */
+    int32_t cluster_size;        /* solvent i-cluster width 4 or 8 (0 = 4) */
     int32_t water_layout;        /* 0 default, 1 lanes share mask bits (width 4), 2 lanes iterate own bits */
 } gr_nb_params;
 

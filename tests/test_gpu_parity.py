@@ -78,8 +78,9 @@ def test_pairlist_bit_exact_spc30000_twin_range():
     check_pairlist(generators.config2_spc30000())
 
 
-def compare_eval(s, kernel="fixed", steps=1, tol_rms=1e-5, tol_e=1e-5, move=0.0, seed=0):
-    ff = Forcefield(s, kernel=kernel)
+def compare_eval(s, kernel="fixed", steps=1, tol_rms=1e-5, tol_e=1e-5, move=0.0, seed=0, cluster_size=0,
+                 layout=0):
+    ff = Forcefield(s, kernel=kernel, cluster_size=cluster_size, water_layout=layout)
     orc = ob.OracleForcefield(s)
     rng = np.random.default_rng(seed)
     pos = s.pos.copy()
@@ -144,6 +145,24 @@ def test_fep_synthetic_windows():
 def test_solute_small_box_per_atom_images():
     s = generators.solvated_solute_system(500, 200, seed=1003, rc=1.4)
     compare_eval(s, "fixed", steps=3, move=0.002)
+
+
+WATER_KERNELS = [(1, 4), (2, 4), (2, 8)]
+
+
+@pytest.mark.parametrize("layout,width", WATER_KERNELS)
+@pytest.mark.parametrize("name", ["ch4_water_fep", "water_216_box", "nacl_3water_box", "water_3_box_twinrange"])
+def test_water_kernel_variants_fixtures(name, layout, width):
+    """Every solvent kernel variant (shared-bit width 4, per-lane-bit width 4 and 8) against the oracle."""
+    s, _ = load_fixture(name)
+    compare_eval(s, "fixed", cluster_size=width, layout=layout)
+
+
+@pytest.mark.parametrize("layout,width", WATER_KERNELS)
+def test_water_kernel_variants_twin_range_steps(layout, width):
+    s = generators.spc_water_system(1500, box=generators.box_for_waters(1500), seed=22, rcutp=0.8, rcutl=1.4,
+                                    nsnb=2)
+    compare_eval(s, "fixed", steps=4, move=0.002, seed=6, cluster_size=width, layout=layout)
 
 
 def test_deterministic_bits():
