@@ -171,6 +171,35 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_md(ff, s, args, generators):
+    """MD steps (force evaluation + leap-frog + SETTLE, device resident) for ns/day.
+
+    Timed with CUDA events on the library's stream around gr_md_run; the
+    runner synchronises once per pairlist period (overflow check), which is
+    inside the timed region.
+    """
+    import torch
+
+    mass = generators.masses(s)
+    vel = generators.maxwell_velocities(mass, 300.0, seed=2002)
+    ff.upload_positions(s.pos)
+    ff.md_init(mass, vel, dt=DT_PS, settle=True, dist_oh=0.1, dist_hh=generators.SPC_DHH)
+    ff.md_run(max(args.warmup, 3) * 5)
+    n = max(args.md_steps, 1)
+    stream = torch.cuda.ExternalStream(ff.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    st = ff.md_run(n)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"steps": n, "dt_ps": DT_PS, "ms_per_step": ms / n, "ns_per_day": ns_per_day(ms / n),
+            "settle": True, "settle_failures": st["settle_failures"], "rollbacks": st["rollbacks"],
+            "e_kin_final": st["e_kin"], "start": "seeded Maxwell-Boltzmann velocities at 300 K"}
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
 
@@ -249,6 +278,7 @@ def run_gpu(args, rank, world, local_rank):
     e2e_value = e2e_pairs * world / e2e_s
     h2d = s.topo.n_atoms * 3 * 8
     d2h = s.topo.n_atoms * 3 * 8 + 8 * (2 * ff.G * ff.G + 10)
+    md = run_md(ff, s, args, generators)
     out = None
     if rank == 0:
         peak = ffma_peak(local_rank)
@@ -258,7 +288,7 @@ def run_gpu(args, rank, world, local_rank):
         if not args.no_cpu_baseline:
             cpu = cpu_baseline_sample()
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms_per_step, "ns_per_day": ns_per_day(ms_per_step) * 1.0,
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "ns_per_day": md["ns_per_day"],
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64",
                "data": "synthetic (seeded SPC water box)",
                "config": {"workload": WORKLOAD, "n_atoms": s.topo.n_atoms, "box_nm": 9.65, "rcutp": 0.8,
@@ -266,7 +296,7 @@ def run_gpu(args, rank, world, local_rank):
                           "water_layout": args.layout, "pairs_short_per_step": n_short,
                           "pairs_long_per_rebuild": n_long, "rebuild_steps_timed": rebuilds,
                           "l2": "flushed (256 MiB write) between steps, outside the step events",
-                          "step": "force evaluation only (positions static; MD integration not timed)",
+                          "step": "value: force evaluation (positions static); md: force evaluation + leap-frog + SETTLE",
                           "parallelism": "replicas" if world > 1 else "single system"},
                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "roofline": {"bound": "fp32",
@@ -276,7 +306,7 @@ def run_gpu(args, rank, world, local_rank):
                             "peak_source": "measured FFMA-chain kernel (gr_ffma_peak), one FFMA = one op",
                             "ops_per_pair": OPS_PER_PAIR, "short_kernel_ms": t_short,
                             "long_kernel_ms": statistics.median(long_ms) if long_ms else None},
-               "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
+               "md": md, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
         print(json.dumps(out), flush=True)
     ff.close()
     return 0
@@ -285,12 +315,13 @@ def run_gpu(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--kernel", default="fixed", choices=["fixed", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cluster-size", type=int, default=0, help="water i-cluster width 4 or 8 (0 = default)")
+    ap.add_argument("--md-steps", type=int, default=1000, help="MD steps timed for ns/day")
     ap.add_argument("--layout", type=int, default=0, help="water kernel layout: 1 shared bits, 2 per-lane bits")
     args = ap.parse_args()
     if args.warmup < 3:

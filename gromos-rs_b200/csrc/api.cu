@@ -103,6 +103,15 @@ void NbSystem::release() {
     if (err_host) cudaFreeHost(err_host);
     err_host = nullptr;
     pending_check = false;
+    // MD buffers were freed with `allocs`
+    md_vel = md_mass = md_inv_mass = md_pos_snap = md_vel_snap = nullptr;
+    md_ke = nullptr;
+    md_fail = nullptr;
+    if (md_err_host) cudaFreeHost(md_err_host);
+    md_err_host = nullptr;
+    if (ev_md) cudaEventDestroy(ev_md);
+    ev_md = nullptr;
+    md_ready = false;
 }
 
 // (Re)allocates *p; a previous allocation made through alloc() is freed.

@@ -4,4 +4,5 @@
 #include "forces.cu"
 #include "water.cu"
 #include "api.cu"
+#include "md.cu"
 #include "noalloc.cu"

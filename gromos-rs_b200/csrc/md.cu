@@ -1,0 +1,346 @@
+// md.cu -- MD steps around the force evaluation, device resident.
+//
+// One step is the sequence of gromos-md's md binary (md.rs:1144-1230) without
+// thermostat: Forcefield::apply (the nonbonded path of this library) at r(t),
+// leap-frog velocity v(t+dt/2) = v(t-dt/2) + F/m dt (leap_frog.rs:37-85),
+// leap-frog position r(t+dt) = r(t) + v dt (leap_frog.rs:116-148) and SETTLE
+// for every 3-site solvent molecule (constraints.rs:815-1010).  Positions,
+// velocities and forces never leave the device between steps.
+//
+// Overflow recovery: list overflows (pairlist capacity, deferred water pairs)
+// are detected after the fact from the device error flags.  The runner keeps
+// a device snapshot of (positions, velocities) at the start of every pairlist
+// period (the steps between two rebuilds), reads the flags at the end of the
+// period, and on overflow grows the lists, restores the snapshot and runs the
+// period again, so an overflow never leaks into the trajectory.
+#include <cuda_runtime.h>
+
+namespace gnb {
+
+struct MdDev {
+    double* vel;              // n_atoms*3
+    const double* inv_mass;   // n_atoms
+    const double* mass;       // n_atoms
+    double dt, dt_i;
+    int settle;               // SETTLE every solvent molecule
+    double m_o, m_h, ra, rb, rc;  // canonical SETTLE triangle (constraints.rs:836-840)
+    long long* ke;            // [1] kinetic energy, fixed point 2^24
+    int* failures;            // [1] molecules SETTLE could not solve
+};
+
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ D3 d3(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator*(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double dot3(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross3(D3 a, D3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// SETTLE for one molecule (Miyamoto & Kollman 1992, eqs. A3-A17): the frame
+// is spanned by the old molecular plane and the new centre of mass; the
+// three rotation sines are solved analytically.  Velocities receive the
+// displacement / dt.  Returns false (molecule left unconstrained, as the
+// reference does) when a sine leaves [-1, 1].
+__device__ bool settle_molecule(const D3 old[3], D3 nw[3], D3 v[3], const MdDev& md) {
+    D3 b0 = old[1] - old[0], c0 = old[2] - old[0];
+    const double mt_i = 1.0 / (md.m_o + 2.0 * md.m_h);
+    const D3 d0 = (nw[0] * md.m_o + nw[1] * md.m_h + nw[2] * md.m_h) * mt_i;
+    D3 a1 = nw[0] - d0, b1 = nw[1] - d0, c1 = nw[2] - d0;
+    D3 n0 = cross3(b0, c0);
+    D3 n1 = cross3(a1, n0);
+    D3 n2 = cross3(n0, n1);
+    n0 = n0 * rsqrt(dot3(n0, n0));
+    n1 = n1 * rsqrt(dot3(n1, n1));
+    n2 = n2 * rsqrt(dot3(n2, n2));
+    b0 = d3(dot3(n1, b0), dot3(n2, b0), dot3(n0, b0));
+    c0 = d3(dot3(n1, c0), dot3(n2, c0), dot3(n0, c0));
+    a1 = d3(dot3(n1, a1), dot3(n2, a1), dot3(n0, a1));
+    b1 = d3(dot3(n1, b1), dot3(n2, b1), dot3(n0, b1));
+    c1 = d3(dot3(n1, c1), dot3(n2, c1), dot3(n0, c1));
+    const double sinphi = a1.z / md.ra;
+    const double omp = 1.0 - sinphi * sinphi;
+    if (omp < 0.0) return false;
+    const double cosphi = sqrt(omp);
+    const double sinpsi = (b1.z - c1.z) / (2.0 * md.rc * cosphi);
+    const double omq = 1.0 - sinpsi * sinpsi;
+    if (omq < 0.0) return false;
+    const double cospsi = sqrt(omq);
+    const double y_a2 = md.ra * cosphi, x_b2 = -md.rc * cospsi;
+    const double y_b2 = -md.rb * cosphi - md.rc * sinpsi * sinphi;
+    const double y_c2 = -md.rb * cosphi + md.rc * sinpsi * sinphi;
+    const double alpha = x_b2 * (b0.x - c0.x) + b0.y * y_b2 + c0.y * y_c2;
+    const double beta = x_b2 * (c0.y - b0.y) + b0.x * y_b2 + c0.x * y_c2;
+    const double gamma = b0.x * b1.y - b1.x * b0.y + c0.x * c1.y - c1.x * c0.y;
+    const double ab2 = alpha * alpha + beta * beta;
+    const double disc = ab2 - gamma * gamma;
+    if (disc < 0.0) return false;
+    const double sintheta = (alpha * gamma - beta * sqrt(disc)) / ab2;
+    const double omt = 1.0 - sintheta * sintheta;
+    if (omt < 0.0) return false;
+    const double costheta = sqrt(omt);
+    const D3 r3[3] = {d3(-y_a2 * sintheta, y_a2 * costheta, a1.z),
+                      d3(x_b2 * costheta - y_b2 * sintheta, x_b2 * sintheta + y_b2 * costheta, b1.z),
+                      d3(-x_b2 * costheta - y_c2 * sintheta, -x_b2 * sintheta + y_c2 * costheta, c1.z)};
+    // back to the lab frame: rows of the transposed basis
+    const D3 m1 = d3(n1.x, n2.x, n0.x), m2 = d3(n1.y, n2.y, n0.y), m0 = d3(n1.z, n2.z, n0.z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const D3 p = d3(dot3(r3[k], m1), dot3(r3[k], m2), dot3(r3[k], m0)) + d0;
+        const D3 d = p - nw[k];
+        nw[k] = p;
+        v[k] = v[k] + d * md.dt_i;
+    }
+    return true;
+}
+
+// One thread per unit: a solute atom (leap-frog only) or a solvent molecule
+// (leap-frog of its atoms, then SETTLE).  Forces are the finalized FP64
+// forces of this step's evaluation.
+__global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
+    const SysDev& s = *sys;
+    const int nsa = s.n_solute_atoms, n = s.n_atoms;
+    const int n_mol = md.settle ? (n - nsa) / 3 : 0;
+    const int n_units = md.settle ? nsa + n_mol : n;
+    long long ke = 0;
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n_units; u += gridDim.x * blockDim.x) {
+        const bool mol = md.settle && u >= nsa;
+        const int a0 = mol ? nsa + 3 * (u - nsa) : u;
+        const int na = mol ? 3 : 1;
+        D3 old[3], nw[3], v[3];
+        for (int k = 0; k < na; ++k) {
+            const int i = a0 + k;
+            const D3 f = d3(s.f_out[3 * i], s.f_out[3 * i + 1], s.f_out[3 * i + 2]);
+            const double im = md.inv_mass[i];
+            v[k] = d3(md.vel[3 * i], md.vel[3 * i + 1], md.vel[3 * i + 2]) + f * im * md.dt;
+            old[k] = d3(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2]);
+            nw[k] = old[k] + v[k] * md.dt;
+        }
+        if (mol && !settle_molecule(old, nw, v, md)) atomicAdd(md.failures, 1);
+        for (int k = 0; k < na; ++k) {
+            const int i = a0 + k;
+            s.pos[3 * i] = nw[k].x;
+            s.pos[3 * i + 1] = nw[k].y;
+            s.pos[3 * i + 2] = nw[k].z;
+            md.vel[3 * i] = v[k].x;
+            md.vel[3 * i + 1] = v[k].y;
+            md.vel[3 * i + 2] = v[k].z;
+            ke += to_fixed_d(0.5 * md.mass[i] * dot3(v[k], v[k]), kEnergyScale);
+        }
+    }
+    ke = warp_sum_ll(ke);
+    if ((threadIdx.x & 31) == 0 && ke) atomicAdd(reinterpret_cast<unsigned long long*>(md.ke),
+                                                  static_cast<unsigned long long>(ke));
+}
+
+}  // namespace gnb
+
+using namespace gnb;
+
+gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_params* p) {
+    if (!uploaded) {
+        set_error("gr_md_init before gr_system_upload");
+        return GR_ERR_STATE;
+    }
+    if (!mass || !p) {
+        set_error("gr_md_init: null mass or params");
+        return GR_ERR_INVALID;
+    }
+    if (!(p->dt > 0.0)) {
+        set_error("gr_md_init: dt must be positive");
+        return GR_ERR_INVALID;
+    }
+    for (int i = 0; i < N; ++i)
+        if (!(mass[i] > 0.0)) {
+            set_error("gr_md_init: every mass must be positive");
+            return GR_ERR_INVALID;
+        }
+    const bool settle = p->settle != 0 && N > NSA;
+    if (settle) {
+        if (aps != 3 || (N - NSA) % 3 != 0) {
+            set_error("gr_md_init: SETTLE needs 3-site solvent molecules");
+            return GR_ERR_UNSUPPORTED;
+        }
+        for (int i = NSA; i < N; i += 3)
+            if (mass[i] != mass[NSA] || mass[i + 1] != mass[NSA + 1] || mass[i + 2] != mass[NSA + 1]) {
+                set_error("gr_md_init: SETTLE needs one solvent with equal masses of sites 1 and 2");
+                return GR_ERR_UNSUPPORTED;
+            }
+        if (!(p->dist_oh > 0.0) || !(p->dist_hh > 0.0) || !(p->dist_hh < 2.0 * p->dist_oh)) {
+            set_error("gr_md_init: SETTLE lengths must satisfy 0 < dist_hh < 2 dist_oh");
+            return GR_ERR_INVALID;
+        }
+    }
+    std::vector<double> inv(N);
+    for (int i = 0; i < N; ++i) inv[i] = 1.0 / mass[i];
+    std::vector<double> v0(size_t(N) * 3, 0.0);
+    if (vel) std::copy(vel, vel + size_t(N) * 3, v0.begin());
+    gr_status st;
+    if ((st = upload_array(&md_mass, mass, N)) || (st = upload_array(&md_inv_mass, inv.data(), N)) ||
+        (st = upload_array(&md_vel, v0.data(), size_t(N) * 3)) || (st = alloc(&md_pos_snap, size_t(N) * 3)) ||
+        (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 1)) || (st = alloc(&md_fail, 1)))
+        return st;
+    if (!md_err_host) GR_CUDA(cudaMallocHost(&md_err_host, 8 * sizeof(long long)));
+    if (!ev_md) GR_CUDA(cudaEventCreateWithFlags(&ev_md, cudaEventDisableTiming));
+    mdp = *p;
+    md_settle = settle;
+    if (settle) {  // canonical triangle (constraints.rs:836-840)
+        md_m_o = mass[NSA];
+        md_m_h = mass[NSA + 1];
+        const double half_mo_div_mh = 0.5 * md_m_o / md_m_h;
+        md_rc = 0.5 * p->dist_hh;
+        md_ra = std::sqrt(p->dist_oh * p->dist_oh - md_rc * md_rc) / (1.0 + half_mo_div_mh);
+        md_rb = half_mo_div_mh * md_ra;
+    }
+    md_ready = true;
+    return GR_OK;
+}
+
+gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
+    if (!md_ready) {
+        set_error("gr_md_run before gr_md_init");
+        return GR_ERR_STATE;
+    }
+    if (n_steps < 0) {
+        set_error("gr_md_run: n_steps must be >= 0");
+        return GR_ERR_INVALID;
+    }
+    MdDev md;
+    md.vel = md_vel;
+    md.inv_mass = md_inv_mass;
+    md.mass = md_mass;
+    md.dt = mdp.dt;
+    md.dt_i = 1.0 / mdp.dt;
+    md.settle = md_settle ? 1 : 0;
+    md.m_o = md_m_o;
+    md.m_h = md_m_h;
+    md.ra = md_ra;
+    md.rb = md_rb;
+    md.rc = md_rc;
+    md.ke = md_ke;
+    md.failures = md_fail;
+    const int n_units = md_settle ? NSA + (N - NSA) / 3 : N;
+    const unsigned grid = std::max(1u, std::min(unsigned((n_units + 255) / 256), unsigned(sm_count() * 8)));
+    const size_t bytes3 = size_t(N) * 3 * sizeof(double);
+    GR_CUDA(cudaMemsetAsync(md_fail, 0, sizeof(int), s));
+    int done = 0, attempts = 0, rollbacks = 0;
+    gr_status st;
+    while (done < n_steps) {
+        // snapshot at the start of the period
+        GR_CUDA(cudaMemcpyAsync(md_pos_snap, h.pos, bytes3, cudaMemcpyDeviceToDevice, s));
+        GR_CUDA(cudaMemcpyAsync(md_vel_snap, md_vel, bytes3, cudaMemcpyDeviceToDevice, s));
+        const int ssu0 = steps_since_update;
+        bool overflow = false;
+        int k = 0;
+        for (;;) {
+            if (pending_check) {  // the flags of this period's rebuild
+                bool of = false;
+                if ((st = resolve_pending(&of))) return st;
+                if (of) {
+                    overflow = true;
+                    break;
+                }
+            }
+            if ((st = eval(s, 0, false))) return st;
+            GR_CUDA(cudaMemsetAsync(md_ke, 0, sizeof(long long), s));
+            (++launches, k_md_step<<<grid, 256, 0, s>>>(d_sys, md));
+            ++k;
+            if (done + k >= n_steps || steps_since_update >= prm.nsnb) break;
+        }
+        if (!overflow) {
+            // everything of this period (build and force kernels) has set its flags
+            GR_CUDA(cudaMemcpyAsync(md_err_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+            GR_CUDA(cudaEventRecord(ev_md, s));
+            GR_CUDA(cudaEventSynchronize(ev_md));
+            const int* e = reinterpret_cast<const int*>(md_err_host);
+            if (pending_check) {  // a rebuild at the period's last step: its flags are in e[0] too
+                pending_check = false;
+            }
+            if (e[0]) {
+                const int f = e[0];
+                GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
+                if (f & (ERR_CELL_TOO_DENSE | ERR_CG_TOO_LARGE)) {
+                    set_error(f & ERR_CELL_TOO_DENSE ? "pairlist: a grid cell holds more than 2048 charge groups"
+                                                     : "pairlist: solute charge group larger than 8 atoms");
+                    return GR_ERR_UNSUPPORTED;
+                }
+                if (f & ERR_WLIST_OVERFLOW) wcap_want = std::max(wcap_want, wcap_alloc) * 2;
+                if (f & ERR_SLIST_OVERFLOW) scap_want = std::max(scap_want, scap_alloc) * 2;
+                if (f & ERR_PERT_OVERFLOW) pcap_want = std::max(pcap_want, pcap_alloc) * 2;
+                if (f & ERR_DEFER_OVERFLOW) {
+                    defer_want = std::max(defer_want, h.defer_cap) * 4;
+                    clus_alloc = 0;
+                }
+                overflow = true;
+            }
+        }
+        if (overflow) {
+            if (++attempts > 8) {
+                set_error("md: list capacity could not be grown far enough");
+                return GR_ERR_OVERFLOW;
+            }
+            GR_CUDA(cudaMemcpyAsync(h.pos, md_pos_snap, bytes3, cudaMemcpyDeviceToDevice, s));
+            GR_CUDA(cudaMemcpyAsync(md_vel, md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, s));
+            steps_since_update = ssu0;
+            built = false;  // the period is re-run from a fresh build with the grown lists
+            lr_computed = false;
+            ++rollbacks;
+            continue;
+        }
+        attempts = 0;
+        done += k;
+    }
+    md_steps_total += done;
+    if (out) {
+        long long ke = 0;
+        int fails = 0;
+        std::vector<double> e(acc_size(G));
+        GR_CUDA(cudaMemcpyAsync(&ke, md_ke, sizeof(ke), cudaMemcpyDeviceToHost, s));
+        GR_CUDA(cudaMemcpyAsync(&fails, md_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GR_CUDA(cudaMemcpyAsync(e.data(), h.e_out, e.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        GR_CUDA(cudaStreamSynchronize(s));
+        double elj = 0.0, ecrf = 0.0;
+        for (int g = 0; g < G * G; ++g) {
+            elj += e[g];
+            ecrf += e[G * G + g];
+        }
+        out->steps = done;
+        out->e_lj = elj;
+        out->e_crf = ecrf;
+        out->e_kin = double(ke) / kEnergyScale;
+        out->settle_failures = fails;
+        out->rollbacks = rollbacks;
+    }
+    return GR_OK;
+}
+
+extern "C" {
+
+gr_status gr_md_init(gr_ctx* ctx, const double* mass, const double* vel, const gr_md_params* params) {
+    CTX_GUARD(ctx);
+    return ctx->sys.md_init(mass, vel, params);
+}
+
+gr_status gr_md_run(gr_ctx* ctx, int32_t n_steps, gr_md_stats* out) {
+    CTX_GUARD(ctx);
+    return ctx->sys.md_run(ctx->stream, n_steps, out);
+}
+
+gr_status gr_md_download(gr_ctx* ctx, double* pos, double* vel) {
+    CTX_GUARD(ctx);
+    NbSystem& S = ctx->sys;
+    if (!S.md_ready) {
+        set_error("gr_md_download before gr_md_init");
+        return GR_ERR_STATE;
+    }
+    const size_t bytes3 = size_t(S.N) * 3 * sizeof(double);
+    if (pos) GR_CUDA(cudaMemcpyAsync(pos, S.h.pos, bytes3, cudaMemcpyDeviceToHost, ctx->stream));
+    if (vel) GR_CUDA(cudaMemcpyAsync(vel, S.md_vel, bytes3, cudaMemcpyDeviceToHost, ctx->stream));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GR_OK;
+}
+
+}  // extern "C"

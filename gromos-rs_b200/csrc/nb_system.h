@@ -33,6 +33,8 @@ class NbSystem {
     int sm_count();
     WaterParams water_params(bool long_range = false) const;
     gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
+    gr_status md_init(const double* mass, const double* vel, const gr_md_params* p);
+    gr_status md_run(cudaStream_t s, int n_steps, gr_md_stats* out);
 
     // sizes
     int N = 0, NCG = 0, NSCG = 0, NSA = 0, NT = 0, G = 1, aps = 3, W = 4, layout = 2;
@@ -65,6 +67,17 @@ class NbSystem {
     bool pending_check = false, ever_built = false;
     bool solvent_excl_intra = false;
     bool fs_long_zeroed = false;  // solvent exclusions are exactly the molecule's other atoms
+    // MD state (md.cu)
+    bool md_ready = false, md_settle = false;
+    gr_md_params mdp{};
+    double md_m_o = 0, md_m_h = 0, md_ra = 0, md_rb = 0, md_rc = 0;
+    double *md_vel = nullptr, *md_mass = nullptr, *md_inv_mass = nullptr;
+    double *md_pos_snap = nullptr, *md_vel_snap = nullptr;
+    long long* md_ke = nullptr;
+    int* md_fail = nullptr;
+    long long* md_err_host = nullptr;  // pinned
+    cudaEvent_t ev_md = nullptr;
+    long long md_steps_total = 0;
 
    private:
     template <class T>

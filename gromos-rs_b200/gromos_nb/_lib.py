@@ -74,6 +74,15 @@ class GrResult(C.Structure):
     ]
 
 
+class GrMdParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("settle", C.c_int32), ("dist_oh", C.c_double), ("dist_hh", C.c_double)]
+
+
+class GrMdStats(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("e_lj", C.c_double), ("e_crf", C.c_double), ("e_kin", C.c_double),
+                ("settle_failures", C.c_int32), ("rollbacks", C.c_int32)]
+
+
 # symbol -> (restype, argtypes)
 _SIGNATURES = {
     "gr_ctx_create": (C.c_int32, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -95,6 +104,9 @@ _SIGNATURES = {
     "gr_last_timings": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
     "gr_ctx_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_ffma_peak": (C.c_int32, [C.c_int, C.POINTER(C.c_double)]),
+    "gr_md_init": (C.c_int32, [C.c_void_p, _f64p, _f64p, C.POINTER(GrMdParams)]),
+    "gr_md_run": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrMdStats)]),
+    "gr_md_download": (C.c_int32, [C.c_void_p, _f64p, _f64p]),
     "gr_lj_crf_innerloop_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                                 C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                                 C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,

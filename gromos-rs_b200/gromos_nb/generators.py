@@ -247,3 +247,26 @@ def config1_spc1000(seed: int = 1001) -> System:
 def config2_spc30000(seed: int = 1002) -> System:
     """30000 SPC waters, 9.65 nm box, twin range 0.8/1.4 nm, EPSRF 61, NSNB 5."""
     return spc_water_system(30000, 9.65, seed, rcutp=0.8, rcutl=1.4, epsrf=61.0, nsnb=5, name="spc30000")
+
+
+# ---- MD inputs ---------------------------------------------------------------
+SPC_MASS = (15.9994, 1.008, 1.008)     # O, H, H (amu)
+SOLUTE_MASS = 12.011                   # synthetic solute atoms (amu)
+SPC_DHH = 2.0 * OH * math.sin(HOH / 2.0)   # H-H distance of the rigid SPC triangle (nm)
+BOLTZ = 0.00831446261815324            # kJ mol^-1 K^-1
+
+
+def masses(system: System) -> np.ndarray:
+    """Per-atom masses: SPC masses for solvent atoms, 12.011 for solute atoms."""
+    t = system.topo
+    m = np.full(t.n_atoms, SOLUTE_MASS)
+    n_w = (t.n_atoms - t.n_solute_atoms) // 3
+    m[t.n_solute_atoms:] = np.tile(SPC_MASS, n_w)
+    return m
+
+
+def maxwell_velocities(mass: np.ndarray, temperature: float, seed: int) -> np.ndarray:
+    """Seeded Maxwell-Boltzmann velocities (nm/ps), sigma = sqrt(k_B T / m) per component."""
+    rng = np.random.default_rng(seed)
+    sig = np.sqrt(BOLTZ * temperature / np.asarray(mass, dtype=np.float64))
+    return rng.normal(size=(len(mass), 3)) * sig[:, None]

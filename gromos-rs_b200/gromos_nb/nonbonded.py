@@ -205,6 +205,33 @@ class Forcefield:
         check(self._L.gr_forces_device(self._h, C.byref(p)))
         return int(p.value)
 
+    # ---- MD (leap-frog + SETTLE around the force call, device resident)
+    def md_init(self, mass, vel=None, dt: float = 0.002, settle: bool = True, dist_oh: float = 0.1,
+                dist_hh: float = 0.1633) -> None:
+        """Positions are those of the last upload; ``vel`` are v(-dt/2) (None = zero)."""
+        m = np.ascontiguousarray(mass, dtype=np.float64)
+        v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64)
+        if m.shape != (self.n_atoms,) or (v is not None and v.shape != (self.n_atoms, 3)):
+            raise ValueError("mass must be (n_atoms,), vel (n_atoms, 3)")
+        self._md_mass, self._md_vel = m, v
+        mp = _lib.GrMdParams(dt, 1 if settle else 0, dist_oh, dist_hh)
+        check(self._L.gr_md_init(self._h, _p(m, C.c_double), _p(v, C.c_double), C.byref(mp)))
+
+    def md_run(self, n_steps: int) -> Dict:
+        st = _lib.GrMdStats()
+        check(self._L.gr_md_run(self._h, int(n_steps), C.byref(st)))
+        return {"steps": st.steps, "e_lj": st.e_lj, "e_crf": st.e_crf, "e_kin": st.e_kin,
+                "settle_failures": st.settle_failures, "rollbacks": st.rollbacks}
+
+    def md_run_async(self, n_steps: int) -> None:
+        check(self._L.gr_md_run(self._h, int(n_steps), None))
+
+    def md_state(self):
+        x = np.zeros((self.n_atoms, 3))
+        v = np.zeros((self.n_atoms, 3))
+        check(self._L.gr_md_download(self._h, _p(x, C.c_double), _p(v, C.c_double)))
+        return x, v
+
     # ---- pairlist
     def build_pairlist(self) -> None:
         check(self._L.gr_pairlist_build(self._h))

@@ -184,6 +184,36 @@ gr_status gr_ctx_launches(gr_ctx* ctx, int64_t* n);
  * FFMA counts as one operation (the force kernel's operation convention). */
 gr_status gr_ffma_peak(int device, double* ops_per_s);
 
+/* ---- MD steps around the force call ------------------------------------- */
+/* The step sequence of gromos-md's md binary without thermostat
+ * (crates/gromos-md/src/bin/md.rs:1144-1230): Forcefield::apply at r(t),
+ * LeapFrogVelocity (crates/gromos-integrators/src/algorithms/leap_frog.rs:37-85),
+ * LeapFrogPosition (:116-148) and SETTLE of every solvent molecule
+ * (crates/gromos-integrators/src/constraints.rs:815-1010), all on the
+ * device; positions and velocities stay resident between calls. */
+typedef struct {
+    double dt;        /* time step, ps */
+    int32_t settle;   /* 1: SETTLE every 3-site solvent molecule */
+    double dist_oh;   /* SETTLE constraint lengths, nm (solvent_constraint_template 0 and 2) */
+    double dist_hh;
+} gr_md_params;
+
+typedef struct {
+    int64_t steps;            /* steps done by the call */
+    double e_lj, e_crf;       /* nonbonded energies of the last force evaluation */
+    double e_kin;             /* sum 0.5 m v^2 of the last half-step velocities */
+    int32_t settle_failures;  /* molecules SETTLE could not solve (left as moved, as the reference) */
+    int32_t rollbacks;        /* pairlist periods re-run after a list overflow */
+} gr_md_stats;
+
+/* masses: n_atoms (all > 0); vel: n_atoms*3 initial v(-dt/2) or NULL (zero).
+ * Positions are those of the last gr_positions_upload. */
+gr_status gr_md_init(gr_ctx* ctx, const double* mass, const double* vel, const gr_md_params* params);
+/* Runs n_steps MD steps on the context's stream; out may be NULL. */
+gr_status gr_md_run(gr_ctx* ctx, int32_t n_steps, gr_md_stats* out);
+/* Current positions and velocities (either may be NULL). */
+gr_status gr_md_download(gr_ctx* ctx, double* pos, double* vel);
+
 /* ---- reference FFI stub replacement ------------------------------------ */
 /* Replaces `rust_lj_crf_innerloop` (crates/gromos-core/src/ffi.rs:55-103):
  * lj_crf_innerloop over an explicit atom-pair list with per-atom nearest

@@ -1156,3 +1156,115 @@ void orc_perturbed_pair(const double r[3], double a_c6, double a_c12, double b_c
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// MD step around Forcefield::apply, the sequence of gromos-md/src/bin/md.rs
+// (:1144-1230) without thermostat: forces at r(t); leap-frog velocity
+// v(t+dt/2) = v(t-dt/2) + F/m dt (leap_frog.rs:37-85); leap-frog position
+// r(t+dt) = r(t) + v dt (leap_frog.rs:116-148); SETTLE of every solvent
+// molecule (crates/gromos-integrators/src/constraints.rs:815-1010).
+namespace {
+inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline double vlen(V3 a) { return std::sqrt(dot(a, a)); }
+
+// SETTLE (Miyamoto & Kollman 1992) for one molecule, following
+// constraints.rs:857-975: canonical triangle, frame from the old plane and the
+// new centre of mass, sin(phi), sin(psi), sin(theta), back-rotation.
+// Returns false when one of the sines leaves [-1, 1] (the molecule is then
+// left as the position update put it, as the reference does).
+bool settle_one(const V3 old[3], V3 nw[3], V3 vel[3], double m_o, double m_h, double ra, double rb, double rc,
+                double dt_i) {
+    V3 b0 = old[1] - old[0], c0 = old[2] - old[0];
+    const double mt = m_o + m_h + m_h;
+    V3 d0 = (nw[0] * m_o + nw[1] * m_h + nw[2] * m_h) * (1.0 / mt);
+    V3 a1 = nw[0] - d0, b1 = nw[1] - d0, c1 = nw[2] - d0;
+    V3 n0 = cross(b0, c0);
+    V3 n1 = cross(a1, n0);
+    V3 n2 = cross(n0, n1);
+    n0 = n0 * (1.0 / vlen(n0));
+    n1 = n1 * (1.0 / vlen(n1));
+    n2 = n2 * (1.0 / vlen(n2));
+    V3 m1 = {n1.x, n2.x, n0.x}, m2 = {n1.y, n2.y, n0.y}, m0 = {n1.z, n2.z, n0.z};
+    b0 = {dot(n1, b0), dot(n2, b0), dot(n0, b0)};
+    c0 = {dot(n1, c0), dot(n2, c0), dot(n0, c0)};
+    a1 = {dot(n1, a1), dot(n2, a1), dot(n0, a1)};
+    b1 = {dot(n1, b1), dot(n2, b1), dot(n0, b1)};
+    c1 = {dot(n1, c1), dot(n2, c1), dot(n0, c1)};
+    const double sinphi = a1.z / ra;
+    const double omp = 1.0 - sinphi * sinphi;
+    if (omp < 0.0) return false;
+    const double cosphi = std::sqrt(omp);
+    const double sinpsi = (b1.z - c1.z) / (2.0 * rc * cosphi);
+    const double omq = 1.0 - sinpsi * sinpsi;
+    if (omq < 0.0) return false;
+    const double cospsi = std::sqrt(omq);
+    const double y_a2 = ra * cosphi, x_b2 = -rc * cospsi;
+    const double y_b2 = -rb * cosphi - rc * sinpsi * sinphi, y_c2 = -rb * cosphi + rc * sinpsi * sinphi;
+    const double alpha = x_b2 * (b0.x - c0.x) + b0.y * y_b2 + c0.y * y_c2;
+    const double beta = x_b2 * (c0.y - b0.y) + b0.x * y_b2 + c0.x * y_c2;
+    const double gamma = b0.x * b1.y - b1.x * b0.y + c0.x * c1.y - c1.x * c0.y;
+    const double ab2 = alpha * alpha + beta * beta;
+    const double sintheta = (alpha * gamma - beta * std::sqrt(ab2 - gamma * gamma)) / ab2;
+    const double omt = 1.0 - sintheta * sintheta;
+    if (omt < 0.0) return false;
+    const double costheta = std::sqrt(omt);
+    const V3 a3 = {-y_a2 * sintheta, y_a2 * costheta, a1.z};
+    const V3 b3 = {x_b2 * costheta - y_b2 * sintheta, x_b2 * sintheta + y_b2 * costheta, b1.z};
+    const V3 c3 = {-x_b2 * costheta - y_c2 * sintheta, -x_b2 * sintheta + y_c2 * costheta, c1.z};
+    const V3 p[3] = {V3{dot(a3, m1), dot(a3, m2), dot(a3, m0)} + d0, V3{dot(b3, m1), dot(b3, m2), dot(b3, m0)} + d0,
+                     V3{dot(c3, m1), dot(c3, m2), dot(c3, m0)} + d0};
+    for (int k = 0; k < 3; ++k) {
+        const V3 d = p[k] - nw[k];
+        nw[k] = p[k];
+        vel[k] = vel[k] + d * dt_i;
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" int orc_md_run(orc_ff* ff, double* pos_io, double* vel_io, const double* mass,
+                          const orc_md_params* mp, int n_steps, double* e_kin, double energies[2]) {
+    const orc_topology* t = ff->T->t;
+    const int n = t->n_atoms, nsa = t->n_solute_atoms, aps = t->atoms_per_solvent;
+    V3* pos = reinterpret_cast<V3*>(pos_io);
+    V3* vel = reinterpret_cast<V3*>(vel_io);
+    std::vector<double> f(size_t(n) * 3);
+    std::vector<V3> old(n);
+    const double dt = mp->dt;
+    int failures = 0;
+    double m_o = 0, m_h = 0, ra = 0, rb = 0, rc = 0;
+    const bool settle = mp->settle && aps == 3 && n > nsa;
+    if (settle) {  // canonical triangle (constraints.rs:836-840)
+        m_o = mass[nsa];
+        m_h = mass[nsa + 1];
+        const double half_mo_div_mh = 0.5 * m_o / m_h;
+        rc = 0.5 * mp->dist_hh;
+        ra = std::sqrt(mp->dist_oh * mp->dist_oh - rc * rc) / (1.0 + half_mo_div_mh);
+        rb = half_mo_div_mh * ra;
+    }
+    for (int step = 0; step < n_steps; ++step) {
+        orc_result r{};
+        r.forces = f.data();
+        orc_ff_apply(ff, pos_io, &r);
+        if (energies) {
+            energies[0] = r.e_lj;
+            energies[1] = r.e_crf;
+        }
+        for (int i = 0; i < n; ++i) {
+            const V3 F = {f[3 * i], f[3 * i + 1], f[3 * i + 2]};
+            vel[i] = vel[i] + F * (1.0 / mass[i]) * dt;
+            old[i] = pos[i];
+            pos[i] = pos[i] + vel[i] * dt;
+        }
+        if (settle)
+            for (int i = nsa; i + 3 <= n; i += 3)
+                if (!settle_one(&old[i], &pos[i], &vel[i], m_o, m_h, ra, rb, rc, 1.0 / dt)) ++failures;
+    }
+    if (e_kin) {
+        double ke = 0.0;
+        for (int i = 0; i < n; ++i) ke += 0.5 * mass[i] * dot(vel[i], vel[i]);
+        *e_kin = ke;
+    }
+    return failures;
+}

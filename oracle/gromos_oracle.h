@@ -116,6 +116,21 @@ void orc_perturbed_pair(const double r[3], double a_c6, double a_c12, double b_c
                         const double lp[17], const double crf[4], double four_pi_eps_i,
                         double out[5]);
 
+/* MD steps around orc_ff_apply, the sequence of gromos-md/src/bin/md.rs
+ * (:1144-1230) without thermostat: leap-frog velocity (leap_frog.rs:37-85),
+ * leap-frog position (:116-148), SETTLE of every solvent molecule
+ * (crates/gromos-integrators/src/constraints.rs:815-1010).  pos/vel are
+ * updated in place; returns the number of molecules SETTLE could not solve.
+ * e_kin = sum 0.5 m v^2 of the final half-step velocities; energies = the
+ * last step's {e_lj, e_crf}. */
+typedef struct {
+    double dt;
+    int32_t settle;
+    double dist_oh, dist_hh;
+} orc_md_params;
+int orc_md_run(orc_ff* ff, double* pos, double* vel, const double* mass, const orc_md_params* p,
+               int n_steps, double* e_kin, double energies[2]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,8 @@ def lib():
         L.orc_crf_params.argtypes = [C.c_double] * 4 + [_f64p]
         L.orc_lambda_params.argtypes = [C.c_double] * 8 + [C.c_int, _f64p]
         L.orc_perturbed_pair.argtypes = [_f64p] + [C.c_double] * 8 + [_f64p, _f64p, C.c_double, _f64p]
+        L.orc_md_run.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, C.POINTER(OrcMdParams), C.c_int, _f64p, _f64p]
+        L.orc_md_run.restype = C.c_int
         _lib = L
     return _lib
 
@@ -155,6 +157,10 @@ def pairlist(sysm, algorithm=None, nthreads=0):
     return out
 
 
+class OrcMdParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("settle", C.c_int32), ("dist_oh", C.c_double), ("dist_hh", C.c_double)]
+
+
 class OracleForcefield:
     """Forcefield::apply restated in FP64 (nonbonded only); one apply() per MD step."""
 
@@ -178,6 +184,18 @@ class OracleForcefield:
         assert rc == 0
         return {"forces": f, "e_lj": r.e_lj, "e_crf": r.e_crf, "dhdl": r.dhdl,
                 "virial": np.asarray(list(r.virial)).reshape(3, 3), "egroup_lj": glj, "egroup_crf": gcrf}
+
+    def md_run(self, pos, vel, mass, n_steps, dt=0.002, settle=True, dist_oh=0.1, dist_hh=0.1633):
+        """n_steps MD steps (leap-frog + SETTLE) in FP64; returns (pos, vel, stats)."""
+        x = np.ascontiguousarray(pos, dtype=np.float64).copy()
+        v = np.ascontiguousarray(vel, dtype=np.float64).copy()
+        m = np.ascontiguousarray(mass, dtype=np.float64)
+        mp = OrcMdParams(dt, 1 if settle else 0, dist_oh, dist_hh)
+        ke = C.c_double(0.0)
+        e = np.zeros(2)
+        fails = lib().orc_md_run(self.h, _p(x, C.c_double), _p(v, C.c_double), _p(m, C.c_double), C.byref(mp),
+                                 int(n_steps), C.byref(ke), _p(e, C.c_double))
+        return x, v, {"e_kin": ke.value, "e_lj": e[0], "e_crf": e[1], "settle_failures": fails}
 
     def close(self):
         if self.h:

@@ -94,3 +94,31 @@ def test_gromos_reader_roundtrip_fixture():
     assert s.topo.n_atoms == 2998 and s.topo.n_solute_cg == 1 and s.topo.n_egroups == 2
     assert s.params.rcutp == 0.8 and s.params.rcutl == 1.4 and s.params.nsnb == 1
     assert s.topo.pert_idx[0] == 0 and s.topo.pert_alpha_lj[0] == 0.25  # 0.5 * ALPHLJ 0.5
+
+
+def test_oracle_md_settle_constraints_and_cadence():
+    """Oracle MD: SETTLE keeps the rigid SPC triangle; split runs equal one run."""
+    import oracle_binding as ob
+    from gromos_nb import generators as g
+    s = g.spc_water_system(216, box=g.box_for_waters(216), seed=5, rcutp=0.8, rcutl=0.8)
+    m = g.masses(s)
+    v = g.maxwell_velocities(m, 300.0, 7)
+    o1 = ob.OracleForcefield(s)
+    x, vv, st = o1.md_run(s.pos, v, m, 10, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    assert st["settle_failures"] == 0
+    w = x.reshape(-1, 3, 3)
+    assert np.abs(np.linalg.norm(w[:, 1] - w[:, 0], axis=1) - 0.1).max() < 1e-12
+    assert np.abs(np.linalg.norm(w[:, 2] - w[:, 1], axis=1) - g.SPC_DHH).max() < 1e-12
+    o2 = ob.OracleForcefield(s)
+    x2, v2, _ = o2.md_run(s.pos, v, m, 4, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    x2, v2, _ = o2.md_run(x2, v2, m, 6, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    assert np.array_equal(x, x2) and np.array_equal(vv, v2)
+
+
+def test_md_entry_points_reject_bad_input_without_device():
+    from gromos_nb import _lib
+    import ctypes as C
+    L = _lib.lib()
+    mp = _lib.GrMdParams(0.002, 1, 0.1, 0.1633)
+    assert L.gr_md_init(None, None, None, C.byref(mp)) == _lib.GR_ERR_INVALID
+    assert L.gr_md_run(None, 1, None) == _lib.GR_ERR_INVALID
