@@ -456,6 +456,7 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
     params_set = true;
     built = false;
     lr_computed = false;
+    warm = false;
     return GR_OK;
 }
 
@@ -577,6 +578,7 @@ gr_status NbSystem::ensure_cgp_capacity() {
 }
 
 gr_status NbSystem::push_descriptor(cudaStream_t s) {
+    if (in_capture) return GR_OK;
     GR_CUDA(cudaMemcpyAsync(d_sys, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s));
     return GR_OK;
 }
@@ -858,7 +860,13 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
     const bool lj00 = h.water_lj00_only != 0;
     // The water kernels are persistent (grid-stride over i-clusters): the grid
     // is exactly one wave, SMs x resident blocks per SM, so that no block
-    // starts after the first ones have finished their share.
+    // starts after the first ones have finished their share -- or fewer
+    // blocks for a small system, which leaves SMs to the other members of a
+    // batch.
+    auto water_grid = [&](int wave) {
+        const long long need = (static_cast<long long>(h.max_clusters) + kWaterWarps - 1) / kWaterWarps;
+        return unsigned(std::max<long long>(1, std::min<long long>(wave, need)));
+    };
 #define GR_WATER_IT(WW, LJ, LL)                                                                          \
     do {                                                                                                 \
         const size_t smem = water_it_smem<WW>();                                                         \
@@ -870,7 +878,7 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
                                                                   128, smem));                           \
             if (occ < 1) occ = 1;                                                                        \
         }                                                                                                \
-        (++launches, k_water_force_it<WW, LJ, LL><<<unsigned(sm * occ), 128, smem, s>>>(d_sys, wp));     \
+        (++launches, k_water_force_it<WW, LJ, LL><<<water_grid(sm * occ), 128, smem, s>>>(d_sys, wp));  \
     } while (0)
 #define GR_WATER_SHARED(LJ, LL)                                                                          \
     do {                                                                                                 \
@@ -879,7 +887,7 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
             GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_water_force<LJ, LL>, 128, 0)); \
             if (occ < 1) occ = 1;                                                                        \
         }                                                                                                \
-        (++launches, k_water_force<LJ, LL><<<unsigned(sm * occ), 128, 0, s>>>(d_sys, wp));               \
+        (++launches, k_water_force<LJ, LL><<<water_grid(sm * occ), 128, 0, s>>>(d_sys, wp));            \
     } while (0)
     if (layout == 1) {
         if (lj00) {

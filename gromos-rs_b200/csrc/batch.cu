@@ -1,0 +1,463 @@
+// batch.cu -- many systems (REMD replicas, FEP lambda windows, serving jobs)
+// stepped together on one GPU.
+//
+// A batch holds member contexts of uneven size.  One MD step of the whole
+// batch is ONE CUDA graph launch: the graph forks one branch per member
+// (force evaluation + leap-frog/SETTLE kernel on the member's own stream) and
+// joins them, so the kernels of different members overlap on the GPU and
+// small members fill the SMs that large ones leave idle.  Each member keeps
+// its own rebuild phase (members may join at any step), so the graph of batch
+// step t depends only on t mod NSNB: NSNB graphs are captured and replayed.
+// After every step a gather kernel collects the members' error flags into
+// pinned host memory; a member whose lists overflowed is rolled back to the
+// snapshot taken at the start of its pairlist period (inside its rebuild
+// step's graph branch), its lists are grown, and its steps are re-run on its
+// own, so an overflow never reaches its trajectory and never disturbs the
+// other members.  Every member's arithmetic is exactly that of a standalone
+// run (fixed-point sums, same kernels, same order of launches per member), so
+// results are bit-identical alone and in the batch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <memory>
+
+namespace gnb {
+
+// err[0] of every member -> flags[i]
+__global__ void k_gather_flags(int* const* __restrict__ err, int n, int* __restrict__ flags) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flags[i] = err[i][0];
+}
+
+}  // namespace gnb
+
+struct gr_batch {
+    struct Member {
+        gr_ctx* ctx = nullptr;
+        int offset = 0;                // member phase at batch step t = (t + offset) mod NSNB
+        cudaEvent_t join = nullptr;
+    };
+    int device = 0;
+    cudaStream_t s0 = nullptr;
+    std::vector<Member> m;
+    int nsnb = 0;
+    long long t = 0;                   // batch MD steps done
+    std::vector<cudaGraphExec_t> g;    // one graph per step phase (t mod NSNB)
+    std::vector<long long> g_launches; // kernels per graph launch
+    bool valid = false;
+    cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
+    int** d_errp = nullptr;            // device array of the members' err pointers
+    int* d_flags = nullptr;
+    int* h_flags = nullptr;            // pinned
+    int cap = 0;
+    long long launches = 0;
+    float last_ms = 0.f;               // device time of the last gr_batch_md_run / gr_batch_eval
+
+    void drop_graphs() {
+        for (auto& x : g)
+            if (x) cudaGraphExecDestroy(x);
+        g.clear();
+        g_launches.clear();
+        valid = false;
+    }
+};
+
+namespace {
+
+using gnb::NbSystem;
+
+int member_phase(const gr_batch& b, const gr_batch::Member& mb) {
+    return int((b.t + mb.offset) % b.nsnb);
+}
+
+gr_status batch_capacity(gr_batch* b) {
+    const int n = int(b->m.size());
+    if (n <= b->cap) return GR_OK;
+    const int c = std::max(n, 2 * b->cap + 8);
+    if (b->d_errp) cudaFree(b->d_errp);
+    if (b->d_flags) cudaFree(b->d_flags);
+    if (b->h_flags) cudaFreeHost(b->h_flags);
+    b->d_errp = nullptr;
+    b->d_flags = nullptr;
+    b->h_flags = nullptr;
+    GR_CUDA(cudaMalloc(&b->d_errp, sizeof(int*) * c));
+    GR_CUDA(cudaMalloc(&b->d_flags, sizeof(int) * c));
+    GR_CUDA(cudaMallocHost(&b->h_flags, sizeof(int) * c));
+    b->cap = c;
+    return GR_OK;
+}
+
+// Members that never ran get one synchronous rebuild + evaluation: it sizes
+// their list capacities and performs the one-time kernel attribute set-up,
+// neither of which may happen while a graph is being recorded.
+gr_status batch_prepare(gr_batch* b, bool need_md) {
+    gr_status st;
+    for (auto& mb : b->m) {
+        NbSystem& S = mb.ctx->sys;
+        if (need_md && !S.md_ready) {
+            set_error("gr_batch_md_run: every member needs gr_md_init first");
+            return GR_ERR_STATE;
+        }
+        if (!S.ever_built || !S.warm) {
+            if ((st = S.eval(mb.ctx->stream, GR_EVAL_FORCE_REBUILD, false))) return st;
+            GR_CUDA(cudaStreamSynchronize(mb.ctx->stream));
+            bool of = false;
+            if ((st = S.resolve_pending(&of))) return st;
+            S.warm = true;
+            b->valid = false;
+        }
+    }
+    return GR_OK;
+}
+
+// Records the NSNB step graphs.
+gr_status batch_capture(gr_batch* b) {
+    b->drop_graphs();
+    gr_status st;
+    const int n = int(b->m.size());
+    if ((st = batch_capacity(b))) return st;
+    std::vector<int*> errp(n);
+    for (int i = 0; i < n; ++i) {
+        NbSystem& S = b->m[i].ctx->sys;
+        // settle every capacity now: nothing may be allocated during capture
+        if ((st = S.ensure_capacity())) return st;
+        if ((st = S.push_descriptor(b->m[i].ctx->stream))) return st;
+        errp[i] = S.h.err;
+    }
+    GR_CUDA(cudaMemcpy(b->d_errp, errp.data(), sizeof(int*) * n, cudaMemcpyHostToDevice));
+    for (auto& mb : b->m) GR_CUDA(cudaStreamSynchronize(mb.ctx->stream));
+    for (auto& mb : b->m) mb.ctx->sys.in_capture = true;
+    std::vector<long long> launches0(n);  // recording is not launching: restored below
+    for (int i = 0; i < n; ++i) launches0[i] = b->m[i].ctx->sys.launches;
+    b->g.assign(b->nsnb, nullptr);
+    b->g_launches.assign(b->nsnb, 0);
+    for (int p = 0; p < b->nsnb; ++p) {
+        long long l0 = 0;
+        for (auto& mb : b->m) l0 += mb.ctx->sys.launches;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(b->s0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) e = cudaEventRecord(b->fork, b->s0);
+        st = GR_OK;
+        for (int i = 0; i < n && e == cudaSuccess && !st; ++i) {
+            auto& mb = b->m[i];
+            NbSystem& S = mb.ctx->sys;
+            cudaStream_t si = mb.ctx->stream;
+            const int ph = int((p + mb.offset) % b->nsnb);
+            e = cudaStreamWaitEvent(si, b->fork, 0);
+            if (e != cudaSuccess) break;
+            const size_t bytes3 = size_t(S.N) * 3 * sizeof(double);
+            if (ph == 0) {  // pairlist period starts: snapshot for rollback, then rebuild
+                e = cudaMemcpyAsync(S.md_pos_snap, S.h.pos, bytes3, cudaMemcpyDeviceToDevice, si);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(S.md_vel_snap, S.md_vel, bytes3, cudaMemcpyDeviceToDevice, si);
+                if (e != cudaSuccess) break;
+                S.steps_since_update = S.prm.nsnb;
+            } else {
+                S.steps_since_update = 1;
+            }
+            S.built = true;
+            S.lr_computed = true;
+            S.pending_check = false;
+            st = S.eval(si, 0, false);
+            if (!st) st = S.md_step_launch(si);
+            if (!st) e = cudaEventRecord(mb.join, si);
+            if (!st && e == cudaSuccess) e = cudaStreamWaitEvent(b->s0, mb.join, 0);
+        }
+        if (e == cudaSuccess && !st) {
+            gnb::k_gather_flags<<<(n + 255) / 256, 256, 0, b->s0>>>(b->d_errp, n, b->d_flags);
+            e = cudaMemcpyAsync(b->h_flags, b->d_flags, sizeof(int) * n, cudaMemcpyDeviceToHost, b->s0);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(b->s0, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess && !st) e = cudaGraphInstantiate(&b->g[p], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        long long l1 = 0;
+        for (auto& mb : b->m) l1 += mb.ctx->sys.launches;
+        b->g_launches[p] = l1 - l0 + 1;  // + the flag gather
+        if (st || e != cudaSuccess) {
+            for (int i = 0; i < n; ++i) b->m[i].ctx->sys.launches = launches0[i];
+            for (auto& mb : b->m) mb.ctx->sys.in_capture = false;
+            b->drop_graphs();
+            if (!st) {
+                set_error(std::string("gr_batch: graph capture failed: ") + cudaGetErrorString(e));
+                st = GR_ERR_CUDA;
+            }
+            return st;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        NbSystem& S = b->m[i].ctx->sys;
+        S.in_capture = false;
+        S.pending_check = false;
+        S.launches = launches0[i];
+    }
+    b->valid = true;
+    return GR_OK;
+}
+
+// A member whose lists overflowed during its current pairlist period: grow,
+// restore its period-start snapshot and re-run its `steps` steps on its own.
+gr_status batch_recover(gr_batch* b, gr_batch::Member& mb, int flags, int steps) {
+    NbSystem& S = mb.ctx->sys;
+    cudaStream_t si = mb.ctx->stream;
+    GR_CUDA(cudaMemsetAsync(S.h.err, 0, 4 * sizeof(int), si));
+    if (flags & (gnb::ERR_CELL_TOO_DENSE | gnb::ERR_CG_TOO_LARGE)) {
+        set_error(flags & gnb::ERR_CELL_TOO_DENSE ? "pairlist: a grid cell holds more than 2048 charge groups"
+                                                  : "pairlist: solute charge group larger than 8 atoms");
+        return GR_ERR_UNSUPPORTED;
+    }
+    if (flags & gnb::ERR_WLIST_OVERFLOW) S.wcap_want = std::max(S.wcap_want, S.wcap_alloc) * 2;
+    if (flags & gnb::ERR_SLIST_OVERFLOW) S.scap_want = std::max(S.scap_want, S.scap_alloc) * 2;
+    if (flags & gnb::ERR_PERT_OVERFLOW) S.pcap_want = std::max(S.pcap_want, S.pcap_alloc) * 2;
+    if (flags & gnb::ERR_DEFER_OVERFLOW) {
+        S.defer_want = std::max(S.defer_want, S.h.defer_cap) * 4;
+        S.clus_alloc = 0;
+    }
+    const size_t bytes3 = size_t(S.N) * 3 * sizeof(double);
+    GR_CUDA(cudaMemcpyAsync(S.h.pos, S.md_pos_snap, bytes3, cudaMemcpyDeviceToDevice, si));
+    GR_CUDA(cudaMemcpyAsync(S.md_vel, S.md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, si));
+    S.steps_since_update = S.prm.nsnb;
+    S.built = false;
+    S.lr_computed = false;
+    S.pending_check = false;
+    gr_status st = S.md_run(si, steps, nullptr);
+    if (st) return st;
+    S.md_steps_total -= steps;  // counted once, by the batch step that failed
+    S.md_rollbacks += 1;
+    GR_CUDA(cudaStreamSynchronize(si));
+    b->valid = false;  // capacities changed: re-record the graphs
+    return GR_OK;
+}
+
+gr_batch::Member* find_member(gr_batch* b, gr_ctx* ctx) {
+    for (auto& mb : b->m)
+        if (mb.ctx == ctx) return &mb;
+    return nullptr;
+}
+
+}  // namespace
+
+#define BATCH_GUARD(b)                                  \
+    do {                                                \
+        if (!(b)) {                                     \
+            set_error("null gr_batch");                 \
+            return GR_ERR_INVALID;                      \
+        }                                               \
+        cudaError_t e_ = cudaSetDevice((b)->device);    \
+        if (e_ != cudaSuccess) {                        \
+            set_error(cudaGetErrorString(e_));          \
+            return GR_ERR_CUDA;                         \
+        }                                               \
+    } while (0)
+
+extern "C" {
+
+gr_status gr_batch_create(int device, gr_batch** out) {
+    if (!out) {
+        set_error("gr_batch_create: null out");
+        return GR_ERR_INVALID;
+    }
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        set_error("gr_batch_create: no CUDA device");
+        return GR_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) {
+        set_error("gr_batch_create: device index out of range");
+        return GR_ERR_INVALID;
+    }
+    GR_CUDA(cudaSetDevice(device));
+    auto b = std::make_unique<gr_batch>();
+    b->device = device;
+    GR_CUDA(cudaStreamCreateWithFlags(&b->s0, cudaStreamNonBlocking));
+    GR_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    GR_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+    GR_CUDA(cudaEventCreate(&b->t0));
+    GR_CUDA(cudaEventCreate(&b->t1));
+    *out = b.release();
+    return GR_OK;
+}
+
+gr_status gr_batch_destroy(gr_batch* b) {
+    if (!b) return GR_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->s0);
+    b->drop_graphs();
+    for (auto& mb : b->m)
+        if (mb.join) cudaEventDestroy(mb.join);
+    if (b->d_errp) cudaFree(b->d_errp);
+    if (b->d_flags) cudaFree(b->d_flags);
+    if (b->h_flags) cudaFreeHost(b->h_flags);
+    for (cudaEvent_t e : {b->fork, b->done, b->t0, b->t1})
+        if (e) cudaEventDestroy(e);
+    cudaStreamDestroy(b->s0);
+    delete b;
+    return GR_OK;
+}
+
+gr_status gr_batch_add(gr_batch* b, gr_ctx* ctx) {
+    BATCH_GUARD(b);
+    if (!ctx) {
+        set_error("gr_batch_add: null ctx");
+        return GR_ERR_INVALID;
+    }
+    NbSystem& S = ctx->sys;
+    if (ctx->device != b->device) {
+        set_error("gr_batch_add: member lives on another device");
+        return GR_ERR_INVALID;
+    }
+    if (!S.uploaded || !S.params_set || !S.box_set || !S.pos_set) {
+        set_error("gr_batch_add: member needs topology, parameters, box and positions");
+        return GR_ERR_STATE;
+    }
+    if (S.prm.kernel != GR_KERNEL_FIXED) {
+        set_error("gr_batch_add: batches run the fixed-point kernel");
+        return GR_ERR_UNSUPPORTED;
+    }
+    if (find_member(b, ctx)) {
+        set_error("gr_batch_add: already a member");
+        return GR_ERR_INVALID;
+    }
+    if (b->m.empty()) b->nsnb = std::max(1, S.prm.nsnb);
+    if (std::max(1, S.prm.nsnb) != b->nsnb) {
+        set_error("gr_batch_add: every member of a batch needs the same NSNB");
+        return GR_ERR_INVALID;
+    }
+    gr_batch::Member mb;
+    mb.ctx = ctx;
+    mb.offset = int((b->nsnb - b->t % b->nsnb) % b->nsnb);  // its first batch step rebuilds
+    GR_CUDA(cudaEventCreateWithFlags(&mb.join, cudaEventDisableTiming));
+    S.steps_since_update = S.prm.nsnb;
+    S.built = false;
+    b->m.push_back(mb);
+    b->valid = false;
+    return GR_OK;
+}
+
+gr_status gr_batch_remove(gr_batch* b, gr_ctx* ctx) {
+    BATCH_GUARD(b);
+    for (size_t i = 0; i < b->m.size(); ++i)
+        if (b->m[i].ctx == ctx) {
+            GR_CUDA(cudaStreamSynchronize(b->s0));
+            NbSystem& S = ctx->sys;
+            const int ph = member_phase(*b, b->m[i]);
+            S.steps_since_update = ph == 0 ? S.prm.nsnb : ph;  // standalone use continues the cadence
+            if (b->m[i].join) cudaEventDestroy(b->m[i].join);
+            b->m.erase(b->m.begin() + long(i));
+            b->valid = false;
+            return GR_OK;
+        }
+    set_error("gr_batch_remove: not a member");
+    return GR_ERR_INVALID;
+}
+
+gr_status gr_batch_size(gr_batch* b, int32_t* n) {
+    BATCH_GUARD(b);
+    if (!n) return GR_ERR_INVALID;
+    *n = int32_t(b->m.size());
+    return GR_OK;
+}
+
+// n MD steps of every member: one graph launch per step.
+gr_status gr_batch_md_run(gr_batch* b, int32_t n_steps) {
+    BATCH_GUARD(b);
+    if (n_steps < 0) {
+        set_error("gr_batch_md_run: n_steps must be >= 0");
+        return GR_ERR_INVALID;
+    }
+    b->last_ms = 0.f;
+    if (b->m.empty() || n_steps == 0) return GR_OK;
+    gr_status st;
+    if ((st = batch_prepare(b, true))) return st;
+    float total_ms = 0.f;
+    for (int k = 0; k < n_steps; ++k) {
+        if (!b->valid && (st = batch_capture(b))) return st;
+        const int p = int(b->t % b->nsnb);
+        GR_CUDA(cudaEventRecord(b->t0, b->s0));
+        GR_CUDA(cudaGraphLaunch(b->g[p], b->s0));
+        GR_CUDA(cudaEventRecord(b->t1, b->s0));
+        b->launches += b->g_launches[p];
+        GR_CUDA(cudaEventSynchronize(b->t1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->t0, b->t1);
+        total_ms += ms;
+        for (auto& mb : b->m) mb.ctx->sys.md_steps_total += 1;
+        for (size_t i = 0; i < b->m.size(); ++i) {
+            const int f = b->h_flags[i];
+            if (!f) continue;
+            auto& mb = b->m[i];
+            const int ph = member_phase(*b, mb);  // phase of the step just run
+            if ((st = batch_recover(b, mb, f, ph + 1))) return st;
+        }
+        b->t += 1;
+    }
+    b->last_ms = total_ms;
+    return GR_OK;
+}
+
+// One force evaluation of every member (no MD); results per member through
+// gr_result_download.  Members are evaluated concurrently on their streams.
+gr_status gr_batch_eval(gr_batch* b, int32_t flags) {
+    BATCH_GUARD(b);
+    gr_status st;
+    if ((st = batch_prepare(b, false))) return st;
+    GR_CUDA(cudaEventRecord(b->t0, b->s0));
+    GR_CUDA(cudaEventRecord(b->fork, b->s0));
+    for (auto& mb : b->m) {
+        GR_CUDA(cudaStreamWaitEvent(mb.ctx->stream, b->fork, 0));
+        if ((st = mb.ctx->sys.eval(mb.ctx->stream, flags & ~GR_EVAL_NO_DOWNLOAD, false))) return st;
+        GR_CUDA(cudaEventRecord(mb.join, mb.ctx->stream));
+        GR_CUDA(cudaStreamWaitEvent(b->s0, mb.join, 0));
+    }
+    GR_CUDA(cudaEventRecord(b->t1, b->s0));
+    GR_CUDA(cudaEventSynchronize(b->t1));
+    cudaEventElapsedTime(&b->last_ms, b->t0, b->t1);
+    // overflow check per member; a member that overflowed is evaluated again
+    // through the retrying single-system path
+    for (auto& mb : b->m) {
+        NbSystem& S = mb.ctx->sys;
+        int e[4] = {0, 0, 0, 0};
+        GR_CUDA(cudaMemcpy(e, S.h.err, sizeof(e), cudaMemcpyDeviceToHost));
+        bool of = false;
+        if ((st = S.resolve_pending(&of))) return st;
+        if (e[0] & gnb::ERR_DEFER_OVERFLOW) {
+            GR_CUDA(cudaMemset(S.h.err, 0, sizeof(e)));
+            S.defer_want = std::max(S.defer_want, S.h.defer_cap) * 4;
+            S.clus_alloc = 0;
+            S.built = false;
+            S.lr_computed = false;
+            of = true;
+        }
+        if (of) {
+            gr_result r{};
+            r.n_pairs_short = -1;
+            S.steps_since_update = S.prm.nsnb;  // the failed evaluation's rebuild is redone
+            if ((st = gr_forces_eval(mb.ctx, flags & ~GR_EVAL_NO_DOWNLOAD, &r))) return st;
+        }
+    }
+    b->valid = false;  // member cadences moved outside the graphs
+    return GR_OK;
+}
+
+gr_status gr_batch_last_ms(gr_batch* b, float* ms) {
+    BATCH_GUARD(b);
+    if (!ms) return GR_ERR_INVALID;
+    *ms = b->last_ms;
+    return GR_OK;
+}
+
+gr_status gr_batch_launches(gr_batch* b, int64_t* n) {
+    BATCH_GUARD(b);
+    if (!n) return GR_ERR_INVALID;
+    *n = b->launches;
+    return GR_OK;
+}
+
+gr_status gr_ctx_device_bytes(gr_ctx* ctx, int64_t* bytes) {
+    CTX_GUARD(ctx);
+    if (!bytes) return GR_ERR_INVALID;
+    *bytes = int64_t(ctx->sys.bytes);
+    return GR_OK;
+}
+
+}  // extern "C"

@@ -5,4 +5,5 @@
 #include "water.cu"
 #include "api.cu"
 #include "md.cu"
+#include "batch.cu"
 #include "noalloc.cu"

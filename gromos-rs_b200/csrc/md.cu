@@ -183,6 +183,10 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
         (st = upload_array(&md_vel, v0.data(), size_t(N) * 3)) || (st = alloc(&md_pos_snap, size_t(N) * 3)) ||
         (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 1)) || (st = alloc(&md_fail, 1)))
         return st;
+    GR_CUDA(cudaMemset(md_ke, 0, sizeof(long long)));
+    GR_CUDA(cudaMemset(md_fail, 0, sizeof(int)));
+    md_steps_total = 0;
+    md_rollbacks = 0;
     if (!md_err_host) GR_CUDA(cudaMallocHost(&md_err_host, 8 * sizeof(long long)));
     if (!ev_md) GR_CUDA(cudaEventCreateWithFlags(&ev_md, cudaEventDisableTiming));
     mdp = *p;
@@ -199,15 +203,8 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
     return GR_OK;
 }
 
-gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
-    if (!md_ready) {
-        set_error("gr_md_run before gr_md_init");
-        return GR_ERR_STATE;
-    }
-    if (n_steps < 0) {
-        set_error("gr_md_run: n_steps must be >= 0");
-        return GR_ERR_INVALID;
-    }
+// Zeroes the kinetic-energy accumulator and launches one MD step kernel.
+gr_status NbSystem::md_step_launch(cudaStream_t s) {
     MdDev md;
     md.vel = md_vel;
     md.inv_mass = md_inv_mass;
@@ -224,8 +221,43 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
     md.failures = md_fail;
     const int n_units = md_settle ? NSA + (N - NSA) / 3 : N;
     const unsigned grid = std::max(1u, std::min(unsigned((n_units + 255) / 256), unsigned(sm_count() * 8)));
+    GR_CUDA(cudaMemsetAsync(md_ke, 0, sizeof(long long), s));
+    (++launches, k_md_step<<<grid, 256, 0, s>>>(d_sys, md));
+    return GR_OK;
+}
+
+gr_status NbSystem::md_stats(cudaStream_t s, gr_md_stats* out) {
+    long long ke = 0;
+    int fails = 0;
+    std::vector<double> e(acc_size(G));
+    GR_CUDA(cudaMemcpyAsync(&ke, md_ke, sizeof(ke), cudaMemcpyDeviceToHost, s));
+    GR_CUDA(cudaMemcpyAsync(&fails, md_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GR_CUDA(cudaMemcpyAsync(e.data(), h.e_out, e.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GR_CUDA(cudaStreamSynchronize(s));
+    double elj = 0.0, ecrf = 0.0;
+    for (int g = 0; g < G * G; ++g) {
+        elj += e[g];
+        ecrf += e[G * G + g];
+    }
+    out->steps = md_steps_total;
+    out->e_lj = elj;
+    out->e_crf = ecrf;
+    out->e_kin = double(ke) / kEnergyScale;
+    out->settle_failures = fails;
+    out->rollbacks = int(md_rollbacks);
+    return GR_OK;
+}
+
+gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
+    if (!md_ready) {
+        set_error("gr_md_run before gr_md_init");
+        return GR_ERR_STATE;
+    }
+    if (n_steps < 0) {
+        set_error("gr_md_run: n_steps must be >= 0");
+        return GR_ERR_INVALID;
+    }
     const size_t bytes3 = size_t(N) * 3 * sizeof(double);
-    GR_CUDA(cudaMemsetAsync(md_fail, 0, sizeof(int), s));
     int done = 0, attempts = 0, rollbacks = 0;
     gr_status st;
     while (done < n_steps) {
@@ -245,8 +277,7 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
                 }
             }
             if ((st = eval(s, 0, false))) return st;
-            GR_CUDA(cudaMemsetAsync(md_ke, 0, sizeof(long long), s));
-            (++launches, k_md_step<<<grid, 256, 0, s>>>(d_sys, md));
+            if ((st = md_step_launch(s))) return st;
             ++k;
             if (done + k >= n_steps || steps_since_update >= prm.nsnb) break;
         }
@@ -294,24 +325,10 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
         done += k;
     }
     md_steps_total += done;
+    md_rollbacks += rollbacks;
     if (out) {
-        long long ke = 0;
-        int fails = 0;
-        std::vector<double> e(acc_size(G));
-        GR_CUDA(cudaMemcpyAsync(&ke, md_ke, sizeof(ke), cudaMemcpyDeviceToHost, s));
-        GR_CUDA(cudaMemcpyAsync(&fails, md_fail, sizeof(int), cudaMemcpyDeviceToHost, s));
-        GR_CUDA(cudaMemcpyAsync(e.data(), h.e_out, e.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-        GR_CUDA(cudaStreamSynchronize(s));
-        double elj = 0.0, ecrf = 0.0;
-        for (int g = 0; g < G * G; ++g) {
-            elj += e[g];
-            ecrf += e[G * G + g];
-        }
+        if ((st = md_stats(s, out))) return st;
         out->steps = done;
-        out->e_lj = elj;
-        out->e_crf = ecrf;
-        out->e_kin = double(ke) / kEnergyScale;
-        out->settle_failures = fails;
         out->rollbacks = rollbacks;
     }
     return GR_OK;
@@ -327,6 +344,15 @@ gr_status gr_md_init(gr_ctx* ctx, const double* mass, const double* vel, const g
 gr_status gr_md_run(gr_ctx* ctx, int32_t n_steps, gr_md_stats* out) {
     CTX_GUARD(ctx);
     return ctx->sys.md_run(ctx->stream, n_steps, out);
+}
+
+gr_status gr_md_stats_get(gr_ctx* ctx, gr_md_stats* out) {
+    CTX_GUARD(ctx);
+    if (!ctx->sys.md_ready || !out) {
+        set_error("gr_md_stats_get: MD not initialised or null out");
+        return ctx->sys.md_ready ? GR_ERR_INVALID : GR_ERR_STATE;
+    }
+    return ctx->sys.md_stats(ctx->stream, out);
 }
 
 gr_status gr_md_download(gr_ctx* ctx, double* pos, double* vel) {

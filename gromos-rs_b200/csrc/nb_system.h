@@ -35,6 +35,9 @@ class NbSystem {
     gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
     gr_status md_init(const double* mass, const double* vel, const gr_md_params* p);
     gr_status md_run(cudaStream_t s, int n_steps, gr_md_stats* out);
+    gr_status md_step_launch(cudaStream_t s);
+    gr_status md_stats(cudaStream_t s, gr_md_stats* out);
+    gr_status ensure_capacity();
 
     // sizes
     int N = 0, NCG = 0, NSCG = 0, NSA = 0, NT = 0, G = 1, aps = 3, W = 4, layout = 2;
@@ -77,14 +80,15 @@ class NbSystem {
     int* md_fail = nullptr;
     long long* md_err_host = nullptr;  // pinned
     cudaEvent_t ev_md = nullptr;
-    long long md_steps_total = 0;
+    long long md_steps_total = 0, md_rollbacks = 0;
+    bool warm = false;        // evaluated at least once with the current parameters
+    bool in_capture = false;  // recording a CUDA graph: the device descriptor is already current
 
    private:
     template <class T>
     gr_status alloc(T** p, size_t n);
     template <class T>
     gr_status upload_array(T** p, const T* host, size_t n);
-    gr_status ensure_capacity();
     gr_status ensure_cgp_capacity();
     gr_status check_errors(cudaStream_t s, bool* retry);
     std::vector<void*> allocs;

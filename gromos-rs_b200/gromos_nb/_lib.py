@@ -107,6 +107,17 @@ _SIGNATURES = {
     "gr_md_init": (C.c_int32, [C.c_void_p, _f64p, _f64p, C.POINTER(GrMdParams)]),
     "gr_md_run": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrMdStats)]),
     "gr_md_download": (C.c_int32, [C.c_void_p, _f64p, _f64p]),
+    "gr_md_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GrMdStats)]),
+    "gr_batch_create": (C.c_int32, [C.c_int, C.POINTER(C.c_void_p)]),
+    "gr_batch_destroy": (C.c_int32, [C.c_void_p]),
+    "gr_batch_add": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "gr_batch_remove": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "gr_batch_size": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "gr_batch_md_run": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "gr_batch_eval": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "gr_batch_last_ms": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
+    "gr_batch_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "gr_ctx_device_bytes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_lj_crf_innerloop_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                                 C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                                 C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,

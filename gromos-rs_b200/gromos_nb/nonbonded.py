@@ -226,6 +226,33 @@ class Forcefield:
     def md_run_async(self, n_steps: int) -> None:
         check(self._L.gr_md_run(self._h, int(n_steps), None))
 
+    def md_stats(self) -> Dict:
+        st = _lib.GrMdStats()
+        check(self._L.gr_md_stats_get(self._h, C.byref(st)))
+        return {"steps": st.steps, "e_lj": st.e_lj, "e_crf": st.e_crf, "e_kin": st.e_kin,
+                "settle_failures": st.settle_failures, "rollbacks": st.rollbacks}
+
+    def result(self) -> Dict:
+        """Results of the last evaluation (e.g. after a batch evaluation), without evaluating."""
+        f = np.zeros((self.n_atoms, 3))
+        glj = np.zeros((self.G, self.G))
+        gcrf = np.zeros((self.G, self.G))
+        r = _lib.GrResult()
+        r.forces = _p(f, C.c_double)
+        r.egroup_lj, r.egroup_crf = _p(glj, C.c_double), _p(gcrf, C.c_double)
+        check(self._L.gr_result_download(self._h, C.byref(r)))
+        return {"forces": f, "e_lj": r.e_lj, "e_crf": r.e_crf, "dhdl": r.dhdl,
+                "virial": np.asarray(list(r.virial)).reshape(3, 3), "egroup_lj": glj, "egroup_crf": gcrf}
+
+    def device_bytes(self) -> int:
+        n = C.c_int64(0)
+        check(self._L.gr_ctx_device_bytes(self._h, C.byref(n)))
+        return int(n.value)
+
+    @property
+    def handle(self):
+        return self._h
+
     def md_state(self):
         x = np.zeros((self.n_atoms, 3))
         v = np.zeros((self.n_atoms, 3))
@@ -255,6 +282,64 @@ class Forcefield:
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._L.gr_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Members (Forcefield objects) stepped together: one CUDA graph launch per MD step.
+
+    Replaces stepping REMD replicas / FEP windows one after the other
+    (replica.rs:163, :315; remd.rs:168).  Members stay owned by the caller;
+    each member's results are bit-identical to its standalone run.
+    """
+
+    def __init__(self, device: int = 0):
+        self._L = _lib.lib()
+        h = C.c_void_p()
+        check(self._L.gr_batch_create(device, C.byref(h)))
+        self._h = h
+        self.members: List["Forcefield"] = []
+
+    def add(self, ff: "Forcefield") -> None:
+        check(self._L.gr_batch_add(self._h, ff.handle))
+        self.members.append(ff)
+
+    def remove(self, ff: "Forcefield") -> None:
+        check(self._L.gr_batch_remove(self._h, ff.handle))
+        self.members.remove(ff)
+
+    def __len__(self) -> int:
+        return len(self.members)
+
+    def md_run(self, n_steps: int) -> float:
+        """MD steps of every member; returns the device time in ms."""
+        check(self._L.gr_batch_md_run(self._h, int(n_steps)))
+        return self.last_ms()
+
+    def eval(self, virial: bool = True) -> float:
+        """One force evaluation of every member (results: ``member.result()``); device ms."""
+        check(self._L.gr_batch_eval(self._h, _lib.GR_EVAL_VIRIAL if virial else 0))
+        return self.last_ms()
+
+    def last_ms(self) -> float:
+        ms = C.c_float(0.0)
+        check(self._L.gr_batch_last_ms(self._h, C.byref(ms)))
+        return float(ms.value)
+
+    def launches(self) -> int:
+        n = C.c_int64(0)
+        check(self._L.gr_batch_launches(self._h, C.byref(n)))
+        return int(n.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.gr_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -199,11 +199,11 @@ typedef struct {
 } gr_md_params;
 
 typedef struct {
-    int64_t steps;            /* steps done by the call */
+    int64_t steps;            /* steps done by the call (gr_md_stats_get: since gr_md_init) */
     double e_lj, e_crf;       /* nonbonded energies of the last force evaluation */
     double e_kin;             /* sum 0.5 m v^2 of the last half-step velocities */
-    int32_t settle_failures;  /* molecules SETTLE could not solve (left as moved, as the reference) */
-    int32_t rollbacks;        /* pairlist periods re-run after a list overflow */
+    int32_t settle_failures;  /* SETTLE failures since gr_md_init (molecule left as moved, as the reference) */
+    int32_t rollbacks;        /* pairlist periods re-run after a list overflow (by the call / since init) */
 } gr_md_stats;
 
 /* masses: n_atoms (all > 0); vel: n_atoms*3 initial v(-dt/2) or NULL (zero).
@@ -211,8 +211,38 @@ typedef struct {
 gr_status gr_md_init(gr_ctx* ctx, const double* mass, const double* vel, const gr_md_params* params);
 /* Runs n_steps MD steps on the context's stream; out may be NULL. */
 gr_status gr_md_run(gr_ctx* ctx, int32_t n_steps, gr_md_stats* out);
+/* Statistics of the last step and totals since gr_md_init. */
+gr_status gr_md_stats_get(gr_ctx* ctx, gr_md_stats* out);
 /* Current positions and velocities (either may be NULL). */
 gr_status gr_md_download(gr_ctx* ctx, double* pos, double* vel);
+
+/* ---- batches: many systems stepped together on one GPU ------------------- */
+/* No single gromos-rs counterpart: replaces stepping REMD replicas
+ * (crates/gromos-integrators/src/replica.rs:163 calculate_forces, :315
+ * run_md_steps, driven by remd.rs:168 run_md_parallel) or FEP lambda windows
+ * one after the other.  Members are ordinary contexts (topology, params, box,
+ * positions and gr_md_init done) of uneven size on the batch's device; they
+ * must use GR_KERNEL_FIXED and share NSNB.  One batch MD step is one CUDA
+ * graph launch whose branches (one per member) overlap on the GPU; each
+ * member's results are bit-identical to a standalone run.  A member may be
+ * added or removed between calls (continuous batching); it stays owned by
+ * the caller. */
+typedef struct gr_batch gr_batch;
+gr_status gr_batch_create(int device, gr_batch** out);
+gr_status gr_batch_destroy(gr_batch* b);            /* members are not destroyed */
+gr_status gr_batch_add(gr_batch* b, gr_ctx* ctx);   /* the member's next step rebuilds its pairlist */
+gr_status gr_batch_remove(gr_batch* b, gr_ctx* ctx);
+gr_status gr_batch_size(gr_batch* b, int32_t* n);
+/* n_steps MD steps of every member (results: gr_md_stats_get / gr_md_download per member). */
+gr_status gr_batch_md_run(gr_batch* b, int32_t n_steps);
+/* One force evaluation of every member (results: gr_result_download per member). */
+gr_status gr_batch_eval(gr_batch* b, int32_t flags);
+/* Device time (CUDA events) of the last gr_batch_md_run / gr_batch_eval, ms. */
+gr_status gr_batch_last_ms(gr_batch* b, float* ms);
+/* Kernels launched by the batch's graphs so far. */
+gr_status gr_batch_launches(gr_batch* b, int64_t* n);
+/* Device bytes held by a context (topology, lists, accumulators, MD state). */
+gr_status gr_ctx_device_bytes(gr_ctx* ctx, int64_t* bytes);
 
 /* ---- reference FFI stub replacement ------------------------------------ */
 /* Replaces `rust_lj_crf_innerloop` (crates/gromos-core/src/ffi.rs:55-103):

@@ -122,3 +122,13 @@ def test_md_entry_points_reject_bad_input_without_device():
     mp = _lib.GrMdParams(0.002, 1, 0.1, 0.1633)
     assert L.gr_md_init(None, None, None, C.byref(mp)) == _lib.GR_ERR_INVALID
     assert L.gr_md_run(None, 1, None) == _lib.GR_ERR_INVALID
+
+
+def test_batch_entry_points_without_device():
+    from gromos_nb import _lib
+    import ctypes as C
+    L = _lib.lib()
+    h = C.c_void_p()
+    assert L.gr_batch_create(0, C.byref(h)) == _lib.GR_ERR_NO_DEVICE
+    assert L.gr_batch_md_run(None, 1) == _lib.GR_ERR_INVALID
+    assert L.gr_batch_add(None, None) == _lib.GR_ERR_INVALID

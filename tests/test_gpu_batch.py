@@ -1,0 +1,123 @@
+"""Batches: many systems stepped together must give each member exactly its
+standalone results (bitwise: fixed-point sums, same kernels per member).
+
+Covers uneven REMD-like members (water boxes of different sizes, one with a
+solute), members that join and leave between calls (continuous batching),
+FEP lambda windows evaluated together, and the batch against the oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle_binding as ob
+from gromos_nb import generators as g
+from gromos_nb.nonbonded import Batch, Forcefield
+
+pytestmark = pytest.mark.gpu
+
+
+def member(s, seed, T=300.0):
+    ff = Forcefield(s)
+    ff.upload_positions(s.pos)
+    m = g.masses(s)
+    ff.md_init(m, g.maxwell_velocities(m, T, seed), dt=0.002, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    return ff
+
+
+def systems():
+    return [
+        g.spc_water_system(300, box=g.box_for_waters(300), seed=41, rcutp=0.8, rcutl=1.0, nsnb=5),
+        g.spc_water_system(1100, box=g.box_for_waters(1100), seed=42, rcutp=0.8, rcutl=1.0, nsnb=5),
+        g.solvated_solute_system(500, 40, seed=43, rc=1.0, nsnb=5),
+        g.spc_water_system(700, box=g.box_for_waters(700), seed=44, rcutp=0.8, rcutl=1.0, nsnb=5),
+    ]
+
+
+def standalone(s, seed, n):
+    ff = member(s, seed)
+    ff.md_run(n)
+    out = ff.md_state()
+    ff.close()
+    return out
+
+
+def test_batch_md_bit_identical_to_standalone():
+    sy = systems()
+    b = Batch()
+    ffs = [member(s, 100 + k) for k, s in enumerate(sy)]
+    for ff in ffs:
+        b.add(ff)
+    b.md_run(5)
+    b.md_run(8)
+    for k, (s, ff) in enumerate(zip(sy, ffs)):
+        x, v = ff.md_state()
+        xr, vr = standalone(s, 100 + k, 13)
+        assert np.array_equal(x, xr) and np.array_equal(v, vr), k
+        assert ff.md_stats()["steps"] == 13
+    b.close()
+    for ff in ffs:
+        ff.close()
+
+
+def test_batch_members_join_and_leave():
+    """Continuous batching: a member joins after 3 steps, another leaves after 7."""
+    sy = systems()
+    b = Batch()
+    a, c, d = member(sy[0], 1), member(sy[1], 2), member(sy[2], 3)
+    b.add(a)
+    b.add(c)
+    b.md_run(3)
+    b.add(d)                 # joins at batch step 3 with its own rebuild phase
+    b.md_run(4)
+    b.remove(c)              # leaves after 7 steps
+    b.md_run(5)
+    xa, va = a.md_state()
+    xc, vc = c.md_state()
+    xd, vd = d.md_state()
+    for (x, v), (s, seed, n) in zip([(xa, va), (xc, vc), (xd, vd)], [(sy[0], 1, 12), (sy[1], 2, 7), (sy[2], 3, 9)]):
+        xr, vr = standalone(s, seed, n)
+        assert np.array_equal(x, xr) and np.array_equal(v, vr)
+    b.close()
+    for ff in (a, c, d):
+        ff.close()
+
+
+def test_batch_fep_windows_eval():
+    """lambda windows of one perturbed system evaluated together == one by one == oracle."""
+    lams = [0.0, 0.25, 0.5, 0.75, 1.0]
+    base = g.solvated_solute_system(600, 30, seed=1004, perturbed=True, rc=1.2)
+    b = Batch()
+    ffs = []
+    for lam in lams:
+        base.params.lam = lam
+        ff = Forcefield(base)
+        ff.upload_positions(base.pos)
+        b.add(ff)
+        ffs.append(ff)
+    b.eval()
+    for lam, ff in zip(lams, ffs):
+        r = ff.result()
+        base.params.lam = lam
+        alone = Forcefield(base)
+        a = alone.apply(base.pos)
+        assert np.array_equal(r["forces"], a["forces"])
+        assert r["e_lj"] == a["e_lj"] and r["e_crf"] == a["e_crf"] and r["dhdl"] == a["dhdl"]
+        o = ob.OracleForcefield(base).apply(base.pos)
+        assert abs(r["dhdl"] - o["dhdl"]) <= 1e-5 * max(abs(o["dhdl"]), 1.0)
+        alone.close()
+    b.close()
+    for ff in ffs:
+        ff.close()
+
+
+def test_batch_launch_accounting():
+    sy = systems()[:2]
+    b = Batch()
+    ffs = [member(s, 7 + k) for k, s in enumerate(sy)]
+    for ff in ffs:
+        b.add(ff)
+    ms = b.md_run(10)
+    assert ms > 0.0
+    assert b.launches() >= 10 * 2 * 4   # at least prep/water/finalize/md per member and step
+    b.close()
+    for ff in ffs:
+        ff.close()
