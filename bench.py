@@ -312,6 +312,150 @@ def run_gpu(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Batched workloads: REMD replicas, FEP lambda windows, serving.  Each prints
+# its own JSON line; the default workload above is the single large system.
+
+def _member(s, seed, T, kernel="fixed"):
+    from gromos_nb import generators
+    from gromos_nb.nonbonded import Forcefield
+
+    ff = Forcefield(s, kernel=kernel)
+    ff.upload_positions(s.pos)
+    m = generators.masses(s)
+    ff.md_init(m, generators.maxwell_velocities(m, T, seed), dt=DT_PS, settle=True, dist_oh=0.1,
+               dist_hh=generators.SPC_DHH)
+    return ff
+
+
+def _pairs_per_step(ff, s):
+    r = ff.apply(s.pos, count_pairs=True, download_forces=False)
+    ff.upload_positions(s.pos)
+    return r["n_pairs_short"] + r["n_pairs_long"] / max(1, s.params.nsnb)
+
+
+def _one_by_one(systems, seeds, temps, steps, kernel):
+    """Members run alone, one after the other (device time per member summed)."""
+    import torch
+
+    total_ms = 0.0
+    for s, seed, T in zip(systems, seeds, temps):
+        ff = _member(s, seed, T, kernel)
+        ff.md_run(max(1, s.params.nsnb))          # warm-up period
+        stream = torch.cuda.ExternalStream(ff.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ff.md_run(steps)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        ff.close()
+    return total_ms
+
+
+def run_batched(args, kind):
+    """REMD replicas (uneven sizes) or FEP lambda windows in one batch."""
+    from gromos_nb import generators
+    from gromos_nb.nonbonded import Batch
+
+    rng = np.random.default_rng(1003 if kind == "remd" else 1004)
+    systems, seeds, temps, lams = [], [], [], []
+    if kind == "remd":
+        n = args.replicas
+        temps = list(300.0 * (450.0 / 300.0) ** (np.arange(n) / max(1, n - 1)))
+        for r in range(n):
+            nw = int(rng.integers(500, 8001))
+            systems.append(generators.solvated_solute_system(nw, 200, seed=1003 + r, rc=1.4, nsnb=5))
+            seeds.append(5000 + r)
+        workload = f"remd_{n}_replicas_spc500-8000_solute200_rc1.4"
+    else:
+        lams = [round(0.05 * k, 2) for k in range(21)]
+        for k, lam in enumerate(lams):
+            s = generators.solvated_solute_system(5000, 30, seed=1004, perturbed=True, lam=lam, rc=1.4, nsnb=5)
+            s.params.lam = lam
+            systems.append(s)
+            seeds.append(6000)                      # same start in every window
+            temps.append(300.0)
+        workload = "fep_21_windows_spc5000_solute30_rc1.4"
+    ffs = [_member(s, seed, T) for s, seed, T in zip(systems, seeds, temps)]
+    pairs = [_pairs_per_step(ff, s) for ff, s in zip(ffs, systems)]
+    b = Batch()
+    for ff in ffs:
+        b.add(ff)
+    tune = b.autotune(periods=1)
+    b.md_run(5)                                     # warm-up period (graph capture)
+    launches0 = b.launches()
+    ms = b.md_run(args.batch_steps)
+    launches = b.launches() - launches0
+    per_step = ms / args.batch_steps
+    value = sum(pairs) / (per_step * 1e-3)
+    stats = [ff.md_stats() for ff in ffs]
+    out_fep = None
+    if kind == "fep":
+        b.eval()
+        res = [ff.result() for ff in ffs]
+        out_fep = {"lambda": lams, "dhdl": [r["dhdl"] for r in res], "e_lj": [r["e_lj"] for r in res],
+                   "e_crf": [r["e_crf"] for r in res]}
+    b.close()
+    for ff in ffs:
+        ff.close()
+    # the same members one by one: fixed-point kernel, and the plain FP32 kernel
+    sample = min(len(systems), args.sample_members)
+    idx = list(range(0, len(systems), max(1, len(systems) // sample)))[:sample]
+    sub = [systems[i] for i in idx]
+    sub_pairs = sum(pairs[i] for i in idx)
+    steps_alone = min(args.batch_steps, 20)
+    ms_fixed = _one_by_one(sub, [seeds[i] for i in idx], [temps[i] for i in idx], steps_alone, "fixed")
+    ms_plain = _one_by_one(sub, [seeds[i] for i in idx], [temps[i] for i in idx], steps_alone, "plain")
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.batch_steps,
+            "warmup": 5, "ms_per_step": per_step,
+            "ns_per_day": ns_per_day(per_step), "ns_per_day_aggregate": ns_per_day(per_step) * len(systems),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64",
+            "data": "synthetic (seeded water boxes + seeded solutes)",
+            "config": {"workload": workload, "members": len(systems),
+                       "atoms_total": int(sum(s.topo.n_atoms for s in systems)),
+                       "pairs_per_batch_step": float(sum(pairs)), "step": "MD step (forces + leap-frog + SETTLE)",
+                       "launch": "one CUDA graph launch per batch step", "autotune": tune},
+            "gpu_launches": launches,
+            "one_by_one": {"sample_members": len(idx), "steps": steps_alone,
+                           "fixed_pair_int_per_s": sub_pairs * steps_alone / (ms_fixed * 1e-3),
+                           "plain_pair_int_per_s": sub_pairs * steps_alone / (ms_plain * 1e-3)},
+            "md": {"settle_failures": int(sum(s["settle_failures"] for s in stats)),
+                   "rollbacks": int(sum(s["rollbacks"] for s in stats))}}
+    if out_fep:
+        line["fep"] = out_fep
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args):
+    from gromos_nb.serving import Server, poisson_jobs
+
+    jobs = poisson_jobs(args.jobs, rate=20.0, seed=1005, waters=(300, 20000), steps=(100, 2000), solute_prob=0.5,
+                        solute_atoms=(50, 500), rc=1.4, nsnb=5)
+    srv = Server(hbm_budget=int(args.hbm_budget_gb * 2 ** 30), chunk_steps=5, count_pairs=True)
+    srv.run(jobs, timeout=1800)
+    rep = srv.report()
+    srv.close()
+    # the same jobs one by one on the plain kernel: a sample, extrapolated by pairs
+    k = min(len(jobs), args.sample_members)
+    ms_plain = _one_by_one([j.system for j in jobs[:k]], [7 for _ in range(k)], [300.0] * k, 20, "plain")
+    plain_rate = sum(j.pairs_per_step for j in jobs[:k]) * 20 / (ms_plain * 1e-3)
+    total_pairs = sum(j.pairs_per_step * j.n_steps for j in jobs)
+    line = {"metric": METRIC, "value": rep["pair_int_per_s"], "unit": METRIC, "n_gpus": 1,
+            "steps": rep["batch_steps"], "warmup": 0, "ms_per_step": rep["gpu_ms"] / max(1, rep["batch_steps"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64",
+            "data": "synthetic (seeded Poisson job stream, seeded systems)",
+            "config": {"workload": f"serving_{len(jobs)}_jobs_poisson20_spc300-20000_steps100-2000",
+                       "hbm_budget_gb": args.hbm_budget_gb, "chunk_steps": 5},
+            "serving": rep,
+            "one_by_one_plain": {"sample_jobs": k, "pair_int_per_s": plain_rate,
+                                 "makespan_s_extrapolated": total_pairs / plain_rate}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -323,6 +467,12 @@ def main():
     ap.add_argument("--cluster-size", type=int, default=0, help="water i-cluster width 4 or 8 (0 = default)")
     ap.add_argument("--md-steps", type=int, default=1000, help="MD steps timed for ns/day")
     ap.add_argument("--layout", type=int, default=0, help="water kernel layout: 1 shared bits, 2 per-lane bits")
+    ap.add_argument("--workload", default="spc30000", choices=["spc30000", "remd", "fep", "serving"])
+    ap.add_argument("--replicas", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--sample-members", type=int, default=8, help="members timed one by one for comparison")
+    ap.add_argument("--jobs", type=int, default=40)
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -331,6 +481,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload in ("remd", "fep"):
+        return run_batched(args, args.workload) if rank == 0 else 0
+    if args.workload == "serving":
+        return run_serving(args) if rank == 0 else 0
     if world > 1:
         import datetime
 

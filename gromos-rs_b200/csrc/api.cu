@@ -423,19 +423,19 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
         set_error("gr_nb_params: unknown kernel");
         return GR_ERR_INVALID;
     }
+    if (p->cluster_size != 0 && p->cluster_size != 4 && p->cluster_size != 8) {
+        set_error("gr_nb_params: cluster_size must be 0, 4 or 8");
+        return GR_ERR_INVALID;
+    }
+    if (p->water_layout == 1 && p->cluster_size == 8) {
+        set_error("gr_nb_params: the shared-bit layout supports cluster_size 4 only");
+        return GR_ERR_INVALID;
+    }
     prm = *p;
     // water kernel layout: 1 = lanes share the mask bits (width 4 only),
     // 2 = each lane iterates over its own bits (width 4 or 8)
     layout = p->water_layout == 1 ? 1 : 2;
     W = (layout == 2 && p->cluster_size == 8) ? 8 : 4;
-    if (p->cluster_size != 0 && p->cluster_size != 4 && p->cluster_size != 8) {
-        set_error("gr_nb_params: cluster_size must be 0, 4 or 8");
-        return GR_ERR_INVALID;
-    }
-    if (layout == 1 && p->cluster_size == 8) {
-        set_error("gr_nb_params: the shared-bit layout supports cluster_size 4 only");
-        return GR_ERR_INVALID;
-    }
     h.W = W;
     clus_alloc = 0;  // cluster arrays depend on W
     h.boundary = p->boundary;
@@ -457,6 +457,10 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
     built = false;
     lr_computed = false;
     warm = false;
+    if (box_set) {  // the cell grid depends on the cutoffs
+        const double b[3] = {h.box[0], h.box[1], h.box[2]};
+        return set_box(b);
+    }
     return GR_OK;
 }
 

@@ -461,3 +461,146 @@ gr_status gr_ctx_device_bytes(gr_ctx* ctx, int64_t* bytes) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner: picks the solvent kernel variant (lane layout and i-cluster
+// width) by timing full pairlist periods (one rebuild + long-range refresh +
+// NSNB short-range steps) of the systems themselves.  The rebuild interval is
+// not tuned: with the reference's twin-range scheme (no skin) NSNB decides
+// which pairs are evaluated, so changing it would change the results.
+namespace {
+
+struct Variant {
+    int layout, width;
+};
+constexpr Variant kVariants[] = {{2, 4}, {2, 8}, {1, 4}};
+constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
+
+// `periods` timed pairlist periods of every member, concurrently on their
+// streams; returns device ms per step.
+gr_status time_periods(std::vector<gr_ctx*>& ms, cudaStream_t s0, cudaEvent_t fork,
+                       std::vector<cudaEvent_t>& joins, cudaEvent_t t0, cudaEvent_t t1, int nsnb, int periods,
+                       float* ms_per_step) {
+    gr_status st;
+    GR_CUDA(cudaEventRecord(t0, s0));
+    for (int p = 0; p < periods; ++p)
+        for (int k = 0; k < nsnb; ++k) {
+            GR_CUDA(cudaEventRecord(fork, s0));
+            for (size_t i = 0; i < ms.size(); ++i) {
+                NbSystem& S = ms[i]->sys;
+                GR_CUDA(cudaStreamWaitEvent(ms[i]->stream, fork, 0));
+                if ((st = S.eval(ms[i]->stream, k == 0 ? GR_EVAL_FORCE_REBUILD : 0, false))) return st;
+                GR_CUDA(cudaEventRecord(joins[i], ms[i]->stream));
+                GR_CUDA(cudaStreamWaitEvent(s0, joins[i], 0));
+            }
+        }
+    GR_CUDA(cudaEventRecord(t1, s0));
+    GR_CUDA(cudaEventSynchronize(t1));
+    float t = 0.f;
+    GR_CUDA(cudaEventElapsedTime(&t, t0, t1));
+    *ms_per_step = t / float(periods * nsnb);
+    return GR_OK;
+}
+
+gr_status autotune(std::vector<gr_ctx*>& ms, cudaStream_t s0, cudaEvent_t fork, std::vector<cudaEvent_t>& joins,
+                   cudaEvent_t t0, cudaEvent_t t1, int periods, gr_autotune_result* out) {
+    if (ms.empty()) {
+        set_error("autotune: nothing to tune");
+        return GR_ERR_STATE;
+    }
+    const int nsnb = std::max(1, ms[0]->sys.prm.nsnb);
+    periods = std::max(1, periods);
+    gr_autotune_result r{};
+    float best = 3.0e38f;
+    int best_k = -1;
+    gr_status st;
+    for (int k = 0; k < kNumVariants; ++k) {
+        r.cand_layout[k] = kVariants[k].layout;
+        r.cand_cluster_size[k] = kVariants[k].width;
+        r.cand_ms_per_step[k] = -1.f;
+        bool ok = true;
+        for (gr_ctx* c : ms) {
+            gr_nb_params p = c->sys.prm;
+            p.water_layout = kVariants[k].layout;
+            p.cluster_size = kVariants[k].width;
+            if (c->sys.set_params(&p) != GR_OK) ok = false;
+        }
+        if (!ok) continue;
+        float t = 0.f;
+        // one untimed period: list growth and one-time kernel set-up happen here
+        if ((st = time_periods(ms, s0, fork, joins, t0, t1, nsnb, 1, &t))) return st;
+        if ((st = time_periods(ms, s0, fork, joins, t0, t1, nsnb, periods, &t))) return st;
+        r.cand_ms_per_step[k] = t;
+        if (t < best) {
+            best = t;
+            best_k = k;
+        }
+    }
+    r.n_candidates = kNumVariants;
+    if (best_k < 0) {
+        set_error("autotune: no variant applies");
+        return GR_ERR_UNSUPPORTED;
+    }
+    for (gr_ctx* c : ms) {
+        gr_nb_params p = c->sys.prm;
+        p.water_layout = kVariants[best_k].layout;
+        p.cluster_size = kVariants[best_k].width;
+        if ((st = c->sys.set_params(&p))) return st;
+        bool of = false;
+        GR_CUDA(cudaStreamSynchronize(c->stream));
+        if ((st = c->sys.resolve_pending(&of))) return st;
+        GR_CUDA(cudaMemset(c->sys.h.err, 0, 4 * sizeof(int)));  // trial overflows were absorbed by re-runs
+        c->sys.steps_since_update = c->sys.prm.nsnb;           // the next step rebuilds
+    }
+    r.water_layout = kVariants[best_k].layout;
+    r.cluster_size = kVariants[best_k].width;
+    if (out) *out = r;
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gr_status gr_autotune(gr_ctx* ctx, int32_t periods, gr_autotune_result* out) {
+    CTX_GUARD(ctx);
+    if (!ctx->sys.uploaded || !ctx->sys.params_set || !ctx->sys.box_set || !ctx->sys.pos_set) {
+        set_error("gr_autotune: needs topology, parameters, box and positions");
+        return GR_ERR_STATE;
+    }
+    if (ctx->sys.prm.kernel != GR_KERNEL_FIXED) {
+        set_error("gr_autotune: tunes the fixed-point kernel");
+        return GR_ERR_UNSUPPORTED;
+    }
+    std::vector<gr_ctx*> ms{ctx};
+    cudaEvent_t fork = nullptr, join = nullptr, t0 = nullptr, t1 = nullptr;
+    GR_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    GR_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    GR_CUDA(cudaEventCreate(&t0));
+    GR_CUDA(cudaEventCreate(&t1));
+    std::vector<cudaEvent_t> joins{join};
+    cudaStream_t s0 = nullptr;
+    GR_CUDA(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+    gr_status st = autotune(ms, s0, fork, joins, t0, t1, periods, out);
+    cudaStreamSynchronize(s0);
+    cudaStreamDestroy(s0);
+    for (cudaEvent_t e : {fork, join, t0, t1}) cudaEventDestroy(e);
+    return st;
+}
+
+gr_status gr_batch_autotune(gr_batch* b, int32_t periods, gr_autotune_result* out) {
+    BATCH_GUARD(b);
+    std::vector<gr_ctx*> ms;
+    std::vector<cudaEvent_t> joins;
+    for (auto& mb : b->m) {
+        ms.push_back(mb.ctx);
+        joins.push_back(mb.join);
+    }
+    gr_status st = autotune(ms, b->s0, b->fork, joins, b->t0, b->t1, periods, out);
+    if (st) return st;
+    for (auto& mb : b->m) mb.offset = int((b->nsnb - b->t % b->nsnb) % b->nsnb);  // every member rebuilds next
+    b->valid = false;
+    return GR_OK;
+}
+
+}  // extern "C"

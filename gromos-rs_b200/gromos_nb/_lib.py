@@ -83,6 +83,12 @@ class GrMdStats(C.Structure):
                 ("settle_failures", C.c_int32), ("rollbacks", C.c_int32)]
 
 
+class GrAutotuneResult(C.Structure):
+    _fields_ = [("water_layout", C.c_int32), ("cluster_size", C.c_int32), ("n_candidates", C.c_int32),
+                ("cand_layout", C.c_int32 * 4), ("cand_cluster_size", C.c_int32 * 4),
+                ("cand_ms_per_step", C.c_float * 4)]
+
+
 # symbol -> (restype, argtypes)
 _SIGNATURES = {
     "gr_ctx_create": (C.c_int32, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -118,6 +124,8 @@ _SIGNATURES = {
     "gr_batch_last_ms": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
     "gr_batch_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_ctx_device_bytes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "gr_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrAutotuneResult)]),
+    "gr_batch_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrAutotuneResult)]),
     "gr_lj_crf_innerloop_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                                 C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                                 C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,

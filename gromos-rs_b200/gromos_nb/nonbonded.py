@@ -244,6 +244,12 @@ class Forcefield:
         return {"forces": f, "e_lj": r.e_lj, "e_crf": r.e_crf, "dhdl": r.dhdl,
                 "virial": np.asarray(list(r.virial)).reshape(3, 3), "egroup_lj": glj, "egroup_crf": gcrf}
 
+    def autotune(self, periods: int = 2) -> Dict:
+        """Pick the fastest solvent kernel variant by timing pairlist periods (forces only)."""
+        r = _lib.GrAutotuneResult()
+        check(self._L.gr_autotune(self._h, int(periods), C.byref(r)))
+        return _autotune_dict(r)
+
     def device_bytes(self) -> int:
         n = C.c_int64(0)
         check(self._L.gr_ctx_device_bytes(self._h, C.byref(n)))
@@ -291,6 +297,12 @@ class Forcefield:
             pass
 
 
+def _autotune_dict(r) -> Dict:
+    cands = [{"water_layout": r.cand_layout[k], "cluster_size": r.cand_cluster_size[k],
+              "ms_per_step": float(r.cand_ms_per_step[k])} for k in range(r.n_candidates)]
+    return {"water_layout": r.water_layout, "cluster_size": r.cluster_size, "candidates": cands}
+
+
 class Batch:
     """Members (Forcefield objects) stepped together: one CUDA graph launch per MD step.
 
@@ -326,6 +338,11 @@ class Batch:
         """One force evaluation of every member (results: ``member.result()``); device ms."""
         check(self._L.gr_batch_eval(self._h, _lib.GR_EVAL_VIRIAL if virial else 0))
         return self.last_ms()
+
+    def autotune(self, periods: int = 2) -> Dict:
+        r = _lib.GrAutotuneResult()
+        check(self._L.gr_batch_autotune(self._h, int(periods), C.byref(r)))
+        return _autotune_dict(r)
 
     def last_ms(self) -> float:
         ms = C.c_float(0.0)

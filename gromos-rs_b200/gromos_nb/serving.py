@@ -1,0 +1,213 @@
+"""Continuous-batching MD job server on one GPU.
+
+Jobs (a system, a number of MD steps, initial velocities) arrive over time.
+The server keeps every admitted job resident on the device -- coordinates,
+velocities, pairlists, force caches -- and steps all resident jobs together
+through one :class:`~gromos_nb.nonbonded.Batch` (one CUDA graph launch per MD
+step for all of them).  Between chunks of steps it admits queued jobs while
+their device memory fits the HBM budget, and retires finished jobs, whose
+memory is freed at once.  A job that arrives while others run joins the
+running batch at the next chunk boundary: that is continuous batching, not a
+queue in front of a single-job runner.
+
+Admission: a job is admitted when the resident bytes plus its estimated
+bytes stay within ``hbm_budget``.  The estimate is ``n_atoms`` times the
+largest device-bytes-per-atom ratio seen so far (``bytes_per_atom`` until the
+first job has been measured); after admission the job is accounted with its
+measured bytes (``gr_ctx_device_bytes``).  A job whose measured bytes would
+exceed the budget is released again and waits.
+
+Every job's trajectory is bit-identical to a standalone run of the same job
+(fixed-point force sums, the same kernels per member), whatever else runs
+beside it.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from collections import deque
+from typing import Deque, Dict, List, Optional
+
+import numpy as np
+
+from . import generators
+from .nonbonded import Batch, Forcefield
+from .system import System
+
+
+@dataclasses.dataclass
+class Job:
+    job_id: int
+    system: System
+    n_steps: int
+    mass: np.ndarray
+    vel: np.ndarray
+    dt: float = 0.002
+    arrival: float = 0.0              # seconds since the server started
+    # filled in by the server
+    admitted: Optional[float] = None
+    finished: Optional[float] = None
+    steps_done: int = 0
+    result_pos: Optional[np.ndarray] = None
+    result_vel: Optional[np.ndarray] = None
+    stats: Optional[Dict] = None
+    device_bytes: int = 0
+    pairs_per_step: float = 0.0
+
+    @property
+    def latency(self) -> float:
+        return (self.finished - self.arrival) if self.finished is not None else float("nan")
+
+
+class Server:
+    """One GPU, one batch of resident jobs, admission by device memory."""
+
+    def __init__(self, hbm_budget: int, device: int = 0, chunk_steps: int = 5, bytes_per_atom: float = 8192.0,
+                 count_pairs: bool = False):
+        self.budget = int(hbm_budget)
+        self.device = device
+        self.chunk = max(1, int(chunk_steps))
+        self.bytes_per_atom = float(bytes_per_atom)
+        self.count_pairs = count_pairs
+        self.batch = Batch(device)
+        self.queue: Deque[Job] = deque()
+        self.resident: Dict[int, tuple] = {}   # job_id -> (job, Forcefield)
+        self.done: List[Job] = []
+        self.resident_bytes = 0
+        self.t0 = time.perf_counter()
+        self.gpu_ms = 0.0
+        self.steps_run = 0                     # batch steps
+        self.pair_steps = 0.0                  # atom-pair interactions evaluated (when counted)
+        self.sim_ps = 0.0                      # simulated time summed over jobs
+        self.max_resident_jobs = 0
+        self.max_resident_bytes = 0
+        self.joined_running = 0                # jobs admitted into a batch that was already stepping
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def submit(self, job: Job) -> None:
+        self.queue.append(job)
+
+    # ---- admission / retirement
+    def _admit(self) -> None:
+        while self.queue:
+            job = self.queue[0]
+            est = int(job.system.topo.n_atoms * self.bytes_per_atom)
+            if self.resident and self.resident_bytes + est > self.budget:
+                return
+            ff = Forcefield(job.system, device=self.device)
+            ff.upload_positions(job.system.pos)
+            if self.count_pairs:
+                r = ff.apply(job.system.pos, count_pairs=True, download_forces=False)
+                nsnb = max(1, job.system.params.nsnb)
+                job.pairs_per_step = r["n_pairs_short"] + r["n_pairs_long"] / nsnb
+                ff.upload_positions(job.system.pos)
+            ff.md_init(job.mass, job.vel, dt=job.dt, settle=True, dist_oh=0.1, dist_hh=generators.SPC_DHH)
+            nbytes = ff.device_bytes()
+            self.bytes_per_atom = max(self.bytes_per_atom if self.resident or self.done else 0.0,
+                                      nbytes / max(1, job.system.topo.n_atoms))
+            if self.resident and self.resident_bytes + nbytes > self.budget:
+                ff.close()                   # does not fit after all: wait for memory
+                return
+            self.queue.popleft()
+            if self.resident and self.steps_run > 0:
+                self.joined_running += 1
+            self.batch.add(ff)
+            job.admitted = self.now()
+            job.device_bytes = nbytes
+            self.resident[job.job_id] = (job, ff)
+            self.resident_bytes += nbytes
+            self.max_resident_jobs = max(self.max_resident_jobs, len(self.resident))
+            self.max_resident_bytes = max(self.max_resident_bytes, self.resident_bytes)
+
+    def _retire(self) -> None:
+        for jid in [j for j, (job, _) in self.resident.items() if job.steps_done >= job.n_steps]:
+            job, ff = self.resident.pop(jid)
+            self.batch.remove(ff)
+            job.result_pos, job.result_vel = ff.md_state()
+            job.stats = ff.md_stats()
+            job.finished = self.now()
+            ff.close()
+            self.resident_bytes -= job.device_bytes
+            self.done.append(job)
+
+    # ---- one scheduling round
+    def step(self) -> int:
+        """Admit, run one chunk of MD steps for every resident job, retire. Returns steps run."""
+        self._admit()
+        if not self.resident:
+            return 0
+        n = min(self.chunk, min(job.n_steps - job.steps_done for job, _ in self.resident.values()))
+        self.gpu_ms += self.batch.md_run(n)
+        self.steps_run += n
+        for job, _ in self.resident.values():
+            job.steps_done += n
+            self.pair_steps += job.pairs_per_step * n
+            self.sim_ps += job.dt * n
+        self._retire()
+        return n
+
+    def run(self, jobs: List[Job], timeout: float = 600.0) -> None:
+        """Serve ``jobs`` arriving at their ``arrival`` times (seconds from now)."""
+        pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        self.t0 = time.perf_counter()
+        while pending or self.queue or self.resident:
+            t = self.now()
+            if t > timeout:
+                raise TimeoutError("serving run exceeded its time limit")
+            while pending and pending[0].arrival <= t:
+                self.submit(pending.popleft())
+            if self.step() == 0 and pending and not self.queue:
+                time.sleep(max(0.0, min(pending[0].arrival - self.now(), 0.01)))
+
+    # ---- report
+    def report(self) -> Dict:
+        lat = np.array([j.latency for j in self.done])
+        wall = max((j.finished for j in self.done), default=0.0)
+        return {
+            "jobs": len(self.done),
+            "latency_p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+            "latency_p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+            "wall_s": wall,
+            "gpu_ms": self.gpu_ms,
+            "batch_steps": self.steps_run,
+            "pair_int_per_s": self.pair_steps / wall if wall > 0 and self.count_pairs else None,
+            "ns_per_day_aggregate": self.sim_ps * 1e-3 / wall * 86400.0 if wall > 0 else None,
+            "launches": self.batch.launches(),
+            "max_resident_jobs": self.max_resident_jobs,
+            "joined_running": self.joined_running,
+            "max_resident_bytes": self.max_resident_bytes,
+        }
+
+    def close(self) -> None:
+        for job, ff in self.resident.values():
+            self.batch.remove(ff)
+            ff.close()
+        self.resident.clear()
+        self.batch.close()
+
+
+def poisson_jobs(n_jobs: int, rate: float, seed: int, waters=(300, 20000), steps=(100, 2000),
+                 solute_prob: float = 0.5, solute_atoms=(50, 500), rc: float = 1.4, nsnb: int = 5,
+                 T: float = 300.0) -> List[Job]:
+    """Seeded Poisson arrival stream of MD jobs: uniform water counts and
+    lengths, an optional seeded solute (as in the batched REMD replicas)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    jobs = []
+    for k in range(n_jobs):
+        t += rng.exponential(1.0 / rate)
+        nw = int(rng.integers(waters[0], waters[1] + 1))
+        ns = int(rng.integers(solute_atoms[0], solute_atoms[1] + 1)) if rng.random() < solute_prob else 0
+        sseed = seed * 1000 + k
+        if ns >= 3:
+            s = generators.solvated_solute_system(nw, ns, seed=sseed, rc=rc, nsnb=nsnb)
+        else:
+            s = generators.spc_water_system(nw, box=generators.box_for_waters(nw), seed=sseed, rcutp=rc,
+                                            rcutl=rc, nsnb=nsnb)
+        m = generators.masses(s)
+        v = generators.maxwell_velocities(m, T, sseed + 7)
+        jobs.append(Job(job_id=k, system=s, n_steps=int(rng.integers(steps[0], steps[1] + 1)), mass=m, vel=v,
+                        arrival=t))
+    return jobs

@@ -241,6 +241,20 @@ gr_status gr_batch_eval(gr_batch* b, int32_t flags);
 gr_status gr_batch_last_ms(gr_batch* b, float* ms);
 /* Kernels launched by the batch's graphs so far. */
 gr_status gr_batch_launches(gr_batch* b, int64_t* n);
+/* Autotuner (no counterpart in gromos-rs): times full pairlist periods
+ * (rebuild + long-range refresh + NSNB short-range steps) of the system(s)
+ * for every solvent kernel variant -- lane layout x i-cluster width -- and
+ * keeps the fastest.  NSNB is not tuned: in the reference's twin-range
+ * scheme it decides which pairs are evaluated.  Tuning evaluates forces only
+ * (positions and velocities are untouched); the next step rebuilds. */
+typedef struct {
+    int32_t water_layout, cluster_size;   /* chosen variant (gr_nb_params fields) */
+    int32_t n_candidates;
+    int32_t cand_layout[4], cand_cluster_size[4];
+    float cand_ms_per_step[4];            /* device ms per step; -1 = not applicable */
+} gr_autotune_result;
+gr_status gr_autotune(gr_ctx* ctx, int32_t periods, gr_autotune_result* out);
+gr_status gr_batch_autotune(gr_batch* b, int32_t periods, gr_autotune_result* out);
 /* Device bytes held by a context (topology, lists, accumulators, MD state). */
 gr_status gr_ctx_device_bytes(gr_ctx* ctx, int64_t* bytes);
 

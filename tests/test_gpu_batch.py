@@ -121,3 +121,42 @@ def test_batch_launch_accounting():
     b.close()
     for ff in ffs:
         ff.close()
+
+
+def test_autotune_picks_a_variant_and_keeps_results():
+    s = g.spc_water_system(2000, box=g.box_for_waters(2000), seed=45, rcutp=0.8, rcutl=1.2, nsnb=5)
+    ff = Forcefield(s)
+    ff.upload_positions(s.pos)
+    r = ff.autotune(periods=1)
+    assert (r["water_layout"], r["cluster_size"]) in [(2, 4), (2, 8), (1, 4)]
+    assert all(c["ms_per_step"] > 0 for c in r["candidates"])
+    a = ff.apply(s.pos)
+    o = ob.OracleForcefield(s).apply(s.pos)
+    d = a["forces"] - o["forces"]
+    assert np.sqrt((d * d).sum() / (o["forces"] ** 2).sum()) <= 1e-5
+    ff.close()
+    b = Batch()
+    ffs = [member(x, 50 + k) for k, x in enumerate(systems()[:3])]
+    for f in ffs:
+        b.add(f)
+    rb = b.autotune(periods=1)
+    assert len(rb["candidates"]) == 3
+    b.md_run(6)
+    for k, f in enumerate(ffs):
+        x, v = f.md_state()
+        xr, vr = standalone_variant(systems()[k], 50 + k, 6, rb["water_layout"], rb["cluster_size"])
+        assert np.array_equal(x, xr) and np.array_equal(v, vr)
+    b.close()
+    for f in ffs:
+        f.close()
+
+
+def standalone_variant(s, seed, n, layout, width):
+    ff = Forcefield(s, cluster_size=width, water_layout=layout)
+    ff.upload_positions(s.pos)
+    m = g.masses(s)
+    ff.md_init(m, g.maxwell_velocities(m, 300.0, seed), dt=0.002, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    ff.md_run(n)
+    out = ff.md_state()
+    ff.close()
+    return out
