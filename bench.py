@@ -316,6 +316,26 @@ def run_gpu(args, rank, world, local_rank):
 # Batched workloads: REMD replicas, FEP lambda windows, serving.  Each prints
 # its own JSON line; the default workload above is the single large system.
 
+def _make_system(spec):
+    from gromos_nb import generators
+
+    nw, ns, seed, perturbed, lam = spec
+    s = generators.solvated_solute_system(nw, ns, seed=seed, perturbed=perturbed, lam=lam, rc=1.4, nsnb=5)
+    s.params.lam = lam
+    return s
+
+
+def _generate(specs):
+    """Seeded systems, generated on the host's cores by a spawn pool (no GPU
+    work has started in this process yet)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    with cf.ProcessPoolExecutor(max_workers=min(len(specs), os.cpu_count() or 1),
+                                mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_make_system, specs))
+
+
 def _member(s, seed, T, kernel="fixed"):
     from gromos_nb import generators
     from gromos_nb.nonbonded import Forcefield
@@ -364,20 +384,16 @@ def run_batched(args, kind):
     if kind == "remd":
         n = args.replicas
         temps = list(300.0 * (450.0 / 300.0) ** (np.arange(n) / max(1, n - 1)))
-        for r in range(n):
-            nw = int(rng.integers(500, 8001))
-            systems.append(generators.solvated_solute_system(nw, 200, seed=1003 + r, rc=1.4, nsnb=5))
-            seeds.append(5000 + r)
+        specs = [(int(rng.integers(500, 8001)), 200, 1003 + r, False, 0.0) for r in range(n)]
+        seeds = [5000 + r for r in range(n)]
         workload = f"remd_{n}_replicas_spc500-8000_solute200_rc1.4"
     else:
         lams = [round(0.05 * k, 2) for k in range(21)]
-        for k, lam in enumerate(lams):
-            s = generators.solvated_solute_system(5000, 30, seed=1004, perturbed=True, lam=lam, rc=1.4, nsnb=5)
-            s.params.lam = lam
-            systems.append(s)
-            seeds.append(6000)                      # same start in every window
-            temps.append(300.0)
+        specs = [(5000, 30, 1004, True, lam) for lam in lams]
+        seeds = [6000] * len(lams)                  # same start in every window
+        temps = [300.0] * len(lams)
         workload = "fep_21_windows_spc5000_solute30_rc1.4"
+    systems = _generate(specs)
     ffs = [_member(s, seed, T) for s, seed, T in zip(systems, seeds, temps)]
     pairs = [_pairs_per_step(ff, s) for ff, s in zip(ffs, systems)]
     b = Batch()

@@ -66,6 +66,30 @@ def _bad_molecules(pos: np.ndarray, mol: np.ndarray, box: float, dmin: float, is
     return np.unique(np.concatenate([mol[a[sel]], mol[b[sel]]]))
 
 
+def _bad_moved(kept_tree, kept_mol: np.ndarray, kept_is_h: np.ndarray, pos: np.ndarray, mol: np.ndarray,
+               box: float, dmin: float, is_h: np.ndarray, moved: np.ndarray, check: np.ndarray) -> np.ndarray:
+    """Molecules of ``check`` with an H-involving contact closer than dmin to
+    another molecule: against the never-moved molecules (``kept_tree``) and
+    against the current positions of the ``moved`` ones."""
+    from scipy.spatial import cKDTree
+
+    atoms = (3 * check[:, None] + np.arange(3)[None, :]).reshape(-1)
+    matoms = (3 * moved[:, None] + np.arange(3)[None, :]).reshape(-1)
+    q = np.mod(pos[atoms], box)
+    mtree = cKDTree(np.mod(pos[matoms], box), boxsize=box)
+    out = set()
+    for a, nb in zip(atoms, kept_tree.query_ball_point(q, dmin)):
+        if any(is_h[a] or kept_is_h[b] for b in nb):
+            out.add(int(mol[a]))
+    for a, nb in zip(atoms, mtree.query_ball_point(q, dmin)):
+        for bi in nb:
+            b = matoms[bi]
+            if mol[b] != mol[a] and (is_h[a] or is_h[b]):
+                out.add(int(mol[a]))
+                break
+    return np.array(sorted(out), dtype=np.int64)
+
+
 def spc_positions(n_waters: int, box: float, seed: int, jitter: float = 0.05, dmin: float = 0.15,
                   max_rounds: int = 200) -> np.ndarray:
     rng = np.random.default_rng(seed)
@@ -83,13 +107,27 @@ def spc_positions(n_waters: int, box: float, seed: int, jitter: float = 0.05, dm
     def place(Rm):
         return (centers[:, None, :] + np.einsum("nij,aj->nai", Rm, frame)).reshape(-1, 3)
 
+    from scipy.spatial import cKDTree
+
     pos = place(R)
+    bad = _bad_molecules(pos, mol, box, dmin, is_h)
+    if bad.size:
+        # the first round's bad molecules are the only ones ever re-oriented:
+        # the others keep the positions indexed here
+        moved = bad.copy()
+        keep = np.ones(n_waters, dtype=bool)
+        keep[moved] = False
+        katoms = np.nonzero(np.repeat(keep, 3))[0]
+        tree = cKDTree(np.mod(pos[katoms], box), boxsize=box)
+        tmol = mol[katoms]
+        tis_h = is_h[katoms]
     for _ in range(max_rounds):
-        bad = _bad_molecules(pos, mol, box, dmin, is_h)
         if bad.size == 0:
             break
+        # re-orient the molecules in contact, then re-check only those
         R[bad] = _random_rotations(rng, bad.size)
-        pos = place(R)
+        pos.reshape(n_waters, 3, 3)[bad] = centers[bad][:, None, :] + np.einsum("nij,aj->nai", R[bad], frame)
+        bad = _bad_moved(tree, tmol, tis_h, pos, mol, box, dmin, is_h, moved, bad)
     return pos
 
 
@@ -135,17 +173,29 @@ def solvated_solute_system(n_waters: int, n_solute_atoms: int, seed: int, rc: fl
         left -= s
     sizes.append(left)
     ncg = len(sizes)
-    # CG centres near the box centre, at least 0.55 nm apart (seeded rejection),
-    # so atoms of different CGs stay >= 0.25 nm apart
+    # CG centres near the box centre, at least 0.55 nm apart as periodic
+    # minimum images (seeded rejection), so atoms of different CGs stay
+    # >= 0.25 nm apart; the box grows when the solute does not fit
     spread = max(0.35, 0.42 * ncg ** (1.0 / 3.0))
     cg_centres = []
     tries = 0
+
+    def min_dist(c):
+        if not cg_centres:
+            return np.inf
+        d = np.asarray(cg_centres) - c
+        d -= box * np.round(d / box)
+        return float(np.sqrt((d * d).sum(axis=1)).min())
+
     while len(cg_centres) < ncg:
-        c = box / 2 + rng.uniform(-spread, spread, size=3)
-        if all(np.linalg.norm(c - d) >= 0.55 for d in cg_centres):
+        c = box / 2 + rng.uniform(-min(spread, box / 2), min(spread, box / 2), size=3)
+        if min_dist(c) >= 0.55:
             cg_centres.append(c)
         tries += 1
         if tries > 200 * ncg:
+            if spread >= box / 2:
+                box *= 1.02
+                cg_centres = [x - (box / 1.02) / 2 + box / 2 for x in cg_centres]
             spread *= 1.1
             tries = 0
     cg_centres = np.asarray(cg_centres)
