@@ -382,7 +382,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&h.f_out, size_t(N) * 3))) return st;
     if ((st = alloc(&h.e_out, size_t(acc_size(G))))) return st;
     if ((st = alloc(&h.err, 4))) return st;
-    if ((st = alloc(&h.n_deferred, 2))) return st;
+    if ((st = alloc(&h.n_deferred, 4))) return st;  // deferred counts [2] + water work counters [2]
     if ((st = alloc(&h.max_delta, 1))) return st;
     GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
     GR_CUDA(cudaMemset(h.f_long, 0, size_t(N) * 3 * sizeof(long long)));
@@ -778,7 +778,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         if (NCG > NSCG) {
             wp = water_params();
             (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
-            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 2 * sizeof(int), s));
+            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 4 * sizeof(int), s));
             if ((st = launch_water(s, wp, false))) return st;
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));

@@ -434,19 +434,48 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
 #pragma unroll
     for (int c = 0; c < W * 3; ++c) myrow[c] = make_float4(0.f, 0.f, 0.f, 0.f);
     long long acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const int stride = gridDim.x * kWaterWarps;
-    int ci = blockIdx.x * kWaterWarps + wid;
-    int ib = 0;
-    if (ci < nclus && lane < W * 3) cp_async16(&ibuf[wid][0][lane], wrec4 + 3 * (ci * W) + lane);
+    // Clusters are handed out dynamically (one counter per launch), so warps
+    // that drew cheap clusters take more and all warps finish together.  The
+    // next cluster's list head, i-records and first j-chunk are fetched while
+    // the current cluster's last chunk is computed.
+    int* __restrict__ ctr = s.n_deferred + (LONG ? 3 : 2);
+    auto fetch = [&]() {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(ctr, 1);
+        return __shfl_sync(0xffffffffu, c, 0);
+    };
+    int ci = fetch();
+    int ib = 0, jb = 0;
+    int cnt = 0;
+    uint32_t e_cur = 0u, e_nx = 0u;
+    if (ci < nclus) {
+        cnt = wn[ci];
+        const uint32_t* __restrict__ l0 = wl + static_cast<size_t>(ci) * wcap;
+        e_cur = lane < cnt ? __ldg(l0 + lane) : 0u;
+        e_nx = 32 + lane < cnt ? __ldg(l0 + 32 + lane) : 0u;
+        if (lane < W * 3) cp_async16(&ibuf[wid][ib][lane], wrec4 + 3 * (ci * W) + lane);
+        if (e_cur & 0xffu) {
+            const int js = static_cast<int>(e_cur >> 8);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][jb][3 * lane + q], wrec4 + 3 * js + q);
+        }
+    }
     cp_async_commit();
 
-    for (; ci < nclus; ci += stride) {
+    while (ci < nclus) {
         const int n = clus_n[ci];
         const int base = ci * W;
-        const int cnt = wn[ci];
         const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * wcap;
-        uint32_t e_cur = lane < cnt ? __ldg(list + lane) : 0u;
-        uint32_t e_nx = 32 + lane < cnt ? __ldg(list + 32 + lane) : 0u;
+        // the next cluster: index now, list head in flight during this cluster
+        const int cn = fetch();
+        int cnt_n = 0;
+        uint32_t raw0 = 0u, raw1 = 0u;
+        if (cn < nclus) {
+            cnt_n = wn[cn];
+            const uint32_t* __restrict__ ln = wl + static_cast<size_t>(cn) * wcap;
+            raw0 = __ldg(ln + lane);
+            if (32 + lane < wcap) raw1 = __ldg(ln + 32 + lane);
+        }
         cp_async_wait<0>();
         __syncwarp();
         const double x00 = rec_x(ibuf[wid][ib][0]), y00 = rec_y(ibuf[wid][ib][0]);
@@ -465,21 +494,26 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
             }
             sp[lane] = p;
         }
-        if (e_cur & 0xffu) {
-            const int js = static_cast<int>(e_cur >> 8);
-#pragma unroll
-            for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][0][3 * lane + q], wrec4 + 3 * js + q);
-        }
-        cp_async_commit();
-        __syncwarp();
         float elj = 0.f, ecrf = 0.f, v0s = 0.f, v1s = 0.f, v2s = 0.f, v3s = 0.f, v4s = 0.f, v5s = 0.f;
         const int nch = (cnt + 31) >> 5;
+        uint32_t e_cur_n = 0u, e_nx_n = 0u;
         for (int c = 0; c < nch; ++c) {
-            const int jb = c & 1;
-            if (c + 1 < nch && (e_nx & 0xffu)) {
-                const int js = static_cast<int>(e_nx >> 8);
+            if (c + 1 < nch) {
+                if (e_nx & 0xffu) {
+                    const int js = static_cast<int>(e_nx >> 8);
 #pragma unroll
-                for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][jb ^ 1][3 * lane + q], wrec4 + 3 * js + q);
+                    for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][jb ^ 1][3 * lane + q], wrec4 + 3 * js + q);
+                }
+            } else if (cn < nclus) {
+                // last chunk: the next cluster's i-records and first j-chunk
+                e_cur_n = lane < cnt_n ? raw0 : 0u;
+                e_nx_n = 32 + lane < cnt_n ? raw1 : 0u;
+                if (lane < W * 3) cp_async16(&ibuf[wid][ib ^ 1][lane], wrec4 + 3 * (cn * W) + lane);
+                if (e_cur_n & 0xffu) {
+                    const int js = static_cast<int>(e_cur_n >> 8);
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][jb ^ 1][3 * lane + q], wrec4 + 3 * js + q);
+                }
             }
             cp_async_commit();
             const int e2 = (c + 2) * 32 + lane;
@@ -587,11 +621,20 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
             }
             e_cur = e_nx;
             e_nx = e_nn;
+            jb ^= 1;
             __syncwarp();
         }
-        const int cn = ci + stride;
-        if (cn < nclus && lane < W * 3) cp_async16(&ibuf[wid][ib ^ 1][lane], wrec4 + 3 * (cn * W) + lane);
-        cp_async_commit();
+        if (nch == 0 && cn < nclus) {  // empty list: fetch the next cluster here
+            e_cur_n = lane < cnt_n ? raw0 : 0u;
+            e_nx_n = 32 + lane < cnt_n ? raw1 : 0u;
+            if (lane < W * 3) cp_async16(&ibuf[wid][ib ^ 1][lane], wrec4 + 3 * (cn * W) + lane);
+            if (e_cur_n & 0xffu) {
+                const int js = static_cast<int>(e_cur_n >> 8);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) cp_async16(&jbuf[wid][jb][3 * lane + q], wrec4 + 3 * js + q);
+            }
+            cp_async_commit();
+        }
         __syncwarp();
         // column sums of the lane rows: lane c < 3W owns i atom c (water c / 3)
         if (lane < W * 3) {
@@ -622,6 +665,10 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
         acc[6] += to_fixed_f(v4s, 16777216.0f);
         acc[7] += to_fixed_f(v5s, 16777216.0f);
         ib ^= 1;
+        ci = cn;
+        cnt = cnt_n;
+        e_cur = e_cur_n;
+        e_nx = e_nx_n;
         __syncwarp();
     }
     cp_async_wait<0>();
