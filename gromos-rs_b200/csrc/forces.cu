@@ -38,6 +38,7 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     double e_excl = 0.0;
+    float m = 0.f;
     if (slot < s.n_clusters[0] * s.W) {
         const int cg = s.slot_cg[slot];
         if (cg >= 0) {
@@ -55,9 +56,8 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
             w.h2z = float(s.pos[3 * a0 + 8] - z0);
             s.wrec[slot] = w;
             // extent of the molecule (per-atom images of the long list need it)
-            float m = fmaxf(fmaxf(fabsf(w.h1x), fabsf(w.h1y)), fmaxf(fabsf(w.h1z), fabsf(w.h2x)));
+            m = fmaxf(fmaxf(fabsf(w.h1x), fabsf(w.h1y)), fmaxf(fabsf(w.h1z), fabsf(w.h2x)));
             m = fmaxf(m, fmaxf(fabsf(w.h2y), fabsf(w.h2z)));
-            atomicMax(reinterpret_cast<int*>(s.max_delta), __float_as_int(m));
             // solvent excluded pairs: energy only, -q_i q_j fpe crf_2cut3i r^2
             // (rf_excluded_interactions, excluded.rs:81-96)
             if (s.excl_atoms < s.n_atoms)
@@ -71,6 +71,10 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
                     }
         }
     }
+    // one atomicMax per warp (the extents are >= 0, so their bit patterns order like the values)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(reinterpret_cast<int*>(s.max_delta), __float_as_int(m));
     if (s.excl_atoms < s.n_atoms) {
         long long v = warp_sum_ll(to_fixed_d(e_excl, kEnergyScale));
         __shared__ unsigned long long sh;

@@ -195,8 +195,10 @@ __device__ __forceinline__ long long to_fixed_f(float v, float scale) {
 }
 __device__ __forceinline__ long long to_fixed_d(double v, double scale) { return __double2ll_rn(v * scale); }
 
+// Fire-and-forget reduction into global memory (red, not atom: no value comes
+// back, so the issuing warp never waits on it).
 __device__ __forceinline__ void red_add(long long* addr, long long v) {
-    if (v != 0) atomicAdd(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(v));
+    if (v != 0) asm volatile("red.global.add.u64 [%0], %1;" ::"l"(addr), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ float warp_sum(float v) {
