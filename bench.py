@@ -217,8 +217,9 @@ def run_gpu(args, rank, world, local_rank):
     r0 = ff.apply(s.pos, count_pairs=True)
     n_short, n_long = int(r0["n_pairs_short"]), int(r0["n_pairs_long"])
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    graph = not args.no_graph
     for _ in range(args.warmup):
-        ff.eval_async()
+        ff.eval_async(graph=graph)
     torch.cuda.synchronize()
     # continue the cadence: the next eval after (1 + warmup) evals
     evals_done = 1 + args.warmup
@@ -235,7 +236,7 @@ def run_gpu(args, rank, world, local_rank):
         flush.zero_()                      # L2 flush between steps (not in the step's events)
         torch.cuda.synchronize()
         rebuild = (evals_done % s.params.nsnb) == 0
-        ff.eval_async()
+        ff.eval_async(graph=graph)
         evals_done += 1
         t = ff.timings()                   # CUDA events on the library's stream
         step_ms.append(t[4])
@@ -270,7 +271,7 @@ def run_gpu(args, rank, world, local_rank):
     e2e_pairs = 0
     for k in range(args.steps):
         rebuild = (evals_done % s.params.nsnb) == 0
-        ff.apply(pinned, count_pairs=False, out=fout)
+        ff.apply(pinned, count_pairs=False, out=fout, graph=graph)
         evals_done += 1
         e2e_pairs += n_short + (n_long if rebuild else 0)
     torch.cuda.synchronize()
@@ -294,6 +295,7 @@ def run_gpu(args, rank, world, local_rank):
                "config": {"workload": WORKLOAD, "n_atoms": s.topo.n_atoms, "box_nm": 9.65, "rcutp": 0.8,
                           "rcutl": 1.4, "nsnb": 5, "kernel": args.kernel, "cluster_size": args.cluster_size,
                           "water_layout": args.layout, "pairs_short_per_step": n_short,
+                          "launch": "kernel by kernel" if args.no_graph else "recorded CUDA graph per step",
                           "pairs_long_per_rebuild": n_long, "rebuild_steps_timed": rebuilds,
                           "l2": "flushed (256 MiB write) between steps, outside the step events",
                           "step": "value: force evaluation (positions static); md: force evaluation + leap-frog + SETTLE",
@@ -483,6 +485,7 @@ def main():
     ap.add_argument("--cluster-size", type=int, default=0, help="water i-cluster width 4 or 8 (0 = default)")
     ap.add_argument("--md-steps", type=int, default=1000, help="MD steps timed for ns/day")
     ap.add_argument("--layout", type=int, default=0, help="water kernel layout: 1 shared bits, 2 per-lane bits")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of replaying graphs")
     ap.add_argument("--workload", default="spc30000", choices=["spc30000", "remd", "fep", "serving"])
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=100)

@@ -103,6 +103,12 @@ void NbSystem::release() {
     if (err_host) cudaFreeHost(err_host);
     err_host = nullptr;
     pending_check = false;
+    drop_graphs();
+    if (err_step_host) cudaFreeHost(err_step_host);
+    err_step_host = nullptr;
+    if (ev_step) cudaEventDestroy(ev_step);
+    ev_step = nullptr;
+    step_check = false;
     // MD buffers were freed with `allocs`
     md_vel = md_mass = md_inv_mass = md_pos_snap = md_vel_snap = nullptr;
     md_ke = nullptr;
@@ -134,6 +140,7 @@ gr_status NbSystem::alloc(T** p, size_t n) {
     }
     allocs.push_back(*p);
     bytes += n * sizeof(T);
+    ++alloc_gen;
     return GR_OK;
 }
 
@@ -581,6 +588,13 @@ gr_status NbSystem::ensure_cgp_capacity() {
     return GR_OK;
 }
 
+// Events the host waits on or times: while a graph is being recorded they
+// become event-record nodes of the graph (external records), so replays
+// record them like a plain launch sequence would.
+cudaError_t NbSystem::record_event(cudaEvent_t e, cudaStream_t s) {
+    return in_capture ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
+}
+
 gr_status NbSystem::push_descriptor(cudaStream_t s) {
     if (in_capture) return GR_OK;
     GR_CUDA(cudaMemcpyAsync(d_sys, &h, sizeof(SysDev), cudaMemcpyHostToDevice, s));
@@ -693,7 +707,7 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
             // overflow flags are read back asynchronously and resolved by the next
             // call that synchronises (resolve_pending)
             GR_CUDA(cudaMemcpyAsync(err_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
-            GR_CUDA(cudaEventRecord(ev_err, s));
+            GR_CUDA(record_event(ev_err, s));
             pending_check = true;
             break;
         }
@@ -745,7 +759,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     if ((st = resolve_pending(&overflowed))) return st;
     if (overflowed) lr_computed = false;
     bool rebuild = !built || steps_since_update >= prm.nsnb || (flags & GR_EVAL_FORCE_REBUILD);
-    if (record_events) GR_CUDA(cudaEventRecord(ev[0], s));
+    if (record_events) GR_CUDA(record_event(ev[0], s));
     if (rebuild) {
         // the first build of a system synchronises to size the list capacities
         if ((st = build_pairlist(s, !ever_built))) return st;
@@ -757,7 +771,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     }
     last_rebuilt = rebuild;
     steps_since_update += 1;
-    if (record_events) GR_CUDA(cudaEventRecord(ev[1], s));
+    if (record_events) GR_CUDA(record_event(ev[1], s));
     const int NA = acc_size(G);
     GR_CUDA(cudaMemsetAsync(h.f_short, 0, size_t(N) * 3 * sizeof(long long), s));
     GR_CUDA(cudaMemsetAsync(h.acc_short, 0, size_t(NA) * sizeof(long long), s));
@@ -782,7 +796,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             if ((st = launch_water(s, wp, false))) return st;
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
-        if (record_events) GR_CUDA(cudaEventRecord(ev[2], s));
+        if (record_events) GR_CUDA(record_event(ev[2], s));
         if (do_long) {
             GR_CUDA(cudaMemsetAsync(h.f_long, 0, size_t(N) * 3 * sizeof(long long), s));
             GR_CUDA(cudaMemsetAsync(h.acc_long, 0, size_t(NA) * sizeof(long long), s));
@@ -803,7 +817,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         GR_CUDA(cudaMemsetAsync(h.e64, 0, 16 * sizeof(double), s));
         unsigned grid = std::max(1u, std::min(blocks_for(n_cgp_host[0], 256), unsigned(sm * 16)));
         (++launches, k_plain_force<<<grid, 256, 0, s>>>(d_sys, 0));
-        if (record_events) GR_CUDA(cudaEventRecord(ev[2], s));
+        if (record_events) GR_CUDA(record_event(ev[2], s));
         if (do_long) {
             GR_CUDA(cudaMemsetAsync(h.f32_long, 0, size_t(N) * 3 * sizeof(float), s));
             GR_CUDA(cudaMemsetAsync(h.e64_long, 0, 16 * sizeof(double), s));
@@ -812,7 +826,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             lr_computed = true;
         }
     }
-    if (record_events) GR_CUDA(cudaEventRecord(ev[3], s));
+    if (record_events) GR_CUDA(record_event(ev[3], s));
     const size_t sha = size_t(NA) * sizeof(unsigned long long);
     if (h.excl_atoms > 0) (++launches, k_excluded_14<<<blocks_for(h.excl_atoms, 128), 128, sha, s>>>(d_sys));
     if (n_pert > 0) {
@@ -821,8 +835,114 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     }
     (++launches, k_finalize<<<blocks_for(std::max<long long>(3LL * N, NA), 256), 256, 0, s>>>(d_sys, prm.kernel == GR_KERNEL_PLAIN));
     if (prm.kernel == GR_KERNEL_PLAIN) (++launches, k_finalize_plain_energies<<<1, 32, 0, s>>>(d_sys));
-    if (record_events) GR_CUDA(cudaEventRecord(ev[4], s));
+    if (record_events) GR_CUDA(record_event(ev[4], s));
     GR_CUDA(cudaGetLastError());
+    last_long = do_long;
+    return GR_OK;
+}
+
+void NbSystem::drop_graphs() {
+    for (auto& g : g_step) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    g_gen = -1;
+}
+
+// One evaluation replayed from a recorded CUDA graph: the whole step (memsets,
+// kernels, timing events, error-flag copies) is submitted with one launch, so
+// the kernels run back to back instead of waiting for the host's launches.
+// Two graphs are recorded on first use: the short-range step and the rebuild
+// step (pairlist build + long-range refresh); they are recorded again after
+// any device reallocation.  The host-side cadence (steps since the rebuild)
+// is kept exactly as eval() keeps it.  Cases the graphs do not cover (first
+// evaluation, plain kernel, a long-range refresh outside a rebuild step after
+// an overflow) run through eval().
+gr_status NbSystem::eval_graph(cudaStream_t s, int flags) {
+    gr_status st;
+    if (!err_step_host) GR_CUDA(cudaMallocHost(&err_step_host, 4 * sizeof(int)));
+    if (!ev_step) GR_CUDA(cudaEventCreateWithFlags(&ev_step, cudaEventDisableTiming));
+    if (step_check) {  // flags of the previous graph step (deferred-pair overflow)
+        GR_CUDA(cudaEventSynchronize(ev_step));
+        step_check = false;
+        if (err_step_host[0] & ERR_DEFER_OVERFLOW) {
+            GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
+            defer_want = std::max(defer_want, h.defer_cap) * 4;
+            clus_alloc = 0;
+            built = false;
+            lr_computed = false;
+            pending_check = false;
+            set_error("the previous evaluation overflowed the deferred-pair list; the list was grown, evaluate again");
+            return GR_ERR_OVERFLOW;
+        }
+    }
+    bool overflowed = false;
+    if ((st = resolve_pending(&overflowed))) return st;
+    if (overflowed) lr_computed = false;
+    const bool rebuild = !built || steps_since_update >= prm.nsnb || (flags & GR_EVAL_FORCE_REBUILD);
+    const bool do_long = h.twin && (rebuild || !lr_computed);
+    if (!ever_built || !warm || prm.kernel != GR_KERNEL_FIXED || (!rebuild && do_long)) {
+        st = eval(s, flags, true);
+        if (!st) warm = true;
+        return st;
+    }
+    if (g_gen != alloc_gen) {
+        drop_graphs();
+        if ((st = ensure_capacity())) return st;
+        if ((st = push_descriptor(s))) return st;
+        GR_CUDA(cudaStreamSynchronize(s));
+        const int ssu0 = steps_since_update;
+        const bool built0 = built, lr0 = lr_computed;
+        const long long l0 = launches;
+        in_capture = true;
+        for (int v = 0; v < 2 && !st; ++v) {
+            steps_since_update = v ? prm.nsnb : 1;
+            built = true;
+            lr_computed = true;
+            pending_check = false;
+            const long long lv = launches;
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                st = eval(s, v ? GR_EVAL_FORCE_REBUILD : 0, true);
+                if (!st) e = cudaMemcpyAsync(err_step_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s);
+                cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+                if (e == cudaSuccess) e = e2;
+            }
+            if (!st && e == cudaSuccess) e = cudaGraphInstantiate(&g_step[v], graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            g_step_launches[v] = launches - lv;
+            if (!st && e != cudaSuccess) {
+                set_error(std::string("evaluation graph: ") + cudaGetErrorString(e));
+                st = GR_ERR_CUDA;
+            }
+        }
+        in_capture = false;
+        launches = l0;
+        steps_since_update = ssu0;
+        built = built0;
+        lr_computed = lr0;
+        pending_check = false;
+        if (st) {
+            drop_graphs();
+            return st;
+        }
+        g_gen = alloc_gen;
+    }
+    GR_CUDA(cudaGraphLaunch(g_step[rebuild ? 1 : 0], s));
+    GR_CUDA(cudaEventRecord(ev_step, s));
+    step_check = true;
+    launches += g_step_launches[rebuild ? 1 : 0];
+    // the cadence eval() keeps
+    if (rebuild) {
+        built = true;
+        cgp_valid = false;
+        steps_since_update = 0;
+        pending_check = true;  // the rebuild's flags were copied to err_host inside the graph
+    }
+    last_rebuilt = rebuild;
+    steps_since_update += 1;
+    if (do_long) lr_computed = true;
     last_long = do_long;
     return GR_OK;
 }
@@ -1251,10 +1371,11 @@ gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out) {
     gr_status st;
     for (int attempt = 0;; ++attempt) {
         const bool had_pending = S.pending_check;
-        st = S.eval(ctx->stream, flags, true);
+        st = (flags & GR_EVAL_GRAPH) ? S.eval_graph(ctx->stream, flags) : S.eval(ctx->stream, flags, true);
         if (st) return st;
         if (!download) return GR_OK;  // overflow (if any) is reported by the next call
         if ((st = S.download(ctx->stream, out))) return st;
+        S.step_check = false;  // the flags are checked here, synchronously
         int errs[4] = {0, 0, 0, 0};
         if (cudaMemcpy(errs, S.h.err, sizeof(errs), cudaMemcpyDeviceToHost) == cudaSuccess &&
             (errs[0] & gnb::ERR_DEFER_OVERFLOW)) {

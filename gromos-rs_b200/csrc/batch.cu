@@ -44,6 +44,7 @@ struct gr_batch {
     long long t = 0;                   // batch MD steps done
     std::vector<cudaGraphExec_t> g;    // one graph per step phase (t mod NSNB)
     std::vector<long long> g_launches; // kernels per graph launch
+    std::vector<long long> gens;       // members' allocation generations the graphs were recorded with
     bool valid = false;
     cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
     int** d_errp = nullptr;            // device array of the members' err pointers
@@ -184,11 +185,13 @@ gr_status batch_capture(gr_batch* b) {
             return st;
         }
     }
+    b->gens.resize(n);
     for (int i = 0; i < n; ++i) {
         NbSystem& S = b->m[i].ctx->sys;
         S.in_capture = false;
         S.pending_check = false;
         S.launches = launches0[i];
+        b->gens[i] = S.alloc_gen;
     }
     b->valid = true;
     return GR_OK;
@@ -371,6 +374,11 @@ gr_status gr_batch_md_run(gr_batch* b, int32_t n_steps) {
     if ((st = batch_prepare(b, true))) return st;
     float total_ms = 0.f;
     for (int k = 0; k < n_steps; ++k) {
+        // a member reallocated since the graphs were recorded (parameters,
+        // list growth): record them again
+        if (b->valid)
+            for (size_t i = 0; i < b->m.size(); ++i)
+                if (b->gens[i] != b->m[i].ctx->sys.alloc_gen) b->valid = false;
         if (!b->valid && (st = batch_capture(b))) return st;
         const int p = int(b->t % b->nsnb);
         GR_CUDA(cudaEventRecord(b->t0, b->s0));

@@ -27,9 +27,12 @@ class NbSystem {
     gr_status resolve_pending(bool* overflowed);
     gr_status expand_cg_pairs(cudaStream_t s);
     gr_status eval(cudaStream_t s, int flags, bool record_events);
+    gr_status eval_graph(cudaStream_t s, int flags);
+    void drop_graphs();
     gr_status download(cudaStream_t s, gr_result* out);
     gr_status pair_counts(cudaStream_t s, long long* n_short, long long* n_long);
     gr_status push_descriptor(cudaStream_t s);
+    cudaError_t record_event(cudaEvent_t e, cudaStream_t s);
     int sm_count();
     WaterParams water_params(bool long_range = false) const;
     gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
@@ -82,6 +85,14 @@ class NbSystem {
     cudaEvent_t ev_md = nullptr;
     long long md_steps_total = 0, md_rollbacks = 0;
     bool warm = false;        // evaluated at least once with the current parameters
+    long long alloc_gen = 0;  // bumped by every device (re)allocation: recorded graphs are stale
+    // recorded evaluation graphs (GR_EVAL_GRAPH): [0] short-range step, [1] rebuild step
+    cudaGraphExec_t g_step[2] = {nullptr, nullptr};
+    long long g_step_launches[2] = {0, 0};
+    long long g_gen = -1;
+    int* err_step_host = nullptr;  // pinned: device error flags after the last graph step
+    cudaEvent_t ev_step = nullptr;
+    bool step_check = false;
     bool in_capture = false;  // recording a CUDA graph: the device descriptor is already current
 
    private:

@@ -23,7 +23,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
 GR_OK, GR_ERR_INVALID, GR_ERR_CUDA, GR_ERR_OOM, GR_ERR_STATE = 0, 1, 2, 3, 4
 GR_ERR_UNSUPPORTED, GR_ERR_OVERFLOW, GR_ERR_TIMEOUT, GR_ERR_NO_DEVICE = 5, 6, 7, 8
 GR_KERNEL_FIXED, GR_KERNEL_PLAIN = 0, 1
-GR_EVAL_VIRIAL, GR_EVAL_FORCE_REBUILD, GR_EVAL_NO_DOWNLOAD = 1, 2, 4
+GR_EVAL_VIRIAL, GR_EVAL_FORCE_REBUILD, GR_EVAL_NO_DOWNLOAD, GR_EVAL_GRAPH = 1, 2, 4, 8
 
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)

@@ -154,12 +154,15 @@ class Forcefield:
 
     # ---- evaluation
     def apply(self, pos=None, virial: bool = True, force_rebuild: bool = False, count_pairs: bool = True,
-              download_forces: bool = True, out: Optional[np.ndarray] = None) -> Dict:
+              download_forces: bool = True, out: Optional[np.ndarray] = None, graph: bool = False) -> Dict:
         """One Forcefield::apply.  ``out`` (n_atoms, 3) float64, ideally in
-        pinned memory, receives the forces without a per-call allocation."""
+        pinned memory, receives the forces without a per-call allocation;
+        ``graph`` replays the step from a recorded CUDA graph."""
         if pos is not None:
             self.upload_positions(pos)
         flags = (_lib.GR_EVAL_VIRIAL if virial else 0) | (_lib.GR_EVAL_FORCE_REBUILD if force_rebuild else 0)
+        if graph:
+            flags |= _lib.GR_EVAL_GRAPH
         if out is not None:
             if out.shape != (self.n_atoms, 3) or out.dtype != np.float64 or not out.flags.c_contiguous:
                 raise ValueError("out must be a C-contiguous float64 (n_atoms, 3) array")
@@ -177,9 +180,11 @@ class Forcefield:
                 "virial": np.asarray(list(r.virial)).reshape(3, 3), "egroup_lj": glj, "egroup_crf": gcrf,
                 "n_pairs_short": r.n_pairs_short, "n_pairs_long": r.n_pairs_long, "rebuilt": bool(r.rebuilt)}
 
-    def eval_async(self, force_rebuild: bool = False) -> None:
+    def eval_async(self, force_rebuild: bool = False, graph: bool = False) -> None:
         """Evaluate without reading results back (device-resident pipelines)."""
         flags = _lib.GR_EVAL_VIRIAL | _lib.GR_EVAL_NO_DOWNLOAD | (_lib.GR_EVAL_FORCE_REBUILD if force_rebuild else 0)
+        if graph:
+            flags |= _lib.GR_EVAL_GRAPH
         check(self._L.gr_forces_eval(self._h, flags, None))
 
     def timings(self) -> List[float]:

@@ -55,7 +55,10 @@ enum {
 enum {
     GR_EVAL_VIRIAL = 1,           /* compute the virial tensor */
     GR_EVAL_FORCE_REBUILD = 2,    /* rebuild the pairlist now regardless of NSNB */
-    GR_EVAL_NO_DOWNLOAD = 4       /* keep results on the device (read them later) */
+    GR_EVAL_NO_DOWNLOAD = 4,      /* keep results on the device (read them later) */
+    GR_EVAL_GRAPH = 8             /* replay the step from a recorded CUDA graph (recorded on first
+                                     use, again after reallocation); with GR_EVAL_NO_DOWNLOAD a
+                                     deferred-pair overflow is reported by the next call */
 };
 
 /* Perturbed atom: PertAtomInfo (crates/gromos-forces/src/nonbonded/perturbed.rs:271-279);
