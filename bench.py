@@ -338,7 +338,8 @@ def _generate(specs):
         return list(ex.map(_make_system, specs))
 
 
-def _member(s, seed, T, kernel="fixed"):
+def _member(s, seed, T, kernel="fixed", tau=0.1):
+    """A replica: seeded Maxwell-Boltzmann start at T, Berendsen bath at T (tau in ps)."""
     from gromos_nb import generators
     from gromos_nb.nonbonded import Forcefield
 
@@ -346,7 +347,7 @@ def _member(s, seed, T, kernel="fixed"):
     ff.upload_positions(s.pos)
     m = generators.masses(s)
     ff.md_init(m, generators.maxwell_velocities(m, T, seed), dt=DT_PS, settle=True, dist_oh=0.1,
-               dist_hh=generators.SPC_DHH)
+               dist_hh=generators.SPC_DHH, temperature=T, tau=tau)
     return ff
 
 
@@ -433,7 +434,8 @@ def run_batched(args, kind):
             "data": "synthetic (seeded water boxes + seeded solutes)",
             "config": {"workload": workload, "members": len(systems),
                        "atoms_total": int(sum(s.topo.n_atoms for s in systems)),
-                       "pairs_per_batch_step": float(sum(pairs)), "step": "MD step (forces + leap-frog + SETTLE)",
+                       "pairs_per_batch_step": float(sum(pairs)),
+                       "step": "MD step (forces + leap-frog + Berendsen bath at the replica temperature + SETTLE)",
                        "launch": "one CUDA graph launch per batch step", "autotune": tune},
             "gpu_launches": launches,
             "one_by_one": {"sample_members": len(idx), "steps": steps_alone,

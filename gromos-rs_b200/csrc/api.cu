@@ -112,6 +112,7 @@ void NbSystem::release() {
     // MD buffers were freed with `allocs`
     md_vel = md_mass = md_inv_mass = md_pos_snap = md_vel_snap = nullptr;
     md_ke = nullptr;
+    md_ke_snap = nullptr;
     md_fail = nullptr;
     if (md_err_host) cudaFreeHost(md_err_host);
     md_err_host = nullptr;

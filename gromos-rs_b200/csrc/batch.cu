@@ -150,6 +150,8 @@ gr_status batch_capture(gr_batch* b) {
             if (ph == 0) {  // pairlist period starts: snapshot for rollback, then rebuild
                 e = cudaMemcpyAsync(S.md_pos_snap, S.h.pos, bytes3, cudaMemcpyDeviceToDevice, si);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(S.md_vel_snap, S.md_vel, bytes3, cudaMemcpyDeviceToDevice, si);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(S.md_ke_snap, S.md_ke, sizeof(long long), cudaMemcpyDeviceToDevice, si);
                 if (e != cudaSuccess) break;
                 S.steps_since_update = S.prm.nsnb;
             } else {
@@ -218,6 +220,7 @@ gr_status batch_recover(gr_batch* b, gr_batch::Member& mb, int flags, int steps)
     const size_t bytes3 = size_t(S.N) * 3 * sizeof(double);
     GR_CUDA(cudaMemcpyAsync(S.h.pos, S.md_pos_snap, bytes3, cudaMemcpyDeviceToDevice, si));
     GR_CUDA(cudaMemcpyAsync(S.md_vel, S.md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, si));
+    GR_CUDA(cudaMemcpyAsync(S.md_ke, S.md_ke_snap, sizeof(long long), cudaMemcpyDeviceToDevice, si));
     S.steps_since_update = S.prm.nsnb;
     S.built = false;
     S.lr_computed = false;

@@ -24,9 +24,35 @@ struct MdDev {
     double dt, dt_i;
     int settle;               // SETTLE every solvent molecule
     double m_o, m_h, ra, rb, rc;  // canonical SETTLE triangle (constraints.rs:836-840)
-    long long* ke;            // [1] kinetic energy, fixed point 2^24
+    long long* ke;            // [2]: [0] kinetic energy of the velocities entering the step, [1] accumulator
+                              // of the velocities leaving it (fixed point 2^24)
     int* failures;            // [1] molecules SETTLE could not solve
+    double t0, tau, dof;      // Berendsen bath (tau < 0: none)
 };
+
+// Berendsen weak coupling (berendsen_thermostat.rs:74-98): lambda from the
+// kinetic energy of the velocities entering this step.
+__device__ __forceinline__ double berendsen_lambda(const MdDev& md) {
+    if (md.tau < 0.0) return 1.0;
+    const double kB = 0.00831446261815324;
+    const double ekin = double(md.ke[0]) / kEnergyScale;
+    double t = md.dof > 0.0 ? 2.0 * ekin / (md.dof * kB) : 0.0;
+    if (t < 1e-10) t = md.t0;
+    if (t < 1e-10) return 1.0;
+    return md.tau == 0.0 ? sqrt(md.t0 / t) : sqrt(1.0 + md.dt / md.tau * (md.t0 / t - 1.0));
+}
+
+// The accumulated kinetic energy becomes the next step's input.
+__global__ void k_ke_commit(long long* ke) {
+    ke[0] = ke[1];
+    ke[1] = 0;
+}
+
+// Velocities scaled by `f` (temperature exchange), kinetic energy with them.
+__global__ void k_scale_velocities(double* __restrict__ vel, int n3, double f, long long* ke) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) vel[i] *= f;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ke[0] = __double2ll_rn(double(ke[0]) * f * f);
+}
 
 struct D3 {
     double x, y, z;
@@ -105,6 +131,7 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
     const int nsa = s.n_solute_atoms, n = s.n_atoms;
     const int n_mol = md.settle ? (n - nsa) / 3 : 0;
     const int n_units = md.settle ? nsa + n_mol : n;
+    const double lambda = berendsen_lambda(md);
     long long ke = 0;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n_units; u += gridDim.x * blockDim.x) {
         const bool mol = md.settle && u >= nsa;
@@ -115,7 +142,7 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
             const int i = a0 + k;
             const D3 f = d3(s.f_out[3 * i], s.f_out[3 * i + 1], s.f_out[3 * i + 2]);
             const double im = md.inv_mass[i];
-            v[k] = d3(md.vel[3 * i], md.vel[3 * i + 1], md.vel[3 * i + 2]) + f * im * md.dt;
+            v[k] = (d3(md.vel[3 * i], md.vel[3 * i + 1], md.vel[3 * i + 2]) + f * im * md.dt) * lambda;
             old[k] = d3(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2]);
             nw[k] = old[k] + v[k] * md.dt;
         }
@@ -132,7 +159,7 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
         }
     }
     ke = warp_sum_ll(ke);
-    if ((threadIdx.x & 31) == 0 && ke) atomicAdd(reinterpret_cast<unsigned long long*>(md.ke),
+    if ((threadIdx.x & 31) == 0 && ke) atomicAdd(reinterpret_cast<unsigned long long*>(md.ke + 1),
                                                   static_cast<unsigned long long>(ke));
 }
 
@@ -181,9 +208,16 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
     gr_status st;
     if ((st = upload_array(&md_mass, mass, N)) || (st = upload_array(&md_inv_mass, inv.data(), N)) ||
         (st = upload_array(&md_vel, v0.data(), size_t(N) * 3)) || (st = alloc(&md_pos_snap, size_t(N) * 3)) ||
-        (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 1)) || (st = alloc(&md_fail, 1)))
+        (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 2)) || (st = alloc(&md_ke_snap, 1)) ||
+        (st = alloc(&md_fail, 1)))
         return st;
-    GR_CUDA(cudaMemset(md_ke, 0, sizeof(long long)));
+    {
+        double ke0 = 0.0;
+        for (int i = 0; i < N; ++i)
+            ke0 += 0.5 * mass[i] * (v0[3 * i] * v0[3 * i] + v0[3 * i + 1] * v0[3 * i + 1] + v0[3 * i + 2] * v0[3 * i + 2]);
+        const long long k[2] = {static_cast<long long>(std::llround(ke0 * kEnergyScale)), 0};
+        GR_CUDA(cudaMemcpy(md_ke, k, sizeof(k), cudaMemcpyHostToDevice));
+    }
     GR_CUDA(cudaMemset(md_fail, 0, sizeof(int)));
     md_steps_total = 0;
     md_rollbacks = 0;
@@ -191,6 +225,8 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
     if (!ev_md) GR_CUDA(cudaEventCreateWithFlags(&ev_md, cudaEventDisableTiming));
     mdp = *p;
     md_settle = settle;
+    // degrees of freedom: 3N minus the solvent constraints (md.rs:1158-1172; NDFMIN 0)
+    md_dof = 3.0 * N - (settle ? 3.0 * ((N - NSA) / 3) : 0.0);
     if (settle) {  // canonical triangle (constraints.rs:836-840)
         md_m_o = mass[NSA];
         md_m_h = mass[NSA + 1];
@@ -219,10 +255,13 @@ gr_status NbSystem::md_step_launch(cudaStream_t s) {
     md.rc = md_rc;
     md.ke = md_ke;
     md.failures = md_fail;
+    md.t0 = mdp.temperature;
+    md.tau = mdp.tau;
+    md.dof = md_dof;
     const int n_units = md_settle ? NSA + (N - NSA) / 3 : N;
     const unsigned grid = std::max(1u, std::min(unsigned((n_units + 255) / 256), unsigned(sm_count() * 8)));
-    GR_CUDA(cudaMemsetAsync(md_ke, 0, sizeof(long long), s));
     (++launches, k_md_step<<<grid, 256, 0, s>>>(d_sys, md));
+    (++launches, k_ke_commit<<<1, 1, 0, s>>>(md_ke));
     return GR_OK;
 }
 
@@ -264,6 +303,7 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
         // snapshot at the start of the period
         GR_CUDA(cudaMemcpyAsync(md_pos_snap, h.pos, bytes3, cudaMemcpyDeviceToDevice, s));
         GR_CUDA(cudaMemcpyAsync(md_vel_snap, md_vel, bytes3, cudaMemcpyDeviceToDevice, s));
+        GR_CUDA(cudaMemcpyAsync(md_ke_snap, md_ke, sizeof(long long), cudaMemcpyDeviceToDevice, s));
         const int ssu0 = steps_since_update;
         bool overflow = false;
         int k = 0;
@@ -315,6 +355,7 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
             }
             GR_CUDA(cudaMemcpyAsync(h.pos, md_pos_snap, bytes3, cudaMemcpyDeviceToDevice, s));
             GR_CUDA(cudaMemcpyAsync(md_vel, md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, s));
+            GR_CUDA(cudaMemcpyAsync(md_ke, md_ke_snap, sizeof(long long), cudaMemcpyDeviceToDevice, s));
             steps_since_update = ssu0;
             built = false;  // the period is re-run from a fresh build with the grown lists
             lr_computed = false;
@@ -344,6 +385,40 @@ gr_status gr_md_init(gr_ctx* ctx, const double* mass, const double* vel, const g
 gr_status gr_md_run(gr_ctx* ctx, int32_t n_steps, gr_md_stats* out) {
     CTX_GUARD(ctx);
     return ctx->sys.md_run(ctx->stream, n_steps, out);
+}
+
+gr_status gr_md_set_temperature(gr_ctx* ctx, double t0, int32_t rescale_velocities) {
+    CTX_GUARD(ctx);
+    NbSystem& S = ctx->sys;
+    if (!S.md_ready) {
+        set_error("gr_md_set_temperature before gr_md_init");
+        return GR_ERR_STATE;
+    }
+    if (!(t0 > 0.0)) {
+        set_error("gr_md_set_temperature: t0 must be positive");
+        return GR_ERR_INVALID;
+    }
+    if (rescale_velocities) {
+        // Replica::rescale_velocities (replica.rs:355-371): scale to t0 from the
+        // instantaneous temperature over 3N degrees of freedom
+        long long ke = 0;
+        GR_CUDA(cudaMemcpyAsync(&ke, S.md_ke, sizeof(ke), cudaMemcpyDeviceToHost, ctx->stream));
+        GR_CUDA(cudaStreamSynchronize(ctx->stream));
+        const double t_now = 2.0 * (double(ke) / gnb::kEnergyScale) / (3.0 * S.N * 0.00831446261815324);
+        if (!(t_now > 0.0)) {
+            S.mdp.temperature = t0;
+            S.alloc_gen++;
+            return GR_OK;
+        }
+        const double f = std::sqrt(t0 / t_now);
+        const int n3 = 3 * S.N;
+        (++S.launches, gnb::k_scale_velocities<<<std::max(1, std::min((n3 + 255) / 256, 1024)), 256, 0, ctx->stream>>>(
+            S.md_vel, n3, f, S.md_ke));
+        GR_CUDA(cudaGetLastError());
+    }
+    S.mdp.temperature = t0;
+    S.alloc_gen++;  // the thermostat target is a kernel parameter of recorded graphs
+    return GR_OK;
 }
 
 gr_status gr_md_stats_get(gr_ctx* ctx, gr_md_stats* out) {

@@ -79,7 +79,9 @@ class NbSystem {
     double md_m_o = 0, md_m_h = 0, md_ra = 0, md_rb = 0, md_rc = 0;
     double *md_vel = nullptr, *md_mass = nullptr, *md_inv_mass = nullptr;
     double *md_pos_snap = nullptr, *md_vel_snap = nullptr;
-    long long* md_ke = nullptr;
+    long long* md_ke = nullptr;      // [2]: kinetic energy entering the next step, accumulator
+    long long* md_ke_snap = nullptr;
+    double md_dof = 0.0;
     int* md_fail = nullptr;
     long long* md_err_host = nullptr;  // pinned
     cudaEvent_t ev_md = nullptr;

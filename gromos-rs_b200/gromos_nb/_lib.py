@@ -75,7 +75,8 @@ class GrResult(C.Structure):
 
 
 class GrMdParams(C.Structure):
-    _fields_ = [("dt", C.c_double), ("settle", C.c_int32), ("dist_oh", C.c_double), ("dist_hh", C.c_double)]
+    _fields_ = [("dt", C.c_double), ("settle", C.c_int32), ("dist_oh", C.c_double), ("dist_hh", C.c_double),
+                ("temperature", C.c_double), ("tau", C.c_double)]
 
 
 class GrMdStats(C.Structure):
@@ -114,6 +115,7 @@ _SIGNATURES = {
     "gr_md_run": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrMdStats)]),
     "gr_md_download": (C.c_int32, [C.c_void_p, _f64p, _f64p]),
     "gr_md_stats_get": (C.c_int32, [C.c_void_p, C.POINTER(GrMdStats)]),
+    "gr_md_set_temperature": (C.c_int32, [C.c_void_p, C.c_double, C.c_int32]),
     "gr_batch_create": (C.c_int32, [C.c_int, C.POINTER(C.c_void_p)]),
     "gr_batch_destroy": (C.c_int32, [C.c_void_p]),
     "gr_batch_add": (C.c_int32, [C.c_void_p, C.c_void_p]),

@@ -212,15 +212,21 @@ class Forcefield:
 
     # ---- MD (leap-frog + SETTLE around the force call, device resident)
     def md_init(self, mass, vel=None, dt: float = 0.002, settle: bool = True, dist_oh: float = 0.1,
-                dist_hh: float = 0.1633) -> None:
-        """Positions are those of the last upload; ``vel`` are v(-dt/2) (None = zero)."""
+                dist_hh: float = 0.1633, temperature: float = 300.0, tau: float = -1.0) -> None:
+        """Positions are those of the last upload; ``vel`` are v(-dt/2) (None = zero).
+        ``tau`` >= 0 couples to a Berendsen bath at ``temperature`` (tau < 0: NVE)."""
         m = np.ascontiguousarray(mass, dtype=np.float64)
         v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64)
         if m.shape != (self.n_atoms,) or (v is not None and v.shape != (self.n_atoms, 3)):
             raise ValueError("mass must be (n_atoms,), vel (n_atoms, 3)")
         self._md_mass, self._md_vel = m, v
-        mp = _lib.GrMdParams(dt, 1 if settle else 0, dist_oh, dist_hh)
+        mp = _lib.GrMdParams(dt, 1 if settle else 0, dist_oh, dist_hh, temperature, tau)
+        self.temperature = temperature
         check(self._L.gr_md_init(self._h, _p(m, C.c_double), _p(v, C.c_double), C.byref(mp)))
+
+    def md_set_temperature(self, t0: float, rescale_velocities: bool = True) -> None:
+        check(self._L.gr_md_set_temperature(self._h, float(t0), 1 if rescale_velocities else 0))
+        self.temperature = t0
 
     def md_run(self, n_steps: int) -> Dict:
         st = _lib.GrMdStats()

@@ -1,0 +1,116 @@
+"""Temperature replica exchange over a batch of replicas on one GPU.
+
+Restates the exchange controller of gromos-rs (crates/gromos-integrators/src/
+remd.rs:168-420): replicas run ``exchange_interval`` MD steps (here all in
+one batch, one CUDA graph launch per step, each with its own Berendsen bath,
+berendsen_thermostat.rs:58-118), then neighbouring replicas on the
+temperature ladder attempt an exchange with the Metropolis criterion
+``delta = (beta_1 - beta_2) (E_2 - E_1)``, accepted when a uniform number is
+below ``min(1, exp(-delta))`` (remd.rs:259-308).  Pairs follow the odd-even
+scheme (remd.rs:211-226) or the sequential one.
+
+An accepted exchange swaps the two replicas' temperatures instead of their
+coordinates -- the same ensemble move without moving coordinates across the
+device -- and rescales each replica's velocities to its new temperature
+(replica.rs:355-371).  The random numbers come from a seeded generator, so
+runs are reproducible (the reference draws from the thread RNG).
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from .nonbonded import Batch, Forcefield
+
+KB = 0.00831446261815324  # kJ mol^-1 K^-1
+
+
+class ReplicaExchange:
+    def __init__(self, replicas: Sequence[Forcefield], temperatures: Sequence[float], exchange_interval: int = 100,
+                 scheme: str = "odd_even", seed: int = 0, equilibration_steps: int = 0,
+                 rescale_velocities: bool = True, batch: Optional[Batch] = None):
+        if len(replicas) != len(temperatures) or len(replicas) < 2:
+            raise ValueError("need one temperature per replica and at least two replicas")
+        if len({r.n_atoms for r in replicas}) != 1:
+            raise ValueError("temperature exchange needs replicas of one system")
+        if scheme not in ("odd_even", "sequential"):
+            raise ValueError("scheme must be odd_even or sequential")
+        self.replicas = list(replicas)
+        self.ladder = sorted(float(t) for t in temperatures)
+        # position on the ladder of each replica, and the replica at each position
+        order = np.argsort(np.asarray(temperatures, dtype=float), kind="stable")
+        self.at = [0] * len(replicas)
+        for pos, r in enumerate(order):
+            self.at[int(r)] = pos
+        self.interval = max(1, int(exchange_interval))
+        self.scheme = scheme
+        self.rng = np.random.default_rng(seed)
+        self.equilibration = int(equilibration_steps)
+        self.rescale = rescale_velocities
+        self.odd_even_state = False
+        self.step = 0
+        self.attempts = np.zeros(len(replicas) - 1, dtype=np.int64)
+        self.accepts = np.zeros(len(replicas) - 1, dtype=np.int64)
+        self.own_batch = batch is None
+        self.batch = batch or Batch()
+        if self.own_batch:
+            for r in self.replicas:
+                self.batch.add(r)
+        for r, pos in zip(self.replicas, self.at):
+            r.md_set_temperature(self.ladder[pos], rescale_velocities=False)
+
+    def replica_at(self, pos: int) -> int:
+        return self.at.index(pos)
+
+    def temperature_of(self, replica: int) -> float:
+        return self.ladder[self.at[replica]]
+
+    def _pairs(self) -> List[tuple]:
+        n = len(self.replicas)
+        if self.scheme == "sequential":
+            start = 0
+        else:
+            start = 0 if self.odd_even_state else 1
+            self.odd_even_state = not self.odd_even_state
+        return [(p, p + 1) for p in range(start, n - 1, 2)]
+
+    def attempt_exchanges(self) -> None:
+        if self.step < self.equilibration:
+            return
+        energy = [st["e_lj"] + st["e_crf"] for st in (r.md_stats() for r in self.replicas)]
+        for p, q in self._pairs():
+            a, b = self.replica_at(p), self.replica_at(q)
+            beta_a, beta_b = 1.0 / (KB * self.ladder[p]), 1.0 / (KB * self.ladder[q])
+            delta = (beta_a - beta_b) * (energy[b] - energy[a])
+            prob = 1.0 if delta < 0.0 else float(np.exp(-delta))
+            accepted = self.rng.random() < prob
+            self.attempts[p] += 1
+            if accepted:
+                self.accepts[p] += 1
+                self.at[a], self.at[b] = q, p
+                self.replicas[a].md_set_temperature(self.ladder[q], rescale_velocities=self.rescale)
+                self.replicas[b].md_set_temperature(self.ladder[p], rescale_velocities=self.rescale)
+
+    def run(self, total_steps: int) -> None:
+        done = 0
+        while done < total_steps:
+            n = min(self.interval, total_steps - done)
+            self.batch.md_run(n)
+            done += n
+            self.step += n
+            if self.step % self.interval == 0:
+                self.attempt_exchanges()
+
+    def statistics(self) -> Dict:
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rate = np.where(self.attempts > 0, self.accepts / np.maximum(self.attempts, 1), 0.0)
+        return {"attempts": self.attempts.tolist(), "accepts": self.accepts.tolist(),
+                "acceptance": rate.tolist(), "temperatures": [self.temperature_of(r) for r in
+                                                              range(len(self.replicas))]}
+
+    def close(self) -> None:
+        if self.own_batch:
+            for r in self.replicas:
+                self.batch.remove(r)
+            self.batch.close()

@@ -199,6 +199,8 @@ typedef struct {
     int32_t settle;   /* 1: SETTLE every 3-site solvent molecule */
     double dist_oh;   /* SETTLE constraint lengths, nm (solvent_constraint_template 0 and 2) */
     double dist_hh;
+    double temperature; /* Berendsen reference temperature T0, K */
+    double tau;         /* Berendsen coupling time, ps (berendsen_thermostat.rs:58-118); < 0 = none (NVE) */
 } gr_md_params;
 
 typedef struct {
@@ -214,6 +216,11 @@ typedef struct {
 gr_status gr_md_init(gr_ctx* ctx, const double* mass, const double* vel, const gr_md_params* params);
 /* Runs n_steps MD steps on the context's stream; out may be NULL. */
 gr_status gr_md_run(gr_ctx* ctx, int32_t n_steps, gr_md_stats* out);
+/* New Berendsen reference temperature (an accepted replica exchange); with
+ * rescale_velocities the velocities are scaled to t0 from the instantaneous
+ * temperature over 3N degrees of freedom (replica.rs:355-371, called by
+ * remd.rs perform_exchange).  Takes effect for the next step. */
+gr_status gr_md_set_temperature(gr_ctx* ctx, double t0, int32_t rescale_velocities);
 /* Statistics of the last step and totals since gr_md_init. */
 gr_status gr_md_stats_get(gr_ctx* ctx, gr_md_stats* out);
 /* Current positions and velocities (either may be NULL). */

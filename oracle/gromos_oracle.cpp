@@ -1243,6 +1243,14 @@ extern "C" int orc_md_run(orc_ff* ff, double* pos_io, double* vel_io, const doub
         ra = std::sqrt(mp->dist_oh * mp->dist_oh - rc * rc) / (1.0 + half_mo_div_mh);
         rb = half_mo_div_mh * ra;
     }
+    auto kinetic = [&]() {
+        double ke = 0.0;
+        for (int i = 0; i < n; ++i) ke += 0.5 * mass[i] * dot(vel[i], vel[i]);
+        return ke;
+    };
+    // degrees of freedom: 3N minus the solvent constraints (md.rs:1158-1172, NDFMIN 0)
+    const double dof = 3.0 * n - (settle ? 3.0 * ((n - nsa) / 3) : 0.0);
+    double ke_in = kinetic();
     for (int step = 0; step < n_steps; ++step) {
         orc_result r{};
         r.forces = f.data();
@@ -1251,20 +1259,26 @@ extern "C" int orc_md_run(orc_ff* ff, double* pos_io, double* vel_io, const doub
             energies[0] = r.e_lj;
             energies[1] = r.e_crf;
         }
+        double lambda = 1.0;
+        if (mp->tau >= 0.0) {  // berendsen_thermostat.rs:74-98
+            const double kB = 0.00831446261815324;
+            double t = dof > 0.0 ? 2.0 * ke_in / (dof * kB) : 0.0;
+            if (t < 1e-10) t = mp->temperature;
+            if (t >= 1e-10)
+                lambda = mp->tau == 0.0 ? std::sqrt(mp->temperature / t)
+                                        : std::sqrt(1.0 + dt / mp->tau * (mp->temperature / t - 1.0));
+        }
         for (int i = 0; i < n; ++i) {
             const V3 F = {f[3 * i], f[3 * i + 1], f[3 * i + 2]};
-            vel[i] = vel[i] + F * (1.0 / mass[i]) * dt;
+            vel[i] = (vel[i] + F * (1.0 / mass[i]) * dt) * lambda;
             old[i] = pos[i];
             pos[i] = pos[i] + vel[i] * dt;
         }
         if (settle)
             for (int i = nsa; i + 3 <= n; i += 3)
                 if (!settle_one(&old[i], &pos[i], &vel[i], m_o, m_h, ra, rb, rc, 1.0 / dt)) ++failures;
+        ke_in = kinetic();
     }
-    if (e_kin) {
-        double ke = 0.0;
-        for (int i = 0; i < n; ++i) ke += 0.5 * mass[i] * dot(vel[i], vel[i]);
-        *e_kin = ke;
-    }
+    if (e_kin) *e_kin = ke_in;
     return failures;
 }

@@ -118,6 +118,8 @@ void orc_perturbed_pair(const double r[3], double a_c6, double a_c12, double b_c
 
 /* MD steps around orc_ff_apply, the sequence of gromos-md/src/bin/md.rs
  * (:1144-1230) without thermostat: leap-frog velocity (leap_frog.rs:37-85),
+ * Berendsen velocity scaling from the kinetic energy entering the step
+ * (berendsen_thermostat.rs:74-98, between the two leap-frog updates),
  * leap-frog position (:116-148), SETTLE of every solvent molecule
  * (crates/gromos-integrators/src/constraints.rs:815-1010).  pos/vel are
  * updated in place; returns the number of molecules SETTLE could not solve.
@@ -127,6 +129,7 @@ typedef struct {
     double dt;
     int32_t settle;
     double dist_oh, dist_hh;
+    double temperature, tau;   /* Berendsen bath (berendsen_thermostat.rs:58-118); tau < 0 = none */
 } orc_md_params;
 int orc_md_run(orc_ff* ff, double* pos, double* vel, const double* mass, const orc_md_params* p,
                int n_steps, double* e_kin, double energies[2]);

@@ -158,7 +158,8 @@ def pairlist(sysm, algorithm=None, nthreads=0):
 
 
 class OrcMdParams(C.Structure):
-    _fields_ = [("dt", C.c_double), ("settle", C.c_int32), ("dist_oh", C.c_double), ("dist_hh", C.c_double)]
+    _fields_ = [("dt", C.c_double), ("settle", C.c_int32), ("dist_oh", C.c_double), ("dist_hh", C.c_double),
+                ("temperature", C.c_double), ("tau", C.c_double)]
 
 
 class OracleForcefield:
@@ -185,12 +186,13 @@ class OracleForcefield:
         return {"forces": f, "e_lj": r.e_lj, "e_crf": r.e_crf, "dhdl": r.dhdl,
                 "virial": np.asarray(list(r.virial)).reshape(3, 3), "egroup_lj": glj, "egroup_crf": gcrf}
 
-    def md_run(self, pos, vel, mass, n_steps, dt=0.002, settle=True, dist_oh=0.1, dist_hh=0.1633):
-        """n_steps MD steps (leap-frog + SETTLE) in FP64; returns (pos, vel, stats)."""
+    def md_run(self, pos, vel, mass, n_steps, dt=0.002, settle=True, dist_oh=0.1, dist_hh=0.1633,
+               temperature=300.0, tau=-1.0):
+        """n_steps MD steps (leap-frog + Berendsen + SETTLE) in FP64; returns (pos, vel, stats)."""
         x = np.ascontiguousarray(pos, dtype=np.float64).copy()
         v = np.ascontiguousarray(vel, dtype=np.float64).copy()
         m = np.ascontiguousarray(mass, dtype=np.float64)
-        mp = OrcMdParams(dt, 1 if settle else 0, dist_oh, dist_hh)
+        mp = OrcMdParams(dt, 1 if settle else 0, dist_oh, dist_hh, temperature, tau)
         ke = C.c_double(0.0)
         e = np.zeros(2)
         fails = lib().orc_md_run(self.h, _p(x, C.c_double), _p(v, C.c_double), _p(m, C.c_double), C.byref(mp),

@@ -119,7 +119,7 @@ def test_md_entry_points_reject_bad_input_without_device():
     from gromos_nb import _lib
     import ctypes as C
     L = _lib.lib()
-    mp = _lib.GrMdParams(0.002, 1, 0.1, 0.1633)
+    mp = _lib.GrMdParams(0.002, 1, 0.1, 0.1633, 300.0, -1.0)
     assert L.gr_md_init(None, None, None, C.byref(mp)) == _lib.GR_ERR_INVALID
     assert L.gr_md_run(None, 1, None) == _lib.GR_ERR_INVALID
 
