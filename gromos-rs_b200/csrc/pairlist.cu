@@ -356,7 +356,7 @@ __device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restric
 }
 
 template <int W, bool POPSORT>
-__global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
+__global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int b = blockIdx.x;
@@ -536,12 +536,19 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                 const float Cx = float(cdx), Cy = float(cdy), Cz = float(cdz);
                 const float cd = sqrtf(Cx * Cx + Cy * Cy + Cz * Cz);
                 if (cd - chr[ch] > reach) continue;
+                // |C - f| <= |C| + chunk radius, and a pair vector adds at most the
+                // cluster radius: when that stays below half a box edge on every
+                // axis, C - f is the minimum image and every pair is inside the box
+                // (warp-uniform; no per-candidate image or box test)
+                const float ext = chr[ch] + rad;
+                const bool edge = P.boundary && !(fabsf(Cx) + ext < limx && fabsf(Cy) + ext < limy &&
+                                                  fabsf(Cz) + ext < limz);
                 const int t = base + lane;
                 const int sp = tbeg + t;
-                unsigned ms = 0, ml = 0;
+                unsigned ms = 0, ml = 0, amb = 0;
                 if (t < tn && sp > first) {
                     float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
-                    if (P.boundary) {  // the sum of two minimum images need not be one
+                    if (edge) {  // the sum of two minimum images need not be one
                         Dx -= P.boxf[0] * rintf(Dx * P.inv_boxf[0]);
                         Dy -= P.boxf[1] * rintf(Dy * P.inv_boxf[1]);
                         Dz -= P.boxf[2] * rintf(Dz * P.inv_boxf[2]);
@@ -550,33 +557,47 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_water_search(const SysDev
                         // branch-free classification of the W pairs; pairs inside a
                         // band around a cutoff or near half a box edge are decided
                         // by the exact FP64 test
-                        unsigned amb = 0;
+                        // pairs {i_k, j} with k < n and i_k before j in sorted order
+                        const int nv = min(n, sp - first);
+                        const unsigned valid = (1u << nv) - 1u;
 #pragma unroll
                         for (int k = 0; k < W; ++k) {
-                            const bool valid = k < n && sp > first + k;
                             const float kx = ex[k] + Dx, ky = ey[k] + Dy, kz = ez[k] + Dz;
                             const float d2 = kx * kx + ky * ky + kz * kz;
-                            const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
-                            const bool sh = d2 < s_lo;
-                            const bool lg = d2 > s_hi && d2 < l_lo;
-                            const bool far = d2 > l_hi;
-                            ms |= unsigned(valid && inbox && sh) << k;
-                            ml |= unsigned(valid && inbox && lg) << k;
-                            amb |= unsigned(valid && !(inbox && (sh || lg || far))) << k;
-                        }
-#pragma unroll
-                        for (int k = 0; k < W; ++k) {
-                            if (!((amb >> k) & 1u)) continue;
-                            double rx, ry, rz;
-                            nearest_image_exact(s, cxs[warp][0][k], cxs[warp][1][k], cxs[warp][2][k], tx[t], ty[t],
-                                                tz[t], rx, ry, rz);
-                            const double e2 = len2_exact(rx, ry, rz);
-                            if (!(e2 > P.c2l)) {
-                                if (e2 > P.c2s)
-                                    ml |= 1u << k;
-                                else
-                                    ms |= 1u << k;
+                            ms |= unsigned(d2 < s_lo) << k;
+                            ml |= unsigned(d2 > s_hi && d2 < l_lo) << k;
+                            amb |= unsigned((d2 >= s_lo && d2 <= s_hi) || (d2 >= l_lo && d2 <= l_hi)) << k;
+                            if (edge) {
+                                const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
+                                amb |= unsigned(!inbox) << k;
                             }
+                        }
+                        ms &= valid & ~amb;
+                        ml &= valid & ~amb;
+                        amb &= valid;
+                    }
+                }
+                // the rare ambiguous pairs: one warp-uniform test, then the exact
+                // FP64 decision (nearest_image_exact + len2_exact, box from the
+                // kernel parameters) for the lanes that have some
+                if (__any_sync(0xffffffffu, amb != 0u) && amb) {
+#pragma unroll 1
+                    for (int k = 0; k < W; ++k) {
+                        if (!((amb >> k) & 1u)) continue;
+                        double rx = __dsub_rn(cxs[warp][0][k], tx[t]);
+                        double ry = __dsub_rn(cxs[warp][1][k], ty[t]);
+                        double rz = __dsub_rn(cxs[warp][2][k], tz[t]);
+                        if (P.boundary) {
+                            rx = image_exact(rx, P.box[0], P.inv_box[0]);
+                            ry = image_exact(ry, P.box[1], P.inv_box[1]);
+                            rz = image_exact(rz, P.box[2], P.inv_box[2]);
+                        }
+                        const double e2 = len2_exact(rx, ry, rz);
+                        if (!(e2 > P.c2l)) {
+                            if (e2 > P.c2s)
+                                ml |= 1u << k;
+                            else
+                                ms |= 1u << k;
                         }
                     }
                 }
