@@ -390,7 +390,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&h.f_out, size_t(N) * 3))) return st;
     if ((st = alloc(&h.e_out, size_t(acc_size(G))))) return st;
     if ((st = alloc(&h.err, 4))) return st;
-    if ((st = alloc(&h.n_deferred, 4))) return st;  // deferred counts [2] + water work counters [2]
+    if ((st = alloc(&h.n_deferred, 6))) return st;  // deferred counts [2], water work counters [2], blocks done [2]
     if ((st = alloc(&h.max_delta, 1))) return st;
     GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
     GR_CUDA(cudaMemset(h.f_long, 0, size_t(N) * 3 * sizeof(long long)));
@@ -793,7 +793,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         if (NCG > NSCG) {
             wp = water_params();
             (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
-            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 4 * sizeof(int), s));
+            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 6 * sizeof(int), s));
             if ((st = launch_water(s, wp, false))) return st;
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
@@ -1035,12 +1035,14 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
     }
 #undef GR_WATER_IT
 #undef GR_WATER_SHARED
-    if (lj00) {
-        if (lr) (++launches, k_water_deferred<true, true><<<sm, 128, 0, s>>>(d_sys, wp));
-        else (++launches, k_water_deferred<true, false><<<sm, 128, 0, s>>>(d_sys, wp));
-    } else {
-        if (lr) (++launches, k_water_deferred<false, true><<<sm, 128, 0, s>>>(d_sys, wp));
-        else (++launches, k_water_deferred<false, false><<<sm, 128, 0, s>>>(d_sys, wp));
+    if (layout == 1) {  // the bit-iterating kernel handles its deferred pairs itself
+        if (lj00) {
+            if (lr) (++launches, k_water_deferred<true, true><<<sm, 128, 0, s>>>(d_sys, wp));
+            else (++launches, k_water_deferred<true, false><<<sm, 128, 0, s>>>(d_sys, wp));
+        } else {
+            if (lr) (++launches, k_water_deferred<false, true><<<sm, 128, 0, s>>>(d_sys, wp));
+            else (++launches, k_water_deferred<false, false><<<sm, 128, 0, s>>>(d_sys, wp));
+        }
     }
     GR_CUDA(cudaGetLastError());
     return GR_OK;

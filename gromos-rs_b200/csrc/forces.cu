@@ -42,7 +42,7 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     if (slot < s.n_clusters[0] * s.W) {
         const int cg = s.slot_cg[slot];
         if (cg >= 0) {
-            const int a0 = s.cg_off[cg];
+            const int a0 = s.n_solute_atoms + 3 * (cg - s.n_solute_cg);  // solvent CGs are whole 3-site molecules
             const double x0 = s.pos[3 * a0], y0 = s.pos[3 * a0 + 1], z0 = s.pos[3 * a0 + 2];
             WaterRec w;
             w.x0 = x0;
@@ -684,18 +684,20 @@ __global__ void k_pert_terms(const SysDev* __restrict__ sys) {
 
 // Fixed point -> FP64 results.  plain != 0 adds the FP32 baseline buffers.
 __global__ void k_finalize(const SysDev* __restrict__ sys, int plain) {
+    // One thread per force component; a water atom's component also gathers
+    // its cluster slot's sum (solvent CG w = atoms nsa + 3w .. nsa + 3w + 2).
     const SysDev& s = sys[blockIdx.y];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double inv = 1.0 / kForceScale;
     if (i < 3 * s.n_atoms) {
         long long fx = s.f_short[i];
         if (s.twin) fx += s.f_long[i];
+        const int nsa = s.n_solute_atoms;
         const int a = i / 3;
-        if (a >= s.n_solute_atoms && s.wrec != nullptr && !plain) {
-            // water atoms: forces accumulated per cluster slot
-            const int cg = s.atom_cg[a];
-            const int slot = s.cg_slot[cg];
-            const int k = (a - s.cg_off[cg]) * 3 + (i - 3 * a);
+        if (a >= nsa && s.wrec != nullptr && !plain) {
+            const int w = (a - nsa) / 3;
+            const int slot = s.cg_slot[s.n_solute_cg + w];
+            const int k = i - 3 * (nsa + 3 * w);
             fx += s.fs_short[slot * 9 + k];
             if (s.twin) fx += s.fs_long[slot * 9 + k];
         }

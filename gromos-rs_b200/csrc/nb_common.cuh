@@ -131,7 +131,7 @@ struct SysDev {
     long long* fs_short;       // [max_clusters*W*9] water forces per slot (fixed 2^32)
     long long* fs_long;        // same, long-range cache
     int* deferred;             // [2 * 2 * defer_cap] (i slot, j slot): short, then long
-    int* n_deferred;           // [4]: deferred pairs (short, long), water-kernel work counters (short, long)
+    int* n_deferred;           // [6]: deferred pairs, water-kernel work counters, finished blocks (short, long each)
     float* max_delta;          // [1] largest |offset| component of a water atom from its first atom (this step)
     int defer_cap;
     // ---- plain-kernel data

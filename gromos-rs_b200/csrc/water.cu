@@ -397,6 +397,41 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
     }
 }
 
+// CG pairs the main kernels deferred: exact FP64 images (first-atom shift for
+// the short list, per-atom images for the long list), FP32 pair arithmetic.
+// Threads tid, tid + nthreads, ... of the caller take one pair each.  The
+// list and its count were written by other blocks: read through L2.
+template <bool LJ00, bool LONG>
+__device__ __forceinline__ void process_deferred(const SysDev& s, const WaterParams& wp, int tid, int nthreads) {
+    long long* __restrict__ FS = LONG ? s.fs_long : s.fs_short;
+    const int nd = min(__ldcg(s.n_deferred + (LONG ? 1 : 0)), s.defer_cap);
+    long long acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int d = tid; d < nd; d += nthreads) {
+        const int e = LONG ? s.defer_cap + d : d;
+        const int islot = __ldcg(s.deferred + 2 * e), jslot = __ldcg(s.deferred + 2 * e + 1);
+        const PairAcc o = water_slow_pair<LJ00, LONG>(s, wp, islot, jslot);
+        for (int c = 0; c < 9; ++c) {
+            red_add(FS + static_cast<size_t>(islot) * 9 + c, to_fixed_f(o.fi[c], 4294967296.0f));
+            red_add(FS + static_cast<size_t>(jslot) * 9 + c, to_fixed_f(o.fj[c], 4294967296.0f));
+        }
+        acc[0] += to_fixed_f(o.elj, 16777216.0f);
+        acc[1] += to_fixed_f(o.ecrf, 16777216.0f);
+        for (int v = 0; v < 6; ++v) acc[2 + v] += to_fixed_f(o.v[v], 16777216.0f);
+    }
+    long long* dst = LONG ? s.acc_long : s.acc_short;
+    const int G = wp.G, vb = 2 * G * G;
+    const int idx0[8] = {wp.slot, G * G + wp.slot, vb + 0, vb + 1, vb + 2, vb + 4, vb + 5, vb + 8};
+    const int idx1[8] = {-1, -1, -1, vb + 3, vb + 6, -1, vb + 7, -1};
+    for (int v = 0; v < 8; ++v) {
+        const long long t = warp_sum_ll(acc[v]);
+        if ((threadIdx.x & 31) == 0 && t) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx0[v]), static_cast<unsigned long long>(t));
+            if (idx1[v] >= 0)
+                atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx1[v]), static_cast<unsigned long long>(t));
+        }
+    }
+}
+
 // Bit-iterating layout: one warp per i-cluster of W waters, one lane per
 // j-water entry; each lane loops over the set bits of its own mask only, so
 // no lane idles on another lane's bits (entries are sorted by popcount, so
@@ -691,6 +726,14 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
         atomicAdd(reinterpret_cast<unsigned long long*>(dst + i0), sh[v]);
         if (i1 >= 0) atomicAdd(reinterpret_cast<unsigned long long*>(dst + i1), sh[v]);
     }
+    // The last block to finish evaluates the pairs every block deferred (no
+    // separate launch): its deferred-list reads follow every block's fence.
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(s.n_deferred + (LONG ? 5 : 4), 1) == int(gridDim.x) - 1;
+    __syncthreads();
+    if (last) process_deferred<LJ00, LONG>(s, wp, threadIdx.x, blockDim.x);
 }
 
 template <int W>
@@ -700,36 +743,11 @@ constexpr size_t water_it_smem() {
 
 // CG pairs the main kernel deferred: exact FP64 images (first-atom shift for
 // the short list, per-atom images for the long list), FP32 pair arithmetic.
+// The deferred pairs of the shared-bit kernel (the bit-iterating kernel
+// evaluates its own in its last block).
 template <bool LJ00, bool LONG>
 __global__ void __launch_bounds__(128) k_water_deferred(const SysDev* __restrict__ sys, const WaterParams wp) {
-    const SysDev& s = sys[blockIdx.y];
-    long long* __restrict__ FS = LONG ? s.fs_long : s.fs_short;
-    const int nd = min(s.n_deferred[LONG ? 1 : 0], s.defer_cap);
-    long long acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nd; d += gridDim.x * blockDim.x) {
-        const int e = LONG ? s.defer_cap + d : d;
-        const int islot = s.deferred[2 * e], jslot = s.deferred[2 * e + 1];
-        const PairAcc o = water_slow_pair<LJ00, LONG>(s, wp, islot, jslot);
-        for (int c = 0; c < 9; ++c) {
-            red_add(FS + static_cast<size_t>(islot) * 9 + c, to_fixed_f(o.fi[c], 4294967296.0f));
-            red_add(FS + static_cast<size_t>(jslot) * 9 + c, to_fixed_f(o.fj[c], 4294967296.0f));
-        }
-        acc[0] += to_fixed_f(o.elj, 16777216.0f);
-        acc[1] += to_fixed_f(o.ecrf, 16777216.0f);
-        for (int v = 0; v < 6; ++v) acc[2 + v] += to_fixed_f(o.v[v], 16777216.0f);
-    }
-    long long* dst = LONG ? s.acc_long : s.acc_short;
-    const int G = wp.G, vb = 2 * G * G;
-    const int idx0[8] = {wp.slot, G * G + wp.slot, vb + 0, vb + 1, vb + 2, vb + 4, vb + 5, vb + 8};
-    const int idx1[8] = {-1, -1, -1, vb + 3, vb + 6, -1, vb + 7, -1};
-    for (int v = 0; v < 8; ++v) {
-        const long long t = warp_sum_ll(acc[v]);
-        if ((threadIdx.x & 31) == 0 && t) {
-            atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx0[v]), static_cast<unsigned long long>(t));
-            if (idx1[v] >= 0)
-                atomicAdd(reinterpret_cast<unsigned long long*>(dst + idx1[v]), static_cast<unsigned long long>(t));
-        }
-    }
+    process_deferred<LJ00, LONG>(sys[blockIdx.y], wp, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 template __global__ void k_water_deferred<true, false>(const SysDev*, const WaterParams);
