@@ -205,6 +205,7 @@ def run_gpu(args, rank, world, local_rank):
 
     from gromos_nb import generators
     from gromos_nb.nonbonded import Forcefield, ffma_peak
+    from gromos_nb.replicas import aggregate
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -251,16 +252,7 @@ def run_gpu(args, rank, world, local_rank):
         dist.barrier()
     launches = ff.launches() - launches0
     clk = clocks.stop()
-    total_ms = float(sum(step_ms))
-    if dist is not None:
-        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-        pp = torch.tensor([float(pairs)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(pp, op=dist.ReduceOp.SUM)
-        pairs_all = float(pp.item())
-    else:
-        pairs_all = float(pairs)
+    total_ms, pairs_all = aggregate(float(sum(step_ms)), float(pairs), device="cuda")
     value = pairs_all / (total_ms * 1e-3)
     ms_per_step = total_ms / args.steps
     # end to end through the public API: host positions in, host forces out
@@ -377,10 +369,17 @@ def _one_by_one(systems, seeds, temps, steps, kernel):
     return total_ms
 
 
-def run_batched(args, kind):
-    """REMD replicas (uneven sizes) or FEP lambda windows in one batch."""
+def run_batched(args, kind, rank=0, world=1, local_rank=0):
+    """REMD replicas (uneven sizes) or FEP lambda windows in one batch.  Under
+    torchrun the members are spread over the ranks by size (whole systems, no
+    collective on the force path); rank 0 prints the aggregate."""
+    import torch
+
     from gromos_nb import generators
     from gromos_nb.nonbonded import Batch
+    from gromos_nb.replicas import aggregate, shard_by_work
+
+    torch.cuda.set_device(local_rank)
 
     rng = np.random.default_rng(1003 if kind == "remd" else 1004)
     systems, seeds, temps, lams = [], [], [], []
@@ -396,6 +395,13 @@ def run_batched(args, kind):
         seeds = [6000] * len(lams)                  # same start in every window
         temps = [300.0] * len(lams)
         workload = "fep_21_windows_spc5000_solute30_rc1.4"
+    n_members = len(specs)
+    if world > 1:
+        mine = shard_by_work([sp[0] + sp[1] for sp in specs], world)[rank]
+        specs = [specs[i] for i in mine]
+        seeds = [seeds[i] for i in mine]
+        temps = [temps[i] for i in mine]
+        lams = [lams[i] for i in mine] if lams else lams
     systems = _generate(specs)
     ffs = [_member(s, seed, T) for s, seed, T in zip(systems, seeds, temps)]
     pairs = [_pairs_per_step(ff, s) for ff, s in zip(ffs, systems)]
@@ -407,8 +413,8 @@ def run_batched(args, kind):
     launches0 = b.launches()
     ms = b.md_run(args.batch_steps)
     launches = b.launches() - launches0
-    per_step = ms / args.batch_steps
-    value = sum(pairs) / (per_step * 1e-3)
+    per_step, pairs_all = aggregate(ms / args.batch_steps, sum(pairs), device="cuda")
+    value = pairs_all / (per_step * 1e-3)
     stats = [ff.md_stats() for ff in ffs]
     out_fep = None
     if kind == "fep":
@@ -427,14 +433,17 @@ def run_batched(args, kind):
     steps_alone = min(args.batch_steps, 20)
     ms_fixed = _one_by_one(sub, [seeds[i] for i in idx], [temps[i] for i in idx], steps_alone, "fixed")
     ms_plain = _one_by_one(sub, [seeds[i] for i in idx], [temps[i] for i in idx], steps_alone, "plain")
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.batch_steps,
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.batch_steps,
             "warmup": 5, "ms_per_step": per_step,
-            "ns_per_day": ns_per_day(per_step), "ns_per_day_aggregate": ns_per_day(per_step) * len(systems),
+            "ns_per_day": ns_per_day(per_step), "ns_per_day_aggregate": ns_per_day(per_step) * n_members,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i64",
             "data": "synthetic (seeded water boxes + seeded solutes)",
-            "config": {"workload": workload, "members": len(systems),
-                       "atoms_total": int(sum(s.topo.n_atoms for s in systems)),
-                       "pairs_per_batch_step": float(sum(pairs)),
+            "config": {"workload": workload, "members": n_members, "members_rank0": len(systems),
+                       "atoms_rank0": int(sum(s.topo.n_atoms for s in systems)),
+                       "pairs_per_batch_step": pairs_all,
+                       "parallelism": f"members sharded over {world} GPUs" if world > 1 else "one GPU",
                        "step": "MD step (forces + leap-frog + Berendsen bath at the replica temperature + SETTLE)",
                        "launch": "one CUDA graph launch per batch step", "autotune": tune},
             "gpu_launches": launches,
@@ -503,7 +512,18 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload in ("remd", "fep"):
-        return run_batched(args, args.workload) if rank == 0 else 0
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            try:
+                return run_batched(args, args.workload, rank, world, local_rank)
+            finally:
+                dist.destroy_process_group()
+        return run_batched(args, args.workload)
     if args.workload == "serving":
         return run_serving(args) if rank == 0 else 0
     if world > 1:
