@@ -263,9 +263,11 @@ __device__ __forceinline__ int axis_offsets(int g, int* off) {
 }
 
 // Water-water search, tiled by cell.  One block per group of up to
-// kSearchWarps clusters of one cell, one warp per cluster; the solvent CGs of
-// each neighbour cell are staged in shared memory in tiles of kTile and every
-// warp tests its cluster against the tile.  Pair {i_k, j} belongs to this
+// kSearchWarps clusters of one cell; the solvent CGs of each neighbour cell are
+// staged in shared memory in tiles of kTile, the (cluster, chunk of 32) pairs
+// of a tile that pass the bounding-sphere test are shared out over the
+// block's warps, and each cluster's warp then appends its results in chunk
+// order.  Pair {i_k, j} belongs to this
 // cluster iff j's sorted position is after i_k's, so every unordered CG pair
 // is listed once.  Bit k of the short (long) mask is set when the reference
 // test puts (i_k, j) in the short (long) range; the solvent reference point
@@ -292,7 +294,7 @@ struct SearchParams {
     int boundary;
     int wcap;
 };
-constexpr int kEntBuf = 512;
+constexpr int kEntBuf = 480;
 
 __device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ buf, int nbuf,
                                                    uint32_t* __restrict__ out, int lane) {
@@ -372,21 +374,37 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const Sys
     const int cell = lo;
     const int ci = s.cell_nclus[cell] + (b - s.cell_part[cell]) * kSearchWarps + warp;
     const bool active = ci < s.cell_nclus[cell + 1];
+    constexpr int kChunks = kTile / 32;
 
     __shared__ double tx[kTile], ty[kTile], tz[kTile];
     __shared__ float fx[kTile], fy[kTile], fz[kTile];       // offsets from the chunk centre (min image)
-    __shared__ double chx[kTile / 32], chy[kTile / 32], chz[kTile / 32];  // chunk centres
-    __shared__ float chr[kTile / 32];                        // chunk radii
+    __shared__ double chx[kChunks], chy[kChunks], chz[kChunks];  // chunk centres
+    __shared__ float chr[kChunks];                          // chunk radii
     __shared__ uint32_t ebuf_s[kSearchWarps][kEntBuf], ebuf_l[kSearchWarps][kEntBuf];
-
-    // the cluster's first atoms: FP64 in shared memory (exact tests), FP32
-    // offsets from the first one in registers
+    // the block's clusters (one per warp, all in this cell): FP64 first atoms
+    // (exact tests), FP32 offsets from the first one, sizes, reach, counters
     __shared__ double cxs[kSearchWarps][3][8];
-    int n = 0, first = 0;
-    float ex[W], ey[W], ez[W];
-    if (active) {
-        n = s.clus_n[ci];
-        first = s.clus_first[ci];
+    __shared__ float cex[kSearchWarps][3][8];
+    __shared__ int c_n[kSearchWarps], c_first[kSearchWarps];
+    __shared__ float c_reach[kSearchWarps], c_rad[kSearchWarps];
+    // (cluster, chunk) pairs of the current tile that survive the bounding
+    // sphere test: the block's warps share them out, so a warp whose cluster
+    // sees few chunks does not wait at the tile barrier for one that sees
+    // many.  Their masks land at fixed places (res_*[cluster chunk][lane]) and
+    // each cluster's warp appends them in chunk order afterwards, so the
+    // lists come out in the same order on every run.
+    __shared__ int n_items;
+    __shared__ int it_cc[kSearchWarps * kChunks];
+    __shared__ float it_C[kSearchWarps * kChunks][3];
+    __shared__ uint8_t res_s[kSearchWarps * kChunks][32], res_l[kSearchWarps * kChunks][32];
+    __shared__ unsigned c_surv[kSearchWarps];  // bit ch: chunk ch survived for this cluster
+
+    {
+        int n = 0, first = 0;
+        if (active) {
+            n = s.clus_n[ci];
+            first = s.clus_first[ci];
+        }
         if (lane < W) {
             double x = 0, y = 0, z = 0;
             if (lane < n) {
@@ -399,19 +417,28 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const Sys
             cxs[warp][1][lane] = y;
             cxs[warp][2][lane] = z;
         }
+        __syncwarp();
+        if (lane < W) {
+            const bool v = lane < n;
+            const float ox = v ? float(cxs[warp][0][lane] - cxs[warp][0][0]) : 0.f;
+            const float oy = v ? float(cxs[warp][1][lane] - cxs[warp][1][0]) : 0.f;
+            const float oz = v ? float(cxs[warp][2][lane] - cxs[warp][2][0]) : 0.f;
+            cex[warp][0][lane] = ox;
+            cex[warp][1][lane] = oy;
+            cex[warp][2][lane] = oz;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            float rad = 0.f;
+            for (int k = 0; k < n; ++k)
+                rad = fmaxf(rad, sqrtf(cex[warp][0][k] * cex[warp][0][k] + cex[warp][1][k] * cex[warp][1][k] +
+                                       cex[warp][2][k] * cex[warp][2][k]));
+            c_n[warp] = n;
+            c_first[warp] = first;
+            c_rad[warp] = rad;
+            c_reach[warp] = sqrtf(float(P.c2l)) + rad + 1e-3f;
+        }
     }
-    __syncwarp();
-    const double x0 = cxs[warp][0][0], y0 = cxs[warp][1][0], z0 = cxs[warp][2][0];
-    float rad = 0.f;
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-        ex[k] = k < n ? float(cxs[warp][0][k] - x0) : 0.f;
-        ey[k] = k < n ? float(cxs[warp][1][k] - y0) : 0.f;
-        ez[k] = k < n ? float(cxs[warp][2][k] - z0) : 0.f;
-        if (k < n) rad = fmaxf(rad, sqrtf(ex[k] * ex[k] + ey[k] * ey[k] + ez[k] * ez[k]));
-    }
-    const float reach = sqrtf(float(P.c2l)) + rad + 1e-3f;
-    const float reach2 = reach * reach;
     const float c2s = float(P.c2s), c2l = float(P.c2l);
     const float s_lo = c2s * (1.f - 1e-5f), s_hi = c2s * (1.f + 1e-5f);
     const float l_lo = c2l * (1.f - 1e-5f), l_hi = c2l * (1.f + 1e-5f);
@@ -422,10 +449,10 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const Sys
     const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
     int ox[3], oy[3], oz[3];
     const int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
+    const unsigned below = (1u << lane) - 1u;
     uint32_t* outs = s.wl_s + static_cast<size_t>(active ? ci : 0) * P.wcap;
     uint32_t* outl = s.wl_l + static_cast<size_t>(active ? ci : 0) * P.wcap;
     int cnt_s = 0, cnt_l = 0;
-    const unsigned below = (1u << lane) - 1u;
     // neighbour cells at or after this one (block-uniform), then the tiles of
     // their solvent CGs; the next tile is prefetched into registers while the
     // current one is processed
@@ -466,8 +493,11 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const Sys
         const int nc = ncell[ic];
         const int tbeg = j0 + t0;
         const int tn = min(kTile, j1 - tbeg);
+        const int nch = (tn + 31) >> 5;
         const int slot0 = s.cell_nclus[nc] * W;
         __syncthreads();
+        if (threadIdx.x == 0) n_items = 0;
+        if (threadIdx.x < kSearchWarps) c_surv[threadIdx.x] = 0u;
         if (threadIdx.x < tn) {
             tx[threadIdx.x] = px;
             ty[threadIdx.x] = py;
@@ -522,86 +552,113 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const Sys
             py = s.sref[stride + q];
             pz = s.sref[2 * stride + q];
         }
-        if (active) {
-            for (int base = 0; base < tn; base += 32) {
-                // cluster-to-chunk vector (FP64 image once per chunk); skip
-                // chunks entirely out of reach (warp-uniform)
-                const int ch = base >> 5;
-                double cdx = x0 - chx[ch], cdy = y0 - chy[ch], cdz = z0 - chz[ch];
-                if (P.boundary) {
-                    cdx -= P.box[0] * rint(cdx * P.inv_box[0]);
-                    cdy -= P.box[1] * rint(cdy * P.inv_box[1]);
-                    cdz -= P.box[2] * rint(cdz * P.inv_box[2]);
+        // bounding-sphere test of every (cluster, chunk) pair: cluster-to-chunk
+        // vector with the FP64 image, rounded once; survivors are queued with
+        // their vector and a flag for chunks near half a box edge
+        for (int q = threadIdx.x; q < kSearchWarps * nch; q += blockDim.x) {
+            const int c = q / nch, ch = q - c * nch;
+            if (c_n[c] == 0) continue;
+            double cdx = cxs[c][0][0] - chx[ch], cdy = cxs[c][1][0] - chy[ch], cdz = cxs[c][2][0] - chz[ch];
+            if (P.boundary) {
+                cdx -= P.box[0] * rint(cdx * P.inv_box[0]);
+                cdy -= P.box[1] * rint(cdy * P.inv_box[1]);
+                cdz -= P.box[2] * rint(cdz * P.inv_box[2]);
+            }
+            const float Cx = float(cdx), Cy = float(cdy), Cz = float(cdz);
+            const float cd = sqrtf(Cx * Cx + Cy * Cy + Cz * Cz);
+            if (cd - chr[ch] > c_reach[c]) continue;
+            // |C - f| <= |C| + chunk radius, and a pair vector adds at most the
+            // cluster radius: when that stays below half a box edge on every
+            // axis, C - f is the minimum image and every pair is inside the box
+            const float ext = chr[ch] + c_rad[c];
+            const bool edge = P.boundary && !(fabsf(Cx) + ext < limx && fabsf(Cy) + ext < limy &&
+                                              fabsf(Cz) + ext < limz);
+            const int k = atomicAdd(&n_items, 1);
+            atomicOr(&c_surv[c], 1u << ch);
+            it_cc[k] = (c << 8) | (ch << 1) | (edge ? 1 : 0);
+            it_C[k][0] = Cx;
+            it_C[k][1] = Cy;
+            it_C[k][2] = Cz;
+        }
+        __syncthreads();
+        const int items = n_items;
+        for (int it = warp; it < items; it += kSearchWarps) {
+            const int cc = it_cc[it];
+            const int c = cc >> 8, ch = (cc >> 1) & 0x7f;
+            const bool edge = cc & 1;
+            const float Cx = it_C[it][0], Cy = it_C[it][1], Cz = it_C[it][2];
+            const int n = c_n[c], first = c_first[c];
+            const float reach2 = c_reach[c] * c_reach[c];
+            const int t = ch * 32 + lane;
+            const int sp = tbeg + t;
+            unsigned ms = 0, ml = 0, amb = 0;
+            if (t < tn && sp > first) {
+                float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
+                if (edge) {  // the sum of two minimum images need not be one
+                    Dx -= P.boxf[0] * rintf(Dx * P.inv_boxf[0]);
+                    Dy -= P.boxf[1] * rintf(Dy * P.inv_boxf[1]);
+                    Dz -= P.boxf[2] * rintf(Dz * P.inv_boxf[2]);
                 }
-                const float Cx = float(cdx), Cy = float(cdy), Cz = float(cdz);
-                const float cd = sqrtf(Cx * Cx + Cy * Cy + Cz * Cz);
-                if (cd - chr[ch] > reach) continue;
-                // |C - f| <= |C| + chunk radius, and a pair vector adds at most the
-                // cluster radius: when that stays below half a box edge on every
-                // axis, C - f is the minimum image and every pair is inside the box
-                // (warp-uniform; no per-candidate image or box test)
-                const float ext = chr[ch] + rad;
-                const bool edge = P.boundary && !(fabsf(Cx) + ext < limx && fabsf(Cy) + ext < limy &&
-                                                  fabsf(Cz) + ext < limz);
-                const int t = base + lane;
-                const int sp = tbeg + t;
-                unsigned ms = 0, ml = 0, amb = 0;
-                if (t < tn && sp > first) {
-                    float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
-                    if (edge) {  // the sum of two minimum images need not be one
-                        Dx -= P.boxf[0] * rintf(Dx * P.inv_boxf[0]);
-                        Dy -= P.boxf[1] * rintf(Dy * P.inv_boxf[1]);
-                        Dz -= P.boxf[2] * rintf(Dz * P.inv_boxf[2]);
-                    }
-                    if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
-                        // branch-free classification of the W pairs; pairs inside a
-                        // band around a cutoff or near half a box edge are decided
-                        // by the exact FP64 test
-                        // pairs {i_k, j} with k < n and i_k before j in sorted order
-                        const int nv = min(n, sp - first);
-                        const unsigned valid = (1u << nv) - 1u;
+                if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
+                    // branch-free classification of the W pairs; pairs inside a
+                    // band around a cutoff or near half a box edge are decided by
+                    // the exact FP64 test; pairs {i_k, j} with k < n and i_k
+                    // before j in sorted order
+                    const int nv = min(n, sp - first);
+                    const unsigned valid = (1u << nv) - 1u;
 #pragma unroll
-                        for (int k = 0; k < W; ++k) {
-                            const float kx = ex[k] + Dx, ky = ey[k] + Dy, kz = ez[k] + Dz;
-                            const float d2 = kx * kx + ky * ky + kz * kz;
-                            ms |= unsigned(d2 < s_lo) << k;
-                            ml |= unsigned(d2 > s_hi && d2 < l_lo) << k;
-                            amb |= unsigned((d2 >= s_lo && d2 <= s_hi) || (d2 >= l_lo && d2 <= l_hi)) << k;
-                            if (edge) {
-                                const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
-                                amb |= unsigned(!inbox) << k;
-                            }
-                        }
-                        ms &= valid & ~amb;
-                        ml &= valid & ~amb;
-                        amb &= valid;
-                    }
-                }
-                // the rare ambiguous pairs: one warp-uniform test, then the exact
-                // FP64 decision (nearest_image_exact + len2_exact, box from the
-                // kernel parameters) for the lanes that have some
-                if (__any_sync(0xffffffffu, amb != 0u) && amb) {
-#pragma unroll 1
                     for (int k = 0; k < W; ++k) {
-                        if (!((amb >> k) & 1u)) continue;
-                        double rx = __dsub_rn(cxs[warp][0][k], tx[t]);
-                        double ry = __dsub_rn(cxs[warp][1][k], ty[t]);
-                        double rz = __dsub_rn(cxs[warp][2][k], tz[t]);
-                        if (P.boundary) {
-                            rx = image_exact(rx, P.box[0], P.inv_box[0]);
-                            ry = image_exact(ry, P.box[1], P.inv_box[1]);
-                            rz = image_exact(rz, P.box[2], P.inv_box[2]);
-                        }
-                        const double e2 = len2_exact(rx, ry, rz);
-                        if (!(e2 > P.c2l)) {
-                            if (e2 > P.c2s)
-                                ml |= 1u << k;
-                            else
-                                ms |= 1u << k;
+                        const float kx = cex[c][0][k] + Dx, ky = cex[c][1][k] + Dy, kz = cex[c][2][k] + Dz;
+                        const float d2 = kx * kx + ky * ky + kz * kz;
+                        ms |= unsigned(d2 < s_lo) << k;
+                        ml |= unsigned(d2 > s_hi && d2 < l_lo) << k;
+                        amb |= unsigned((d2 >= s_lo && d2 <= s_hi) || (d2 >= l_lo && d2 <= l_hi)) << k;
+                        if (edge) {
+                            const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
+                            amb |= unsigned(!inbox) << k;
                         }
                     }
+                    ms &= valid & ~amb;
+                    ml &= valid & ~amb;
+                    amb &= valid;
                 }
-                const uint32_t slot = static_cast<uint32_t>(slot0 + (sp - j0));
+            }
+            // the rare ambiguous pairs: one warp-uniform test, then the exact
+            // FP64 decision (nearest_image_exact + len2_exact, box from the
+            // kernel parameters) for the lanes that have some
+            if (__any_sync(0xffffffffu, amb != 0u) && amb) {
+#pragma unroll 1
+                for (int k = 0; k < W; ++k) {
+                    if (!((amb >> k) & 1u)) continue;
+                    double rx = __dsub_rn(cxs[c][0][k], tx[t]);
+                    double ry = __dsub_rn(cxs[c][1][k], ty[t]);
+                    double rz = __dsub_rn(cxs[c][2][k], tz[t]);
+                    if (P.boundary) {
+                        rx = image_exact(rx, P.box[0], P.inv_box[0]);
+                        ry = image_exact(ry, P.box[1], P.inv_box[1]);
+                        rz = image_exact(rz, P.box[2], P.inv_box[2]);
+                    }
+                    const double e2 = len2_exact(rx, ry, rz);
+                    if (!(e2 > P.c2l)) {
+                        if (e2 > P.c2s)
+                            ml |= 1u << k;
+                        else
+                            ms |= 1u << k;
+                    }
+                }
+            }
+            res_s[c * kChunks + ch][lane] = static_cast<uint8_t>(ms);
+            res_l[c * kChunks + ch][lane] = static_cast<uint8_t>(ml);
+        }
+        __syncthreads();
+        // each cluster's warp appends its surviving chunks in chunk order
+        if (active) {
+            unsigned surv = c_surv[warp];
+            while (surv) {
+                const int ch = __ffs(surv) - 1;
+                surv &= surv - 1;
+                const unsigned ms = res_s[warp * kChunks + ch][lane], ml = res_l[warp * kChunks + ch][lane];
+                const uint32_t slot = static_cast<uint32_t>(slot0 + (tbeg + ch * 32 + lane - j0));
                 const unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
                 const unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
                 if (ms) {
