@@ -142,6 +142,7 @@ gr_status NbSystem::alloc(T** p, size_t n) {
     allocs.push_back(*p);
     bytes += n * sizeof(T);
     ++alloc_gen;
+    acc_clean = false;
     return GR_OK;
 }
 
@@ -774,12 +775,20 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     steps_since_update += 1;
     if (record_events) GR_CUDA(record_event(ev[1], s));
     const int NA = acc_size(G);
-    GR_CUDA(cudaMemsetAsync(h.f_short, 0, size_t(N) * 3 * sizeof(long long), s));
-    GR_CUDA(cudaMemsetAsync(h.acc_short, 0, size_t(NA) * sizeof(long long), s));
-    if (NCG > NSCG) {
-        GR_CUDA(cudaMemsetAsync(h.fs_short, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
-        GR_CUDA(cudaMemsetAsync(h.max_delta, 0, sizeof(float), s));
+    // The per-atom short-range accumulators (and the per-step counters) are
+    // zeroed by the previous evaluation's k_finalize as it reads them; only
+    // after a (re)allocation or an interrupted evaluation are they cleared here.
+    const bool clean = acc_clean;
+    acc_clean = false;  // until this evaluation's finalize is enqueued
+    if (!clean) {
+        GR_CUDA(cudaMemsetAsync(h.f_short, 0, size_t(N) * 3 * sizeof(long long), s));
+        GR_CUDA(cudaMemsetAsync(h.acc_short, 0, size_t(NA) * sizeof(long long), s));
+        if (NCG > NSCG) {
+            GR_CUDA(cudaMemsetAsync(h.max_delta, 0, sizeof(float), s));
+            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 6 * sizeof(int), s));
+        }
     }
+    if (NCG > NSCG) GR_CUDA(cudaMemsetAsync(h.fs_short, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
     if (NCG > NSCG && !fs_long_zeroed) {
         // the slot layout changes at rebuilds; keep the long cache consistent
         GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
@@ -793,7 +802,6 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         if (NCG > NSCG) {
             wp = water_params();
             (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
-            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 6 * sizeof(int), s));
             if ((st = launch_water(s, wp, false))) return st;
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
@@ -835,6 +843,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         (++launches, k_pert_terms<<<blocks_for(std::max(N, h.n_pp), 128), 128, sha, s>>>(d_sys));
     }
     (++launches, k_finalize<<<blocks_for(std::max<long long>(3LL * N, NA), 256), 256, 0, s>>>(d_sys, prm.kernel == GR_KERNEL_PLAIN));
+    acc_clean = true;  // k_finalize leaves the short-range accumulators zero
     if (prm.kernel == GR_KERNEL_PLAIN) (++launches, k_finalize_plain_energies<<<1, 32, 0, s>>>(d_sys));
     if (record_events) GR_CUDA(record_event(ev[4], s));
     GR_CUDA(cudaGetLastError());

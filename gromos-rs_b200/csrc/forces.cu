@@ -689,8 +689,12 @@ __global__ void k_finalize(const SysDev* __restrict__ sys, int plain) {
     const SysDev& s = sys[blockIdx.y];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const double inv = 1.0 / kForceScale;
+    // Every per-atom short-range accumulator is read by exactly one thread
+    // here, which also clears it for the next evaluation (the per-slot water
+    // sums are cleared by one contiguous memset; the long-range cache persists).
     if (i < 3 * s.n_atoms) {
         long long fx = s.f_short[i];
+        s.f_short[i] = 0;
         if (s.twin) fx += s.f_long[i];
         const int nsa = s.n_solute_atoms;
         const int a = i / 3;
@@ -711,8 +715,14 @@ __global__ void k_finalize(const SysDev* __restrict__ sys, int plain) {
     const int NA = acc_size(s.n_egroups);
     if (i < NA) {
         double v = double(s.acc_short[i]) / kEnergyScale;
+        s.acc_short[i] = 0;
         if (s.twin) v += double(s.acc_long[i]) / kEnergyScale;
         s.e_out[i] = v;
+    }
+    if (i == 0) {
+        if (s.max_delta) *s.max_delta = 0.f;
+        if (s.n_deferred)
+            for (int k = 0; k < 6; ++k) s.n_deferred[k] = 0;
     }
 }
 

@@ -87,6 +87,7 @@ class NbSystem {
     cudaEvent_t ev_md = nullptr;
     long long md_steps_total = 0, md_rollbacks = 0;
     bool warm = false;        // evaluated at least once with the current parameters
+    bool acc_clean = false;   // short-range accumulators and per-step counters are zero
     long long alloc_gen = 0;  // bumped by every device (re)allocation: recorded graphs are stale
     // recorded evaluation graphs (GR_EVAL_GRAPH): [0] short-range step, [1] rebuild step
     cudaGraphExec_t g_step[2] = {nullptr, nullptr};
