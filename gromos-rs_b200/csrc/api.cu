@@ -445,8 +445,13 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
     // 2 = each lane iterates over its own bits (width 4 or 8)
     layout = p->water_layout == 1 ? 1 : 2;
     W = (layout == 2 && p->cluster_size == 8) ? 8 : 4;
+    if (p->list_capacity < 0) {
+        set_error("gr_nb_params: list_capacity must be >= 0");
+        return GR_ERR_INVALID;
+    }
     h.W = W;
     clus_alloc = 0;  // cluster arrays depend on W
+    wcap_want = 0;   // list capacity from the (new) parameters
     h.boundary = p->boundary;
     h.twin = p->rcutp < p->rcutl - 1e-10 ? 1 : 0;  // forcefield.rs:126
     double rs = p->rcutp + p->skin, rl = p->rcutl + p->skin;
@@ -544,7 +549,9 @@ gr_status NbSystem::ensure_capacity() {
     h.max_clusters = clus_alloc;
     // entries per cluster: at most every solvent CG of the 27 neighbour cells
     double per_cell = double(NCG) / double(h.n_cells);
-    int want_w = wcap_want ? wcap_want : int(std::min<double>(nsolv, per_cell * 27.0 * 1.25 + 64.0));
+    int want_w = wcap_want ? wcap_want
+                           : (prm.list_capacity > 0 ? prm.list_capacity
+                                                    : int(std::min<double>(nsolv, per_cell * 27.0 * 1.25 + 64.0)));
     want_w = std::max(want_w, 32);
     if (want_w > wcap_alloc) {
         if ((st = alloc(&h.wl_s, size_t(clus_alloc) * want_w))) return st;

@@ -63,6 +63,7 @@ class GrNbParams(C.Structure):
         ("epsilon", C.c_double), ("epsrf", C.c_double), ("kappa", C.c_double),
         ("nsnb", C.c_int32), ("boundary", C.c_int32), ("lam", C.c_double), ("nlam", C.c_int32),
         ("kernel", C.c_int32), ("cluster_size", C.c_int32), ("water_layout", C.c_int32),
+        ("list_capacity", C.c_int32),
     ]
 
 

@@ -101,7 +101,7 @@ class _TopologyStruct:
 
 
 def make_params(p: NonbondedParams, kernel: str = "fixed", cluster_size: int = 0,
-                water_layout: int = 0) -> _lib.GrNbParams:
+                water_layout: int = 0, list_capacity: int = 0) -> _lib.GrNbParams:
     q = _lib.GrNbParams()
     q.rcutp, q.rcutl, q.skin = p.rcutp, p.rcutl, p.skin
     q.epsilon, q.epsrf, q.kappa = p.epsilon, p.epsrf, p.kappa
@@ -109,6 +109,7 @@ def make_params(p: NonbondedParams, kernel: str = "fixed", cluster_size: int = 0
     q.kernel = KERNELS[kernel]
     q.cluster_size = cluster_size
     q.water_layout = water_layout
+    q.list_capacity = list_capacity
     return q
 
 
@@ -121,7 +122,7 @@ class Forcefield:
     """
 
     def __init__(self, system: System, kernel: str = "fixed", device: int = 0, cluster_size: int = 0,
-                 water_layout: int = 0):
+                 water_layout: int = 0, list_capacity: int = 0):
         L = _lib.lib()
         self._L = L
         self.system = system
@@ -131,7 +132,7 @@ class Forcefield:
         self._h = h
         self._topo = _TopologyStruct(system.topo)
         check(L.gr_system_upload(h, C.byref(self._topo.struct)))
-        self._params = make_params(system.params, kernel, cluster_size, water_layout)
+        self._params = make_params(system.params, kernel, cluster_size, water_layout, list_capacity)
         check(L.gr_set_params(h, C.byref(self._params)))
         self.set_box(system.box)
         self.n_atoms = system.topo.n_atoms
@@ -142,6 +143,12 @@ class Forcefield:
                                           system.params.nsnb)
 
     # ---- set-up
+    def set_params(self, **changes) -> None:
+        """Change parameters (e.g. ``list_capacity``, ``water_layout``); the next step rebuilds."""
+        for k, v in changes.items():
+            setattr(self._params, k, v)
+        check(self._L.gr_set_params(self._h, C.byref(self._params)))
+
     def set_box(self, box) -> None:
         b = np.ascontiguousarray(box, dtype=np.float64)
         check(self._L.gr_set_box(self._h, _p(b, C.c_double)))

@@ -112,6 +112,8 @@ typedef struct {
     int32_t kernel;              /* GR_KERNEL_* */
     int32_t cluster_size;        /* solvent i-cluster width 4 or 8 (0 = 4) */
     int32_t water_layout;        /* 0 default, 1 lanes share mask bits (width 4), 2 lanes iterate own bits */
+    int32_t list_capacity;       /* entries per solvent i-cluster list, 0 = sized from the density; a list
+                                    that overflows is grown (doubling) and its step evaluated again */
 } gr_nb_params;
 
 /* Results of one evaluation (ForceStorage + Energy, params.rs:100-138). */

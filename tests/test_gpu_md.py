@@ -75,3 +75,23 @@ def test_md_split_calls_bit_identical():
         out.append(ff.md_state())
         ff.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_md_rollback_after_list_overflow():
+    """A rebuild inside gr_md_run overflows its (deliberately tiny) lists: the period is rolled back,
+    the lists grown and the steps run again -- the trajectory is the oracle's all the same."""
+    s = g.spc_water_system(1200, box=g.box_for_waters(1200), seed=33, rcutp=0.8, rcutl=1.2, nsnb=3)
+    m = g.masses(s)
+    v = g.maxwell_velocities(m, 300.0, 8)
+    ff = Forcefield(s)
+    ff.apply(s.pos)                      # lists sized from the density, built synchronously
+    ff.set_params(list_capacity=16)      # the next rebuild runs asynchronously with tiny lists
+    ff.upload_positions(s.pos)
+    ff.md_init(m, v, dt=0.002, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    st = ff.md_run(12)
+    x, vg = ff.md_state()
+    ff.close()
+    assert st["rollbacks"] >= 1
+    xo, vo, so = ob.OracleForcefield(s).md_run(s.pos, v, m, 12, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    assert np.abs(x - xo).max() <= 1e-5
+    assert np.sqrt(((vg - vo) ** 2).sum() / (vo ** 2).sum()) <= 1e-4

@@ -79,8 +79,8 @@ def test_pairlist_bit_exact_spc30000_twin_range():
 
 
 def compare_eval(s, kernel="fixed", steps=1, tol_rms=1e-5, tol_e=1e-5, move=0.0, seed=0, cluster_size=0,
-                 layout=0):
-    ff = Forcefield(s, kernel=kernel, cluster_size=cluster_size, water_layout=layout)
+                 layout=0, list_capacity=0):
+    ff = Forcefield(s, kernel=kernel, cluster_size=cluster_size, water_layout=layout, list_capacity=list_capacity)
     orc = ob.OracleForcefield(s)
     rng = np.random.default_rng(seed)
     pos = s.pos.copy()
@@ -239,3 +239,10 @@ def test_graph_replay_bit_identical(kind):
         pos = pos + rng.normal(0.0, 0.002, size=pos.shape)
     a.close()
     b.close()
+
+
+def test_list_overflow_regrow():
+    """Solvent lists far too small at the start: every overflow is grown and the step redone."""
+    s = generators.spc_water_system(1500, box=generators.box_for_waters(1500), seed=24, rcutp=0.8, rcutl=1.2,
+                                    nsnb=2)
+    compare_eval(s, "fixed", steps=5, move=0.002, seed=7, list_capacity=16)
