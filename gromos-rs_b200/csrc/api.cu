@@ -1193,6 +1193,10 @@ gr_status gr_ctx_create(int device, gr_ctx** out) {
 
 gr_status gr_ctx_destroy(gr_ctx* ctx) {
     if (!ctx) return GR_OK;
+    if (ctx->sys.batch_member) {
+        set_error("gr_ctx_destroy: the context is a batch member; gr_batch_remove it first");
+        return GR_ERR_STATE;
+    }
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->sys.release();

@@ -289,8 +289,10 @@ gr_status gr_batch_destroy(gr_batch* b) {
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->s0);
     b->drop_graphs();
-    for (auto& mb : b->m)
+    for (auto& mb : b->m) {
         if (mb.join) cudaEventDestroy(mb.join);
+        mb.ctx->sys.batch_member = false;
+    }
     if (b->d_errp) cudaFree(b->d_errp);
     if (b->d_flags) cudaFree(b->d_flags);
     if (b->h_flags) cudaFreeHost(b->h_flags);
@@ -320,8 +322,8 @@ gr_status gr_batch_add(gr_batch* b, gr_ctx* ctx) {
         set_error("gr_batch_add: batches run the fixed-point kernel");
         return GR_ERR_UNSUPPORTED;
     }
-    if (find_member(b, ctx)) {
-        set_error("gr_batch_add: already a member");
+    if (find_member(b, ctx) || S.batch_member) {
+        set_error("gr_batch_add: already a member of a batch");
         return GR_ERR_INVALID;
     }
     if (b->m.empty()) b->nsnb = std::max(1, S.prm.nsnb);
@@ -335,6 +337,7 @@ gr_status gr_batch_add(gr_batch* b, gr_ctx* ctx) {
     GR_CUDA(cudaEventCreateWithFlags(&mb.join, cudaEventDisableTiming));
     S.steps_since_update = S.prm.nsnb;
     S.built = false;
+    S.batch_member = true;
     b->m.push_back(mb);
     b->valid = false;
     return GR_OK;
@@ -349,6 +352,7 @@ gr_status gr_batch_remove(gr_batch* b, gr_ctx* ctx) {
             const int ph = member_phase(*b, b->m[i]);
             S.steps_since_update = ph == 0 ? S.prm.nsnb : ph;  // standalone use continues the cadence
             if (b->m[i].join) cudaEventDestroy(b->m[i].join);
+            S.batch_member = false;
             b->m.erase(b->m.begin() + long(i));
             b->valid = false;
             return GR_OK;

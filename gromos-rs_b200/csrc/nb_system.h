@@ -88,6 +88,7 @@ class NbSystem {
     long long md_steps_total = 0, md_rollbacks = 0;
     bool warm = false;        // evaluated at least once with the current parameters
     bool acc_clean = false;   // short-range accumulators and per-step counters are zero
+    bool batch_member = false;  // held by a gr_batch (its graphs point at this system)
     long long alloc_gen = 0;  // bumped by every device (re)allocation: recorded graphs are stale
     // recorded evaluation graphs (GR_EVAL_GRAPH): [0] short-range step, [1] rebuild step
     cudaGraphExec_t g_step[2] = {nullptr, nullptr};

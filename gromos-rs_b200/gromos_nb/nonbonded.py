@@ -305,7 +305,10 @@ class Forcefield:
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            self._L.gr_ctx_destroy(self._h)
+            batch = getattr(self, "_batch", None)
+            if batch is not None:  # a batch member leaves its batch first
+                batch.remove(self)
+            check(self._L.gr_ctx_destroy(self._h))
             self._h = None
 
     def __del__(self):
@@ -339,10 +342,12 @@ class Batch:
     def add(self, ff: "Forcefield") -> None:
         check(self._L.gr_batch_add(self._h, ff.handle))
         self.members.append(ff)
+        ff._batch = self
 
     def remove(self, ff: "Forcefield") -> None:
         check(self._L.gr_batch_remove(self._h, ff.handle))
         self.members.remove(ff)
+        ff._batch = None
 
     def __len__(self) -> int:
         return len(self.members)
@@ -376,6 +381,9 @@ class Batch:
         if getattr(self, "_h", None):
             self._L.gr_batch_destroy(self._h)
             self._h = None
+            for ff in self.members:
+                ff._batch = None
+            self.members = []
 
     def __del__(self):
         try:

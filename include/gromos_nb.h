@@ -134,6 +134,7 @@ typedef struct gr_ctx gr_ctx;
 /* ---- context lifecycle -------------------------------------------------- */
 /* Replaces constructing gromos-rs `Forcefield::new` (forcefield.rs:119-167). */
 gr_status gr_ctx_create(int device, gr_ctx** out);
+/* GR_ERR_STATE while the context is a batch member (gr_batch_remove it first). */
 gr_status gr_ctx_destroy(gr_ctx* ctx);
 const char* gr_last_error(void);
 /* CUDA stream used by the context (cudaStream_t as void*), for graph capture / interop. */

@@ -160,3 +160,23 @@ def standalone_variant(s, seed, n, layout, width):
     out = ff.md_state()
     ff.close()
     return out
+
+
+def test_member_close_leaves_batch():
+    """Closing a member removes it from its batch first; the C ABI refuses to destroy a member."""
+    import ctypes as C
+    from gromos_nb import _lib
+    sy = systems()[:2]
+    b = Batch()
+    a, c = member(sy[0], 1), member(sy[1], 2)
+    b.add(a)
+    b.add(c)
+    assert _lib.lib().gr_ctx_destroy(a.handle) == _lib.GR_ERR_STATE
+    a.close()                      # leaves the batch, then is destroyed
+    assert len(b) == 1
+    b.md_run(4)
+    x, v = c.md_state()
+    xr, vr = standalone(sy[1], 2, 4)
+    assert np.array_equal(x, xr) and np.array_equal(v, vr)
+    b.close()
+    c.close()
