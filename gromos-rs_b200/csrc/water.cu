@@ -6,17 +6,22 @@
 // image per CG pair taken from the first atoms (innerloops.rs:264-267) for
 // the short list, per-atom images for the long list (innerloops.rs:186).
 //
-// Layout: one warp per i-cluster of W waters; the cluster's atoms live in
-// registers as FP32 offsets from the cluster's first oxygen; one lane per
-// j-water entry of the cluster's list; bit k of the entry mask selects the
-// pair (i_k, j).  The CG-pair image comes from an FP64 difference of first
-// oxygens; FP32 arithmetic for the pairs; forces are accumulated in 64-bit
-// fixed point (2^32 per kJ mol^-1 nm^-1): i-forces in registers over the
-// whole list, reduced once per cluster, j-forces once per (cluster, j).
-// A CG pair whose first-atom vector is not certainly inside half a box edge is
-// re-imaged in FP32; if that is still not certain it is deferred to
-// k_water_deferred, which uses the exact FP64 images, so image choices are
-// always those of the reference.
+// Two layouts, both one warp per i-cluster of W waters and one lane per
+// j-water entry of the cluster's list (bit k of the entry mask selects the
+// pair (i_k, j)):
+//  - k_water_force (layout 1, W = 4): lanes share the mask bits of an entry;
+//    the cluster's atoms live in registers, i-forces are reduced across lanes;
+//  - k_water_force_it (layout 2, default, W = 4 or 8): each lane iterates over
+//    its own bits; the cluster's atoms are read from shared memory by bit
+//    index and i-forces accumulate in lane-private shared-memory rows.
+// The CG-pair image comes from an FP64 difference of first oxygens; FP32
+// arithmetic for the pairs; forces are accumulated in 64-bit fixed point
+// (2^32 per kJ mol^-1 nm^-1) with fire-and-forget reductions.  A CG pair whose
+// first-atom vector is not certainly inside half a box edge is re-imaged in
+// FP32; if that is still not certain it is deferred to the exact FP64 images
+// (process_deferred: k_water_deferred for layout 1, the last block of
+// k_water_force_it for layout 2), so image choices are always those of the
+// reference.
 #include "nb_common.cuh"
 
 namespace gnb {
@@ -741,8 +746,6 @@ constexpr size_t water_it_smem() {
     return size_t(kWaterWarps) * 32 * (W * 3 + 1) * sizeof(float4);
 }
 
-// CG pairs the main kernel deferred: exact FP64 images (first-atom shift for
-// the short list, per-atom images for the long list), FP32 pair arithmetic.
 // The deferred pairs of the shared-bit kernel (the bit-iterating kernel
 // evaluates its own in its last block).
 template <bool LJ00, bool LONG>
