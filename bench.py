@@ -272,6 +272,14 @@ def run_gpu(args, rank, world, local_rank):
     h2d = s.topo.n_atoms * 3 * 8
     d2h = s.topo.n_atoms * 3 * 8 + 8 * (2 * ff.G * ff.G + 10)
     md = run_md(ff, s, args, generators)
+    if args.kernel == "fixed" and not args.no_plain_md:
+        # the same MD on the plain FP32 kernel (the baseline the fixed-point path is compared to)
+        ff_plain = Forcefield(s, kernel="plain", device=local_rank)
+        md_plain = run_md(ff_plain, s, argparse.Namespace(warmup=args.warmup, md_steps=max(50, args.md_steps // 10)),
+                          generators)
+        ff_plain.close()
+        md["plain_kernel"] = {"ms_per_step": md_plain["ms_per_step"], "ns_per_day": md_plain["ns_per_day"],
+                              "steps": md_plain["steps"]}
     out = None
     if rank == 0:
         peak = ffma_peak(local_rank)
@@ -497,6 +505,7 @@ def main():
     ap.add_argument("--md-steps", type=int, default=1000, help="MD steps timed for ns/day")
     ap.add_argument("--layout", type=int, default=0, help="water kernel layout: 1 shared bits, 2 per-lane bits")
     ap.add_argument("--no-graph", action="store_true", help="launch kernel by kernel instead of replaying graphs")
+    ap.add_argument("--no-plain-md", action="store_true", help="skip the plain-kernel MD comparison")
     ap.add_argument("--workload", default="spc30000", choices=["spc30000", "remd", "fep", "serving"])
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=100)

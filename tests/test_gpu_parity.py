@@ -246,3 +246,37 @@ def test_list_overflow_regrow():
     s = generators.spc_water_system(1500, box=generators.box_for_waters(1500), seed=24, rcutp=0.8, rcutl=1.2,
                                     nsnb=2)
     compare_eval(s, "fixed", steps=5, move=0.002, seed=7, list_capacity=16)
+
+
+def _rel_errors(got, ref):
+    d = got - ref
+    rms = float(np.sqrt((d * d).sum() / max((ref * ref).sum(), 1e-300)))
+    mx = float(np.abs(d).max() / max(np.abs(ref).max(), 1e-300))
+    return rms, mx
+
+
+@pytest.mark.parametrize("kernel", ["fixed", "plain"])
+def test_accuracy_report(kernel):
+    """RMS and max relative errors against the FP64 oracle for forces, energy groups, virial and
+    dH/dlambda (1000 SPC waters at 1.4 nm; a solvated perturbed solute at lambda 0.5), printed."""
+    rows = []
+    s1 = generators.config1_spc1000()
+    s2 = generators.solvated_solute_system(700, 30, seed=1004, perturbed=True, lam=0.5, rc=1.4)
+    s2.params.lam = 0.5
+    for name, s in (("spc1000", s1), ("fep_solute30_lambda0.5", s2)):
+        ff = Forcefield(s, kernel=kernel)
+        r = ff.apply(s.pos)
+        o = ob.OracleForcefield(s).apply(s.pos)
+        ff.close()
+        fr, fm = force_errors(r["forces"], o["forces"])
+        lr, lm = _rel_errors(r["egroup_lj"], o["egroup_lj"]) if kernel == "fixed" else (float("nan"),) * 2
+        cr, cm = _rel_errors(r["egroup_crf"], o["egroup_crf"]) if kernel == "fixed" else (float("nan"),) * 2
+        vr, vm = _rel_errors(r["virial"], o["virial"])
+        dh = abs(r["dhdl"] - o["dhdl"]) / max(abs(o["dhdl"]), 1e-12) if abs(o["dhdl"]) > 0 else 0.0
+        rows.append((name, fr, fm, lr, lm, cr, cm, vr, vm, dh))
+        tol = 1e-5 if kernel == "fixed" else 1e-4
+        assert fr <= tol and vr <= 10 * tol
+    print(f"\naccuracy vs FP64 oracle, {kernel} kernel: name | forces rms, max | LJ groups rms, max | "
+          f"CRF groups rms, max | virial rms, max | dH/dlambda rel")
+    for row in rows:
+        print(" | ".join([row[0]] + [f"{v:.2e}" for v in row[1:]]))
