@@ -808,7 +808,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         WaterParams wp;
         if (NCG > NSCG) {
             wp = water_params();
-            (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
+            (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 64), 64, 0, s>>>(d_sys));
             if ((st = launch_water(s, wp, false))) return st;
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
@@ -827,7 +827,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         }
     } else {
         if (NCG > NSCG)  // per-step water data incl. the solvent excluded energies
-            (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 256), 256, 0, s>>>(d_sys));
+            (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 64), 64, 0, s>>>(d_sys));
         (++launches, k_pos32<<<blocks_for(N, 256), 256, 0, s>>>(d_sys));
         GR_CUDA(cudaMemsetAsync(h.f32, 0, size_t(N) * 3 * sizeof(float), s));
         GR_CUDA(cudaMemsetAsync(h.e64, 0, 16 * sizeof(double), s));
