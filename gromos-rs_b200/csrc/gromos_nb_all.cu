@@ -6,4 +6,5 @@
 #include "api.cu"
 #include "md.cu"
 #include "batch.cu"
+#include "server.cu"
 #include "noalloc.cu"

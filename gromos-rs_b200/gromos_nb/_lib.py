@@ -91,6 +91,28 @@ class GrAutotuneResult(C.Structure):
                 ("cand_ms_per_step", C.c_float * 4)]
 
 
+class GrJobDesc(C.Structure):
+    _fields_ = [("topo", C.POINTER(GrTopology)), ("params", C.POINTER(GrNbParams)), ("box", _f64p),
+                ("pos", _f64p), ("mass", _f64p), ("vel", _f64p), ("md", C.POINTER(GrMdParams)),
+                ("n_steps", C.c_int64)]
+
+
+class GrJobStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("steps_done", C.c_int64), ("t_submit", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double), ("device_bytes", C.c_int64),
+                ("stats", GrMdStats), ("error", C.c_int32), ("message", C.c_char * 160)]
+
+
+class GrServerStats(C.Structure):
+    _fields_ = [("jobs_done", C.c_int64), ("jobs_queued", C.c_int64), ("jobs_running", C.c_int64),
+                ("latency_p50_s", C.c_double), ("latency_p99_s", C.c_double), ("resident_bytes", C.c_int64),
+                ("max_resident_bytes", C.c_int64), ("max_resident_jobs", C.c_int32), ("batch_steps", C.c_int64),
+                ("jobs_failed", C.c_int64), ("jobs_cancelled", C.c_int64)]
+
+
+GR_JOB_QUEUED, GR_JOB_RUNNING, GR_JOB_DONE, GR_JOB_FAILED, GR_JOB_CANCELLED = 0, 1, 2, 3, 4
+
+
 # symbol -> (restype, argtypes)
 _SIGNATURES = {
     "gr_ctx_create": (C.c_int32, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -128,6 +150,14 @@ _SIGNATURES = {
     "gr_batch_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_ctx_device_bytes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrAutotuneResult)]),
+    "gr_server_create": (C.c_int32, [C.c_int, C.c_int64, C.c_int32, C.POINTER(C.c_void_p)]),
+    "gr_server_destroy": (C.c_int32, [C.c_void_p]),
+    "gr_server_submit": (C.c_int32, [C.c_void_p, C.POINTER(GrJobDesc), C.POINTER(C.c_int64)]),
+    "gr_server_step": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "gr_server_job": (C.c_int32, [C.c_void_p, C.c_int64, C.POINTER(GrJobStatus), _f64p, _f64p]),
+    "gr_server_cancel": (C.c_int32, [C.c_void_p, C.c_int64]),
+    "gr_server_release": (C.c_int32, [C.c_void_p, C.c_int64]),
+    "gr_server_stats": (C.c_int32, [C.c_void_p, C.POINTER(GrServerStats)]),
     "gr_batch_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrAutotuneResult)]),
     "gr_lj_crf_innerloop_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                                 C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,

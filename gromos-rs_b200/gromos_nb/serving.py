@@ -30,8 +30,10 @@ from typing import Deque, Dict, List, Optional
 
 import numpy as np
 
-from . import generators
-from .nonbonded import Batch, Forcefield
+import ctypes as C
+
+from . import _lib, generators
+from .nonbonded import Batch, Forcefield, _TopologyStruct, make_params
 from .system import System
 
 
@@ -211,3 +213,110 @@ def poisson_jobs(n_jobs: int, rate: float, seed: int, waters=(300, 20000), steps
         jobs.append(Job(job_id=k, system=s, n_steps=int(rng.integers(steps[0], steps[1] + 1)), mass=m, vel=v,
                         arrival=t))
     return jobs
+
+
+class NativeServer:
+    """The same continuous-batching server in the library (``gr_server_*``).
+
+    Jobs are handed to the C ABI with all their inputs; admission, batching
+    and retirement run in C++.  ``run`` serves jobs arriving at their
+    ``arrival`` times like :meth:`Server.run`.
+    """
+
+    def __init__(self, hbm_budget: int, device: int = 0, chunk_steps: int = 5):
+        self._L = _lib.lib()
+        h = C.c_void_p()
+        _lib.check(self._L.gr_server_create(device, int(hbm_budget), int(chunk_steps), C.byref(h)))
+        self._h = h
+        self.ids: Dict[int, int] = {}       # Job.job_id -> server job id
+        self.jobs: Dict[int, Job] = {}
+
+    def submit(self, job: Job, tau: float = -1.0, temperature: float = 300.0, params=None) -> int:
+        """Queue ``job``; ``params`` overrides the system's nonbonded parameters (a gr_nb_params)."""
+        s = job.system
+        topo = _TopologyStruct(s.topo)
+        params = make_params(s.params, "fixed") if params is None else params
+        box = np.ascontiguousarray(s.box, dtype=np.float64)
+        pos = np.ascontiguousarray(s.pos, dtype=np.float64)
+        mass = np.ascontiguousarray(job.mass, dtype=np.float64)
+        vel = np.ascontiguousarray(job.vel, dtype=np.float64)
+        md = _lib.GrMdParams(job.dt, 1, 0.1, generators.SPC_DHH, temperature, tau)
+        f64 = C.POINTER(C.c_double)
+        desc = _lib.GrJobDesc(C.pointer(topo.struct), C.pointer(params), box.ctypes.data_as(f64),
+                              pos.ctypes.data_as(f64), mass.ctypes.data_as(f64), vel.ctypes.data_as(f64),
+                              C.pointer(md), int(job.n_steps))
+        jid = C.c_int64(0)
+        _lib.check(self._L.gr_server_submit(self._h, C.byref(desc), C.byref(jid)))
+        self.ids[job.job_id] = int(jid.value)
+        self.jobs[job.job_id] = job
+        return int(jid.value)
+
+    def step(self) -> int:
+        n = C.c_int32(0)
+        _lib.check(self._L.gr_server_step(self._h, C.byref(n)))
+        return int(n.value)
+
+    def status(self, job: Job, fetch: bool = False) -> Dict:
+        st = _lib.GrJobStatus()
+        n3 = job.system.topo.n_atoms * 3
+        pos = np.zeros(n3) if fetch else None
+        vel = np.zeros(n3) if fetch else None
+        f64 = C.POINTER(C.c_double)
+        _lib.check(self._L.gr_server_job(self._h, self.ids[job.job_id], C.byref(st),
+                                         None if pos is None else pos.ctypes.data_as(f64),
+                                         None if vel is None else vel.ctypes.data_as(f64)))
+        out = {"state": st.state, "steps_done": st.steps_done, "t_submit": st.t_submit, "t_admit": st.t_admit,
+               "t_done": st.t_done, "device_bytes": st.device_bytes, "error": st.error,
+               "message": st.message.decode(errors="replace")}
+        if fetch:
+            out["pos"], out["vel"] = pos.reshape(-1, 3), vel.reshape(-1, 3)
+        return out
+
+    def cancel(self, job: Job) -> None:
+        _lib.check(self._L.gr_server_cancel(self._h, self.ids[job.job_id]))
+
+    def stats(self) -> Dict:
+        st = _lib.GrServerStats()
+        _lib.check(self._L.gr_server_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def run(self, jobs: List[Job], timeout: float = 600.0) -> None:
+        """Serve ``jobs`` arriving at their ``arrival`` times (seconds from now); finished jobs get
+        ``result_pos`` / ``result_vel`` / ``steps_done`` filled in."""
+        pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        t0 = time.perf_counter()
+        open_jobs = []
+        while True:
+            t = time.perf_counter() - t0
+            if t > timeout:
+                raise TimeoutError("serving run exceeded its time limit")
+            while pending and pending[0].arrival <= t:
+                j = pending.popleft()
+                self.submit(j)
+                open_jobs.append(j)
+            running = self.step()
+            for j in list(open_jobs):
+                st = self.status(j)
+                if st["state"] in (_lib.GR_JOB_FAILED, _lib.GR_JOB_CANCELLED):
+                    j.finished = t0 + st["t_done"]
+                    open_jobs.remove(j)
+                elif st["state"] == _lib.GR_JOB_DONE:
+                    full = self.status(j, fetch=True)
+                    j.result_pos, j.result_vel, j.steps_done = full["pos"], full["vel"], full["steps_done"]
+                    j.finished = t0 + full["t_done"]
+                    open_jobs.remove(j)
+            if not pending and not open_jobs:
+                return
+            if running == 0 and pending and not open_jobs:
+                time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.01)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.gr_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

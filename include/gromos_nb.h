@@ -271,6 +271,66 @@ gr_status gr_batch_autotune(gr_batch* b, int32_t periods, gr_autotune_result* ou
 /* Device bytes held by a context (topology, lists, accumulators, MD state). */
 gr_status gr_ctx_device_bytes(gr_ctx* ctx, int64_t* bytes);
 
+/* ---- job server: continuous batching of MD jobs on one GPU ---------------- */
+/* No gromos-rs counterpart (the reference runs one simulation per process).
+ * Jobs are submitted with all their inputs (copied: the caller's buffers are
+ * free after the call) and queue on the host.  Each gr_server_step admits
+ * queued jobs while the resident jobs' device bytes plus the next job's stay
+ * within the HBM budget, runs one chunk of MD steps (at most chunk_steps, and
+ * no job beyond its n_steps) for every resident job through one batch, and
+ * retires finished jobs (their state is copied out and their device memory
+ * freed).  Jobs submitted while others run join them at the next step call.
+ * Each job's trajectory is bit-identical to a standalone run.
+ * A job that cannot be set up (invalid topology or parameters, or a measured
+ * footprint above the whole budget) ends in GR_JOB_FAILED with its status code
+ * and message; the other jobs carry on.  gr_server_cancel ends a queued or
+ * running job (GR_JOB_CANCELLED) and frees its device memory at once. */
+enum { GR_JOB_QUEUED = 0, GR_JOB_RUNNING = 1, GR_JOB_DONE = 2, GR_JOB_FAILED = 3, GR_JOB_CANCELLED = 4 };
+
+typedef struct {
+    const gr_topology* topo;
+    const gr_nb_params* params;   /* kernel must be GR_KERNEL_FIXED */
+    const double* box;            /* 3 edge lengths */
+    const double* pos;            /* n_atoms*3 */
+    const double* mass;           /* n_atoms */
+    const double* vel;            /* n_atoms*3 or NULL (zero) */
+    const gr_md_params* md;
+    int64_t n_steps;
+} gr_job_desc;
+
+typedef struct {
+    int32_t state;                /* GR_JOB_* */
+    int64_t steps_done;
+    double t_submit, t_admit, t_done;  /* seconds since the server was created; -1 = not yet */
+    int64_t device_bytes;         /* measured footprint while resident */
+    gr_md_stats stats;            /* final statistics (done jobs) */
+    int32_t error;                /* gr_status of a failed job, else GR_OK */
+    char message[160];            /* its error message, NUL-terminated */
+} gr_job_status;
+
+typedef struct {
+    int64_t jobs_done, jobs_queued, jobs_running;
+    double latency_p50_s, latency_p99_s;   /* submit -> done, over the done jobs */
+    int64_t resident_bytes, max_resident_bytes;
+    int32_t max_resident_jobs;
+    int64_t batch_steps;
+    int64_t jobs_failed, jobs_cancelled;
+} gr_server_stats_t;
+
+typedef struct gr_server gr_server;
+gr_status gr_server_create(int device, int64_t hbm_budget_bytes, int32_t chunk_steps, gr_server** out);
+gr_status gr_server_destroy(gr_server* srv);
+gr_status gr_server_submit(gr_server* srv, const gr_job_desc* job, int64_t* job_id);
+/* Admit, run one chunk, retire; *n_running = resident jobs afterwards (may be NULL). */
+gr_status gr_server_step(gr_server* srv, int32_t* n_running);
+/* Status of a job; pos/vel (n_atoms*3, may be NULL) receive the final state of a done job. */
+gr_status gr_server_job(gr_server* srv, int64_t job_id, gr_job_status* out, double* pos, double* vel);
+/* End a queued or running job; GR_ERR_STATE if it has already ended. */
+gr_status gr_server_cancel(gr_server* srv, int64_t job_id);
+/* Forget an ended (done, failed or cancelled) job. */
+gr_status gr_server_release(gr_server* srv, int64_t job_id);
+gr_status gr_server_stats(gr_server* srv, gr_server_stats_t* out);
+
 /* ---- reference FFI stub replacement ------------------------------------ */
 /* Replaces `rust_lj_crf_innerloop` (crates/gromos-core/src/ffi.rs:55-103):
  * lj_crf_innerloop over an explicit atom-pair list with per-atom nearest

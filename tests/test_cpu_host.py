@@ -132,3 +132,18 @@ def test_batch_entry_points_without_device():
     assert L.gr_batch_create(0, C.byref(h)) == _lib.GR_ERR_NO_DEVICE
     assert L.gr_batch_md_run(None, 1) == _lib.GR_ERR_INVALID
     assert L.gr_batch_add(None, None) == _lib.GR_ERR_INVALID
+
+
+def test_server_entry_points_without_device():
+    from gromos_nb import _lib
+    import ctypes as C
+    L = _lib.lib()
+    h = C.c_void_p()
+    assert L.gr_server_create(0, 1 << 30, 5, C.byref(h)) == _lib.GR_ERR_NO_DEVICE
+    assert L.gr_server_create(0, 0, 5, C.byref(h)) == _lib.GR_ERR_INVALID
+    assert L.gr_server_create(0, 1 << 30, 0, C.byref(h)) == _lib.GR_ERR_INVALID
+    n = C.c_int32(0)
+    assert L.gr_server_step(None, C.byref(n)) == _lib.GR_ERR_INVALID
+    assert L.gr_server_submit(None, None, None) == _lib.GR_ERR_INVALID
+    assert L.gr_server_release(None, 0) == _lib.GR_ERR_INVALID
+    assert L.gr_server_destroy(None) == _lib.GR_OK
