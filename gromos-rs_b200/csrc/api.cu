@@ -391,7 +391,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&h.f_out, size_t(N) * 3))) return st;
     if ((st = alloc(&h.e_out, size_t(acc_size(G))))) return st;
     if ((st = alloc(&h.err, 4))) return st;
-    if ((st = alloc(&h.n_deferred, 6))) return st;  // deferred counts [2], water work counters [2], blocks done [2]
+    if ((st = alloc(&h.n_deferred, 8))) return st;  // deferred counts [2], water work counters [2], blocks done [2], search counter
     if ((st = alloc(&h.max_delta, 1))) return st;
     GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
     GR_CUDA(cudaMemset(h.f_long, 0, size_t(N) * 3 * sizeof(long long)));
@@ -520,7 +520,6 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.cell_start, size_t(n) + 1))) return st;
         if ((st = alloc(&h.cell_nsolute, size_t(n)))) return st;
         if ((st = alloc(&h.cell_nclus, size_t(n) + 1))) return st;
-        if ((st = alloc(&h.cell_part, size_t(n) + 1))) return st;
         cells_alloc = n;
     }
     int nsolv = NCG - NSCG;
@@ -530,6 +529,10 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.clus_first, size_t(maxc)))) return st;
         if ((st = alloc(&h.clus_n, size_t(maxc)))) return st;
         if ((st = alloc(&h.slot_cg, size_t(maxc) * W))) return st;
+        if ((st = alloc(&h.clus_geo, size_t(maxc)))) return st;
+        if ((st = alloc(&h.clus_ext, size_t(maxc)))) return st;
+        if ((st = alloc(&h.clus_x64, size_t(maxc) * 4))) return st;
+        if ((st = alloc(&h.slot_off, size_t(maxc) * W))) return st;
         if ((st = alloc(&h.wn_s, size_t(maxc)))) return st;
         if ((st = alloc(&h.wn_l, size_t(maxc)))) return st;
         if ((st = alloc(&h.wrec, size_t(maxc) * W))) return st;
@@ -698,13 +701,29 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
             P.c2l = h.c2l;
             P.boundary = h.boundary;
             P.wcap = h.wcap;
-            const unsigned g = unsigned(h.max_clusters / kSearchWarps + h.n_cells + 1);
+            // persistent: one wave of blocks (SMs x resident blocks per SM),
+            // fewer for a small system; warps draw clusters from a counter
+            const long long need = (static_cast<long long>(h.max_clusters) + kSearchWarps - 1) / kSearchWarps;
+            auto search_grid = [&](int occ) {
+                return unsigned(std::max<long long>(1, std::min<long long>(static_cast<long long>(sm_count()) * occ, need)));
+            };
+#define GR_WATER_SEARCH(WW, POP)                                                                            \
+    do {                                                                                                    \
+        static int occ = 0;                                                                                 \
+        if (!occ) {                                                                                         \
+            GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_water_search<WW, POP>,            \
+                                                                  kSearchWarps * 32, 0));                   \
+            if (occ < 1) occ = 1;                                                                           \
+        }                                                                                                   \
+        (++launches, k_water_search<WW, POP><<<search_grid(occ), kSearchWarps * 32, 0, s>>>(d_sys, P));     \
+    } while (0)
             if (layout == 1)
-                (++launches, k_water_search<4, false><<<g, kSearchWarps * 32, 0, s>>>(d_sys, P));
+                GR_WATER_SEARCH(4, false);
             else if (W == 4)
-                (++launches, k_water_search<4, true><<<g, kSearchWarps * 32, 0, s>>>(d_sys, P));
+                GR_WATER_SEARCH(4, true);
             else
-                (++launches, k_water_search<8, true><<<g, kSearchWarps * 32, 0, s>>>(d_sys, P));
+                GR_WATER_SEARCH(8, true);
+#undef GR_WATER_SEARCH
         }
         if (NSCG > 0) (++launches, k_solute_search<<<blocks_for(NSCG, 4), 128, 0, s>>>(d_sys));
         if (n_pert > 0 && NSCG > 0) {
@@ -792,7 +811,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         GR_CUDA(cudaMemsetAsync(h.acc_short, 0, size_t(NA) * sizeof(long long), s));
         if (NCG > NSCG) {
             GR_CUDA(cudaMemsetAsync(h.max_delta, 0, sizeof(float), s));
-            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 6 * sizeof(int), s));
+            GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 8 * sizeof(int), s));
         }
     }
     if (NCG > NSCG) GR_CUDA(cudaMemsetAsync(h.fs_short, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));

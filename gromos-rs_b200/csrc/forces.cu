@@ -35,57 +35,84 @@ constexpr float kE = 16777216.0f;     // energy / virial fixed-point scale (2^24
 
 // ---------------------------------------------------------------------------
 __global__ void k_water_prep(const SysDev* __restrict__ sys) {
+    // Descriptor fields and the molecule's coordinates are read into registers
+    // before the record is stored (a store through a descriptor pointer would
+    // otherwise make every later field read wait for it).  Solvent molecules
+    // are 3-site (checked at upload).
     const SysDev& s = sys[blockIdx.y];
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nslots = s.n_clusters[0] * s.W;
+    const int* __restrict__ slot_cg = s.slot_cg;
+    const double* __restrict__ pos = s.pos;
+    const double* __restrict__ charge = s.charge;
+    WaterRec* __restrict__ wrec = s.wrec;
+    const int nsa = s.n_solute_atoms, nscg = s.n_solute_cg;
+    const bool excl = s.excl_atoms < s.n_atoms;
+    const bool rect = s.boundary == 1;
+    const double bx = s.box[0], by = s.box[1], bz = s.box[2];
+    const double ibx = s.inv_box[0], iby = s.inv_box[1], ibz = s.inv_box[2];
+    const double fpe = s.fpe, crf2 = s.crf_2cut3i;
+    float* max_delta = s.max_delta;
+    long long* acc_short = s.acc_short;
+    const int G = s.n_egroups, gs = s.solvent_group < 0 ? 0 : s.solvent_group;
     double e_excl = 0.0;
     float m = 0.f;
-    if (slot < s.n_clusters[0] * s.W) {
-        const int cg = s.slot_cg[slot];
+    if (slot < nslots) {
+        const int cg = slot_cg[slot];
         if (cg >= 0) {
-            const int a0 = s.n_solute_atoms + 3 * (cg - s.n_solute_cg);  // solvent CGs are whole 3-site molecules
-            const double x0 = s.pos[3 * a0], y0 = s.pos[3 * a0 + 1], z0 = s.pos[3 * a0 + 2];
+            const int a0 = nsa + 3 * (cg - nscg);  // solvent CGs are whole 3-site molecules
+            double p[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) p[q] = pos[3 * a0 + q];
+            double q3[3] = {0.0, 0.0, 0.0};
+            if (excl)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) q3[a] = charge[a0 + a];
             WaterRec w;
-            w.x0 = x0;
-            w.y0 = y0;
-            w.z0 = z0;
-            w.h1x = float(s.pos[3 * a0 + 3] - x0);
-            w.h1y = float(s.pos[3 * a0 + 4] - y0);
-            w.h1z = float(s.pos[3 * a0 + 5] - z0);
-            w.h2x = float(s.pos[3 * a0 + 6] - x0);
-            w.h2y = float(s.pos[3 * a0 + 7] - y0);
-            w.h2z = float(s.pos[3 * a0 + 8] - z0);
-            s.wrec[slot] = w;
+            w.x0 = p[0];
+            w.y0 = p[1];
+            w.z0 = p[2];
+            w.h1x = float(p[3] - p[0]);
+            w.h1y = float(p[4] - p[1]);
+            w.h1z = float(p[5] - p[2]);
+            w.h2x = float(p[6] - p[0]);
+            w.h2y = float(p[7] - p[1]);
+            w.h2z = float(p[8] - p[2]);
             // extent of the molecule (per-atom images of the long list need it)
             m = fmaxf(fmaxf(fabsf(w.h1x), fabsf(w.h1y)), fmaxf(fabsf(w.h1z), fabsf(w.h2x)));
             m = fmaxf(m, fmaxf(fabsf(w.h2y), fabsf(w.h2z)));
             // solvent excluded pairs: energy only, -q_i q_j fpe crf_2cut3i r^2
             // (rf_excluded_interactions, excluded.rs:81-96)
-            if (s.excl_atoms < s.n_atoms)
-                for (int a = 0; a < s.aps; ++a)
-                    for (int b = a + 1; b < s.aps; ++b) {
-                        const int i = a0 + a, j = a0 + b;
-                        double rx, ry, rz;
-                        nearest_image_exact(s, s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], s.pos[3 * j],
-                                            s.pos[3 * j + 1], s.pos[3 * j + 2], rx, ry, rz);
-                        e_excl += -s.charge[i] * s.charge[j] * s.fpe * s.crf_2cut3i * len2_exact(rx, ry, rz);
+            if (excl)
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = a + 1; b < 3; ++b) {
+                        double rx = __dsub_rn(p[3 * a], p[3 * b]);
+                        double ry = __dsub_rn(p[3 * a + 1], p[3 * b + 1]);
+                        double rz = __dsub_rn(p[3 * a + 2], p[3 * b + 2]);
+                        if (rect) {
+                            rx = image_exact(rx, bx, ibx);
+                            ry = image_exact(ry, by, iby);
+                            rz = image_exact(rz, bz, ibz);
+                        }
+                        e_excl += -q3[a] * q3[b] * fpe * crf2 * len2_exact(rx, ry, rz);
                     }
+            wrec[slot] = w;
         }
     }
     // one atomicMax per warp (the extents are >= 0, so their bit patterns order like the values)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(reinterpret_cast<int*>(s.max_delta), __float_as_int(m));
-    if (s.excl_atoms < s.n_atoms) {
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(reinterpret_cast<int*>(max_delta), __float_as_int(m));
+    if (excl) {
         long long v = warp_sum_ll(to_fixed_d(e_excl, kEnergyScale));
         __shared__ unsigned long long sh;
         if (threadIdx.x == 0) sh = 0ull;
         __syncthreads();
         if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh, static_cast<unsigned long long>(v));
         __syncthreads();
-        if (threadIdx.x == 0 && sh) {
-            const int G = s.n_egroups, gs = s.solvent_group < 0 ? 0 : s.solvent_group;
-            atomicAdd(reinterpret_cast<unsigned long long*>(s.acc_short + G * G + gs * G + gs), sh);
-        }
+        if (threadIdx.x == 0 && sh) atomicAdd(reinterpret_cast<unsigned long long*>(acc_short + G * G + gs * G + gs), sh);
     }
 }
 
@@ -686,47 +713,63 @@ __global__ void k_pert_terms(const SysDev* __restrict__ sys) {
 __global__ void k_finalize(const SysDev* __restrict__ sys, int plain) {
     // One thread per force component; a water atom's component also gathers
     // its cluster slot's sum (solvent CG w = atoms nsa + 3w .. nsa + 3w + 2).
+    // The descriptor's fields are read into registers first and every load is
+    // issued before the first store: a store through a pointer taken from the
+    // descriptor would otherwise force the later field reads to wait for it.
     const SysDev& s = sys[blockIdx.y];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n3 = 3 * s.n_atoms, nsa = s.n_solute_atoms, nscg = s.n_solute_cg;
+    const int twin = s.twin, NA = acc_size(s.n_egroups);
+    long long* __restrict__ f_short = s.f_short;
+    const long long* __restrict__ f_long = s.f_long;
+    const long long* __restrict__ fs_short = s.fs_short;
+    const long long* __restrict__ fs_long = s.fs_long;
+    const int* __restrict__ cg_slot = s.cg_slot;
+    const float* __restrict__ f32 = s.f32;
+    const float* __restrict__ f32_long = s.f32_long;
+    double* __restrict__ f_out = s.f_out;
+    long long* __restrict__ acc_short = s.acc_short;
+    const long long* __restrict__ acc_long = s.acc_long;
+    double* __restrict__ e_out = s.e_out;
+    float* max_delta = s.max_delta;
+    int* n_deferred = s.n_deferred;
+    const bool water = s.wrec != nullptr && !plain;
     const double inv = 1.0 / kForceScale;
     // Every per-atom short-range accumulator is read by exactly one thread
     // here, which also clears it for the next evaluation (the per-slot water
     // sums are cleared by one contiguous memset; the long-range cache persists).
-    if (i < 3 * s.n_atoms) {
-        long long fx = s.f_short[i];
-        s.f_short[i] = 0;
-        if (s.twin) fx += s.f_long[i];
-        const int nsa = s.n_solute_atoms;
+    if (i < n3) {
+        long long fx = f_short[i];
+        if (twin) fx += f_long[i];
         const int a = i / 3;
-        if (a >= nsa && s.wrec != nullptr && !plain) {
+        if (a >= nsa && water) {
             const int w = (a - nsa) / 3;
-            const int slot = s.cg_slot[s.n_solute_cg + w];
+            const int slot = cg_slot[nscg + w];
             const int k = i - 3 * (nsa + 3 * w);
-            fx += s.fs_short[slot * 9 + k];
-            if (s.twin) fx += s.fs_long[slot * 9 + k];
+            fx += fs_short[slot * 9 + k];
+            if (twin) fx += fs_long[slot * 9 + k];
         }
         double v = double(fx) * inv;
         if (plain) {
-            v += double(s.f32[i]);
-            if (s.twin) v += double(s.f32_long[i]);
+            v += double(f32[i]);
+            if (twin) v += double(f32_long[i]);
         }
-        s.f_out[i] = v;
+        f_out[i] = v;
+        f_short[i] = 0;
     }
-    const int NA = acc_size(s.n_egroups);
     if (i < NA) {
-        double v = double(s.acc_short[i]) / kEnergyScale;
-        s.acc_short[i] = 0;
-        if (s.twin) v += double(s.acc_long[i]) / kEnergyScale;
-        s.e_out[i] = v;
+        double v = double(acc_short[i]) / kEnergyScale;
+        if (twin) v += double(acc_long[i]) / kEnergyScale;
+        e_out[i] = v;
+        acc_short[i] = 0;
     }
     if (i == 0) {
-        if (s.max_delta) *s.max_delta = 0.f;
-        if (s.n_deferred)
-            for (int k = 0; k < 6; ++k) s.n_deferred[k] = 0;
+        if (max_delta) *max_delta = 0.f;
+        if (n_deferred)
+            for (int k = 0; k < 6; ++k) n_deferred[k] = 0;
     }
 }
 
-// Plain-kernel energies (FP64 buffers) folded into the group/virial outputs.
 __global__ void k_finalize_plain_energies(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
     if (threadIdx.x != 0 || blockIdx.x != 0) return;

@@ -127,8 +127,13 @@ __device__ bool settle_molecule(const D3 old[3], D3 nw[3], D3 v[3], const MdDev&
 // (leap-frog of its atoms, then SETTLE).  Forces are the finalized FP64
 // forces of this step's evaluation.
 __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
+    // descriptor pointers in registers and every load of a unit before its
+    // stores (stores through descriptor pointers would otherwise order the
+    // later reads behind them)
     const SysDev& s = *sys;
     const int nsa = s.n_solute_atoms, n = s.n_atoms;
+    const double* __restrict__ f_out = s.f_out;
+    double* __restrict__ pos = s.pos;
     const int n_mol = md.settle ? (n - nsa) / 3 : 0;
     const int n_units = md.settle ? nsa + n_mol : n;
     const double lambda = berendsen_lambda(md);
@@ -138,24 +143,26 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
         const int a0 = mol ? nsa + 3 * (u - nsa) : u;
         const int na = mol ? 3 : 1;
         D3 old[3], nw[3], v[3];
+        double mass[3];
         for (int k = 0; k < na; ++k) {
             const int i = a0 + k;
-            const D3 f = d3(s.f_out[3 * i], s.f_out[3 * i + 1], s.f_out[3 * i + 2]);
+            const D3 f = d3(f_out[3 * i], f_out[3 * i + 1], f_out[3 * i + 2]);
             const double im = md.inv_mass[i];
+            mass[k] = md.mass[i];
             v[k] = (d3(md.vel[3 * i], md.vel[3 * i + 1], md.vel[3 * i + 2]) + f * im * md.dt) * lambda;
-            old[k] = d3(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2]);
+            old[k] = d3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
             nw[k] = old[k] + v[k] * md.dt;
         }
         if (mol && !settle_molecule(old, nw, v, md)) atomicAdd(md.failures, 1);
         for (int k = 0; k < na; ++k) {
             const int i = a0 + k;
-            s.pos[3 * i] = nw[k].x;
-            s.pos[3 * i + 1] = nw[k].y;
-            s.pos[3 * i + 2] = nw[k].z;
+            pos[3 * i] = nw[k].x;
+            pos[3 * i + 1] = nw[k].y;
+            pos[3 * i + 2] = nw[k].z;
             md.vel[3 * i] = v[k].x;
             md.vel[3 * i + 1] = v[k].y;
             md.vel[3 * i + 2] = v[k].z;
-            ke += to_fixed_d(0.5 * md.mass[i] * dot3(v[k], v[k]), kEnergyScale);
+            ke += to_fixed_d(0.5 * mass[k] * dot3(v[k], v[k]), kEnergyScale);
         }
     }
     ke = warp_sum_ll(ke);

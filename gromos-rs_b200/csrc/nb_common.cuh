@@ -25,7 +25,7 @@ constexpr int kMaxGroups = 16;        // energy groups
 constexpr double kForceScale = 4294967296.0;   // 2^32: force fixed point
 constexpr double kEnergyScale = 16777216.0;    // 2^24: energy / virial fixed point
 constexpr int kMaxCellCGs = 2048;     // bitonic per-cell sort capacity
-constexpr int kSearchWarps = 8;       // clusters (warps) per block of the water search
+constexpr int kSearchWarps = 4;       // warps per block of the water search
 
 // Error flags (bitwise OR into SysDev::err[0]).
 enum : int {
@@ -103,12 +103,15 @@ struct SysDev {
     int* cell_start;           // n_cells+1
     int* cell_nsolute;         // n_cells
     int* cell_nclus;           // n_cells+1 (scanned in place -> cluster start)
-    int* cell_part;            // n_cells+1 (groups of 8 clusters per cell, scanned in place)
     int* sorted_cg;            // n_cg: sorted position -> CG
     double* sref;              // [3][n_cg + 2] sorted reference positions (x, y, z planes)
     int* cg_spos;              // n_cg: CG -> sorted position
     int* clus_cell;            // cluster -> cell
     int* clus_first;           // cluster -> first sorted position
+    float4* clus_geo;          // cluster: FP32 bounding-box centre, radius of the offsets from the first atom
+    float4* clus_ext;          // cluster: FP32 bounding-box half extents
+    double* clus_x64;          // cluster*4: FP64 first-atom position (x, y, z, 0)
+    float4* slot_off;          // slot: FP32 offset from the cluster's first atom
     int* clus_n;               // cluster -> #CGs (<= W)
     int* n_clusters;           // [1]
     int max_clusters;
@@ -131,7 +134,7 @@ struct SysDev {
     long long* fs_short;       // [max_clusters*W*9] water forces per slot (fixed 2^32)
     long long* fs_long;        // same, long-range cache
     int* deferred;             // [2 * 2 * defer_cap] (i slot, j slot): short, then long
-    int* n_deferred;           // [6]: deferred pairs, water-kernel work counters, finished blocks (short, long each)
+    int* n_deferred;           // [8]: deferred pairs, water-kernel work counters, finished blocks (short, long each), search counter
     float* max_delta;          // [1] largest |offset| component of a water atom from its first atom (this step)
     int defer_cap;
     // ---- plain-kernel data

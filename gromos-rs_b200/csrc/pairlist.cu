@@ -194,18 +194,16 @@ __global__ void k_cell_sort(const SysDev* __restrict__ sys) {
         s.cell_nsolute[cell] = nsol;
         int nsolv = n - nsol;
         s.cell_nclus[cell] = (nsolv + s.W - 1) / s.W;
-        s.cell_part[cell] = (s.cell_nclus[cell] + kSearchWarps - 1) / kSearchWarps;
     }
 }
 
 __global__ void k_scan_clusters(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
     __shared__ int total;
-    block_exclusive_scan(s.cell_part, s.cell_part, s.n_cells, nullptr);
-    __syncthreads();
     block_exclusive_scan(s.cell_nclus, s.cell_nclus, s.n_cells, &total);
     __syncthreads();
     if (threadIdx.x == 0) {
+        s.n_deferred[6] = 0;  // the water search's cluster counter
         if (total > s.max_clusters) {
             atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
             total = s.max_clusters;
@@ -231,16 +229,45 @@ __global__ void k_cluster_setup(const SysDev* __restrict__ sys) {
         s.clus_cell[k] = cell;
         s.clus_first[k] = first;
         s.clus_n[k] = n;
+        // search geometry: FP64 first atom, FP32 member offsets from it (one
+        // rounding of the FP64 difference), radius bounding the offsets
+        const int stride = s.n_cg + 2;
+        const double x0 = s.sref[first], y0 = s.sref[stride + first], z0 = s.sref[2 * stride + first];
+        float rad = 0.f;
         for (int m = 0; m < s.W; ++m) {
             int slot = k * s.W + m;
+            float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
             if (m < n) {
                 int cg = s.sorted_cg[first + m];
                 s.slot_cg[slot] = cg;
                 s.cg_slot[cg] = slot;
+                o.x = float(s.sref[first + m] - x0);
+                o.y = float(s.sref[stride + first + m] - y0);
+                o.z = float(s.sref[2 * stride + first + m] - z0);
+                rad = fmaxf(rad, sqrtf(o.x * o.x + o.y * o.y + o.z * o.z));
             } else {
                 s.slot_cg[slot] = -1;
             }
+            s.slot_off[slot] = o;
         }
+        s.clus_x64[4 * k] = x0;
+        s.clus_x64[4 * k + 1] = y0;
+        s.clus_x64[4 * k + 2] = z0;
+        s.clus_x64[4 * k + 3] = 0.0;
+        // axis-aligned bounding box of the first atoms (FP64, then FP32 centre
+        // and slightly widened half extents)
+        double lo[3] = {x0, y0, z0}, hi[3] = {x0, y0, z0};
+        for (int m = 1; m < n; ++m)
+            for (int d = 0; d < 3; ++d) {
+                const double v = s.sref[d * stride + first + m];
+                lo[d] = fmin(lo[d], v);
+                hi[d] = fmax(hi[d], v);
+            }
+        s.clus_geo[k] = make_float4(float(0.5 * (lo[0] + hi[0])), float(0.5 * (lo[1] + hi[1])),
+                                    float(0.5 * (lo[2] + hi[2])), rad * (1.f + 1e-5f) + 1e-5f);
+        s.clus_ext[k] = make_float4(float(0.5 * (hi[0] - lo[0])) * (1.f + 1e-6f) + 1e-6f,
+                                    float(0.5 * (hi[1] - lo[1])) * (1.f + 1e-6f) + 1e-6f,
+                                    float(0.5 * (hi[2] - lo[2])) * (1.f + 1e-6f) + 1e-6f, 0.f);
     }
 }
 
@@ -262,30 +289,29 @@ __device__ __forceinline__ int axis_offsets(int g, int* off) {
     return 1;
 }
 
-// Water-water search, tiled by cell.  One block per group of up to
-// kSearchWarps clusters of one cell; the solvent CGs of each neighbour cell are
-// staged in shared memory in tiles of kTile, the (cluster, chunk of 32) pairs
-// of a tile that pass the bounding-sphere test are shared out over the
-// block's warps, and each cluster's warp then appends its results in chunk
-// order.  Pair {i_k, j} belongs to this
-// cluster iff j's sorted position is after i_k's, so every unordered CG pair
-// is listed once.  Bit k of the short (long) mask is set when the reference
-// test puts (i_k, j) in the short (long) range; the solvent reference point
-// is the first atom for both CGs (pairlist.rs:359-368).
+// Water-water search, one warp per i-cluster (clusters handed out by a
+// counter, so every warp stays busy to the end).  Pair {i_k, j} belongs to
+// this cluster iff j's sorted position is after i_k's, so every unordered CG
+// pair is listed once.  Bit k of the short (long) mask is set when the
+// reference test puts (i_k, j) in the short (long) range; the solvent
+// reference point is the first atom for both CGs (pairlist.rs:359-368).
 //
-// Candidates are staged with FP64 positions and FP32 min-image offsets from
-// the centre of their chunk of 32; a warp skips a chunk whose bounding sphere
-// is out of reach of its cluster.  The test runs in FP32 on
-// cluster-to-chunk vectors (FP64 image, rounded once) minus the offsets; a
-// squared distance within a relative 1e-5 of either cutoff,
-// or a vector near half a box edge (image not certain in FP32), is decided by
-// the exact FP64 test (nearest_image_exact + len2_exact).  The FP32 error is
-// below 1e-6 relative, so the set is exactly the reference's.
+// The candidates are the j-clusters of the neighbour cells at or after this
+// one; their cluster ranges are concatenated and swept 32 at a time with a
+// conservative FP32 test of the gap between the two clusters' axis-aligned
+// bounding boxes (1e-3 nm margin).  Survivors queue in shared memory in candidate order; for
+// 32 of them at a time the cluster-to-cluster vector C is taken with the FP64
+// image of the two first atoms and rounded once, then lanes classify 32 / W
+// survivors x W members per pass: the pair vector is the i offset + C - the
+// j offset (offsets from the cluster's first atom, FP32).  A squared distance
+// within a relative 1e-5 of either cutoff, or a vector near half a box edge
+// (image not certain in FP32), is decided by the exact FP64 test
+// (nearest_image_exact + len2_exact).  The FP32 error is below 1e-6
+// relative, so the set is exactly the reference's.
 //
 // Each cluster's entries are collected in shared memory and written out
-// sorted by mask value, so warp chunks of the force kernel see similar masks.
-constexpr int kTile = 256;
-
+// sorted by mask value (or popcount), so warp chunks of the force kernel see
+// similar masks.
 // Per-launch constants of the water search (kernel parameters, constant bank).
 struct SearchParams {
     double box[3], inv_box[3];
@@ -358,314 +384,213 @@ __device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restric
 }
 
 template <int W, bool POPSORT>
-__global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
+__global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
     const SysDev& s = sys[blockIdx.y];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int b = blockIdx.x;
-    if (b >= s.cell_part[s.n_cells]) return;  // the whole block leaves together
-    int lo = 0, hi = s.n_cells - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s.cell_part[mid] <= b)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    const int cell = lo;
-    const int ci = s.cell_nclus[cell] + (b - s.cell_part[cell]) * kSearchWarps + warp;
-    const bool active = ci < s.cell_nclus[cell + 1];
-    constexpr int kChunks = kTile / 32;
-
-    __shared__ double tx[kTile], ty[kTile], tz[kTile];
-    __shared__ float fx[kTile], fy[kTile], fz[kTile];       // offsets from the chunk centre (min image)
-    __shared__ double chx[kChunks], chy[kChunks], chz[kChunks];  // chunk centres
-    __shared__ float chr[kChunks];                          // chunk radii
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr int kPer = 32 / W;  // survivors per classification pass
     __shared__ uint32_t ebuf_s[kSearchWarps][kEntBuf], ebuf_l[kSearchWarps][kEntBuf];
-    // the block's clusters (one per warp, all in this cell): FP64 first atoms
-    // (exact tests), FP32 offsets from the first one, sizes, reach, counters
-    __shared__ double cxs[kSearchWarps][3][8];
-    __shared__ float cex[kSearchWarps][3][8];
-    __shared__ int c_n[kSearchWarps], c_first[kSearchWarps];
-    __shared__ float c_reach[kSearchWarps], c_rad[kSearchWarps];
-    // (cluster, chunk) pairs of the current tile that survive the bounding
-    // sphere test: the block's warps share them out, so a warp whose cluster
-    // sees few chunks does not wait at the tile barrier for one that sees
-    // many.  Their masks land at fixed places (res_*[cluster chunk][lane]) and
-    // each cluster's warp appends them in chunk order afterwards, so the
-    // lists come out in the same order on every run.
-    __shared__ int n_items;
-    __shared__ int it_cc[kSearchWarps * kChunks];
-    __shared__ float it_C[kSearchWarps * kChunks][3];
-    __shared__ uint8_t res_s[kSearchWarps * kChunks][32], res_l[kSearchWarps * kChunks][32];
-    __shared__ unsigned c_surv[kSearchWarps];  // bit ch: chunk ch survived for this cluster
-
-    {
-        int n = 0, first = 0;
-        if (active) {
-            n = s.clus_n[ci];
-            first = s.clus_first[ci];
-        }
-        if (lane < W) {
-            double x = 0, y = 0, z = 0;
-            if (lane < n) {
-                const int cg = s.sorted_cg[first + lane];
-                x = s.ref[3 * cg];
-                y = s.ref[3 * cg + 1];
-                z = s.ref[3 * cg + 2];
-            }
-            cxs[warp][0][lane] = x;
-            cxs[warp][1][lane] = y;
-            cxs[warp][2][lane] = z;
-        }
-        __syncwarp();
-        if (lane < W) {
-            const bool v = lane < n;
-            const float ox = v ? float(cxs[warp][0][lane] - cxs[warp][0][0]) : 0.f;
-            const float oy = v ? float(cxs[warp][1][lane] - cxs[warp][1][0]) : 0.f;
-            const float oz = v ? float(cxs[warp][2][lane] - cxs[warp][2][0]) : 0.f;
-            cex[warp][0][lane] = ox;
-            cex[warp][1][lane] = oy;
-            cex[warp][2][lane] = oz;
-        }
-        __syncwarp();
-        if (lane == 0) {
-            float rad = 0.f;
-            for (int k = 0; k < n; ++k)
-                rad = fmaxf(rad, sqrtf(cex[warp][0][k] * cex[warp][0][k] + cex[warp][1][k] * cex[warp][1][k] +
-                                       cex[warp][2][k] * cex[warp][2][k]));
-            c_n[warp] = n;
-            c_first[warp] = first;
-            c_rad[warp] = rad;
-            c_reach[warp] = sqrtf(float(P.c2l)) + rad + 1e-3f;
-        }
-    }
+    __shared__ int q_jc[kSearchWarps][64];          // surviving j-clusters, candidate order
+    __shared__ float4 q_d[kSearchWarps][32 * W];    // per survivor and member: i-first to j-member vector, flags
+    __shared__ int seg_lo[kSearchWarps][32], seg_pre[kSearchWarps][33];
+    const int nclus = s.n_clusters[0];
+    const float4* __restrict__ geo = s.clus_geo;
+    const float4* __restrict__ ext = s.clus_ext;
+    const float4* __restrict__ soff = s.slot_off;
+    const double* __restrict__ x64 = s.clus_x64;
+    const double* __restrict__ sref = s.sref;
+    const int stride = s.n_cg + 2;
     const float c2s = float(P.c2s), c2l = float(P.c2l);
     const float s_lo = c2s * (1.f - 1e-5f), s_hi = c2s * (1.f + 1e-5f);
     const float l_lo = c2l * (1.f - 1e-5f), l_hi = c2l * (1.f + 1e-5f);
+    const float rcl = sqrtf(c2l) * (1.f + 1e-6f) + 1e-3f;
     const float limx = P.boundary ? P.half_boxf[0] - 1e-4f : 3e38f;
     const float limy = P.boundary ? P.half_boxf[1] - 1e-4f : 3e38f;
     const float limz = P.boundary ? P.half_boxf[2] - 1e-4f : 3e38f;
     const int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
-    const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
-    int ox[3], oy[3], oz[3];
-    const int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
     const unsigned below = (1u << lane) - 1u;
-    uint32_t* outs = s.wl_s + static_cast<size_t>(active ? ci : 0) * P.wcap;
-    uint32_t* outl = s.wl_l + static_cast<size_t>(active ? ci : 0) * P.wcap;
-    int cnt_s = 0, cnt_l = 0;
-    // neighbour cells at or after this one (block-uniform), then the tiles of
-    // their solvent CGs; the next tile is prefetched into registers while the
-    // current one is processed
-    __shared__ int ncell[27];
-    __shared__ int n_nc;
-    if (threadIdx.x == 0) {
-        int m = 0;
-        for (int iz = 0; iz < nz; ++iz)
-            for (int iy = 0; iy < ny; ++iy)
-                for (int ix = 0; ix < nx; ++ix) {
-                    const int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
-                    if (nc >= cell) ncell[m++] = nc;
-                }
-        n_nc = m;
-    }
-    __syncthreads();
-    const int stride = s.n_cg + 2;
-    int ic = 0, t0 = 0;  // current tile: neighbour index ic, offset t0 into its solvent range
-    auto tile_range = [&](int icc, int& j0, int& j1) {
-        const int nc = ncell[icc];
-        j0 = s.cell_start[nc] + s.cell_nsolute[nc];
-        j1 = s.cell_start[nc + 1];
-    };
-    // skip empty neighbour ranges
-    int j0 = 0, j1 = 0;
-    while (ic < n_nc) {
-        tile_range(ic, j0, j1);
-        if (j1 > j0) break;
-        ++ic;
-    }
-    double px = 0, py = 0, pz = 0;
-    if (ic < n_nc && threadIdx.x < min(kTile, j1 - j0)) {
-        px = s.sref[j0 + threadIdx.x];
-        py = s.sref[stride + j0 + threadIdx.x];
-        pz = s.sref[2 * stride + j0 + threadIdx.x];
-    }
-    while (ic < n_nc) {
-        const int nc = ncell[ic];
-        const int tbeg = j0 + t0;
-        const int tn = min(kTile, j1 - tbeg);
-        const int nch = (tn + 31) >> 5;
-        const int slot0 = s.cell_nclus[nc] * W;
-        __syncthreads();
-        if (threadIdx.x == 0) n_items = 0;
-        if (threadIdx.x < kSearchWarps) c_surv[threadIdx.x] = 0u;
-        if (threadIdx.x < tn) {
-            tx[threadIdx.x] = px;
-            ty[threadIdx.x] = py;
-            tz[threadIdx.x] = pz;
+    for (;;) {
+        int ci = 0;
+        if (lane == 0) ci = atomicAdd(s.n_deferred + 6, 1);
+        ci = __shfl_sync(0xffffffffu, ci, 0);
+        if (ci >= nclus) break;
+        const int n_i = s.clus_n[ci], first_i = s.clus_first[ci], cell = s.clus_cell[ci];
+        const float4 gi = geo[ci], hi = ext[ci];
+        const double X0 = x64[4 * ci], Y0 = x64[4 * ci + 1], Z0 = x64[4 * ci + 2];
+        float ex[W], ey[W], ez[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const float4 o = soff[ci * W + k];
+            ex[k] = o.x;
+            ey[k] = o.y;
+            ez[k] = o.z;
         }
-        // chunk of 32 candidates per warp: centre = first member, FP32 min-image
-        // offsets of the members, radius = largest offset
+        // neighbour cells at or after this one (lane l < 27 takes stencil
+        // offset l, in z-y-x order; grids of 1 or 2 cells along an axis use
+        // the de-duplicated offsets of axis_offsets) as cluster ranges; the
+        // own cell's range starts at this cluster
+        int total;
         {
-            const int cbeg = warp * 32;
-            if (cbeg < tn) {
-                const double cx0 = __shfl_sync(0xffffffffu, px, 0);
-                const double cy0 = __shfl_sync(0xffffffffu, py, 0);
-                const double cz0 = __shfl_sync(0xffffffffu, pz, 0);
-                float r = 0.f;
-                if (threadIdx.x < tn) {
-                    double dx = px - cx0, dy = py - cy0, dz = pz - cz0;
+            const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
+            const int ix = lane % 3, iy = (lane / 3) % 3, iz = lane / 9;
+            const int nx = gx >= 3 ? 3 : gx, ny = gy >= 3 ? 3 : gy, nz = gz >= 3 ? 3 : gz;
+            int lo = 0, len = 0;
+            if (lane < 27 && ix < nx && iy < ny && iz < nz) {
+                const int ox = gx >= 3 ? ix - 1 : ix, oy = gy >= 3 ? iy - 1 : iy, oz = gz >= 3 ? iz - 1 : iz;
+                const int nc = imod(cx + ox, gx) + gx * (imod(cy + oy, gy) + gy * imod(cz + oz, gz));
+                if (nc >= cell) {
+                    lo = nc == cell ? ci : s.cell_nclus[nc];
+                    len = s.cell_nclus[nc + 1] - lo;
+                }
+            }
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const unsigned bseg = __ballot_sync(0xffffffffu, len > 0);
+            if (len > 0) {
+                const int r = __popc(bseg & below);
+                seg_lo[w][r] = lo;
+                seg_pre[w][r] = incl - len;
+            }
+            if (lane == 31) seg_pre[w][__popc(bseg)] = incl;
+            total = __shfl_sync(0xffffffffu, incl, 31);
+        }
+        __syncwarp();
+        uint32_t* outs = s.wl_s + static_cast<size_t>(ci) * P.wcap;
+        uint32_t* outl = s.wl_l + static_cast<size_t>(ci) * P.wcap;
+        int cnt_s = 0, cnt_l = 0, qn = 0, v0 = 0, sg = 0;
+        for (;;) {
+            // sphere tests until 32 survivors are queued or the candidates end
+            while (v0 < total && qn < 32) {
+                while (seg_pre[w][sg + 1] <= v0) ++sg;
+                const int v = v0 + lane;
+                bool surv = false;
+                int jc = 0;
+                if (v < total) {
+                    int g = sg;
+                    while (seg_pre[w][g + 1] <= v) ++g;
+                    jc = min(seg_lo[w][g] + (v - seg_pre[w][g]), nclus - 1);
+                    const float4 gj = geo[jc], hj = ext[jc];
+                    float dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
                     if (P.boundary) {
-                        dx -= P.box[0] * rint(dx * P.inv_box[0]);
-                        dy -= P.box[1] * rint(dy * P.inv_box[1]);
-                        dz -= P.box[2] * rint(dz * P.inv_box[2]);
+                        dx -= P.boxf[0] * rintf(dx * P.inv_boxf[0]);
+                        dy -= P.boxf[1] * rintf(dy * P.inv_boxf[1]);
+                        dz -= P.boxf[2] * rintf(dz * P.inv_boxf[2]);
                     }
-                    fx[threadIdx.x] = float(dx);
-                    fy[threadIdx.x] = float(dy);
-                    fz[threadIdx.x] = float(dz);
-                    r = sqrtf(float(dx) * float(dx) + float(dy) * float(dy) + float(dz) * float(dz));
+                    // gap between the two boxes along each axis
+                    dx = fmaxf(fabsf(dx) - hi.x - hj.x, 0.f);
+                    dy = fmaxf(fabsf(dy) - hi.y - hj.y, 0.f);
+                    dz = fmaxf(fabsf(dz) - hi.z - hj.z, 0.f);
+                    surv = dx * dx + dy * dy + dz * dz <= rcl * rcl;
                 }
+                const unsigned b = __ballot_sync(0xffffffffu, surv);
+                if (surv) q_jc[w][qn + __popc(b & below)] = jc;
+                qn += __popc(b);
+                v0 += 32;
+            }
+            if (qn == 0) break;
+            const int nq = min(qn, 32);
+            __syncwarp();
+            // per survivor: the cluster-to-cluster vector C (FP64 image of the
+            // first atoms, rounded once) and, per member m, C - offset_m
+            if (lane < nq) {
+                const int jc = q_jc[w][lane];
+                const int n_j = s.clus_n[jc];
+                const float span = gi.w + geo[jc].w;
+                float4 o[W];
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, o));
-                if (lane == 0) {
-                    chx[warp] = cx0;
-                    chy[warp] = cy0;
-                    chz[warp] = cz0;
-                    chr[warp] = r * (1.f + 1e-5f) + 1e-5f;
+                for (int m = 0; m < W; ++m) o[m] = soff[jc * W + m];
+                double cdx = X0 - x64[4 * jc], cdy = Y0 - x64[4 * jc + 1], cdz = Z0 - x64[4 * jc + 2];
+                if (P.boundary) {
+                    cdx -= P.box[0] * rint(cdx * P.inv_box[0]);
+                    cdy -= P.box[1] * rint(cdy * P.inv_box[1]);
+                    cdz -= P.box[2] * rint(cdz * P.inv_box[2]);
                 }
-            }
-        }
-        __syncthreads();
-        // advance to the next tile and prefetch it
-        int nic = ic, nt0 = t0 + kTile, nj0 = j0, nj1 = j1;
-        if (nj0 + nt0 >= nj1) {
-            nt0 = 0;
-            ++nic;
-            while (nic < n_nc) {
-                tile_range(nic, nj0, nj1);
-                if (nj1 > nj0) break;
-                ++nic;
-            }
-        }
-        if (nic < n_nc && threadIdx.x < min(kTile, nj1 - (nj0 + nt0))) {
-            const int q = nj0 + nt0 + threadIdx.x;
-            px = s.sref[q];
-            py = s.sref[stride + q];
-            pz = s.sref[2 * stride + q];
-        }
-        // bounding-sphere test of every (cluster, chunk) pair: cluster-to-chunk
-        // vector with the FP64 image, rounded once; survivors are queued with
-        // their vector and a flag for chunks near half a box edge
-        for (int q = threadIdx.x; q < kSearchWarps * nch; q += blockDim.x) {
-            const int c = q / nch, ch = q - c * nch;
-            if (c_n[c] == 0) continue;
-            double cdx = cxs[c][0][0] - chx[ch], cdy = cxs[c][1][0] - chy[ch], cdz = cxs[c][2][0] - chz[ch];
-            if (P.boundary) {
-                cdx -= P.box[0] * rint(cdx * P.inv_box[0]);
-                cdy -= P.box[1] * rint(cdy * P.inv_box[1]);
-                cdz -= P.box[2] * rint(cdz * P.inv_box[2]);
-            }
-            const float Cx = float(cdx), Cy = float(cdy), Cz = float(cdz);
-            const float cd = sqrtf(Cx * Cx + Cy * Cy + Cz * Cz);
-            if (cd - chr[ch] > c_reach[c]) continue;
-            // |C - f| <= |C| + chunk radius, and a pair vector adds at most the
-            // cluster radius: when that stays below half a box edge on every
-            // axis, C - f is the minimum image and every pair is inside the box
-            const float ext = chr[ch] + c_rad[c];
-            const bool edge = P.boundary && !(fabsf(Cx) + ext < limx && fabsf(Cy) + ext < limy &&
-                                              fabsf(Cz) + ext < limz);
-            const int k = atomicAdd(&n_items, 1);
-            atomicOr(&c_surv[c], 1u << ch);
-            it_cc[k] = (c << 8) | (ch << 1) | (edge ? 1 : 0);
-            it_C[k][0] = Cx;
-            it_C[k][1] = Cy;
-            it_C[k][2] = Cz;
-        }
-        __syncthreads();
-        const int items = n_items;
-        for (int it = warp; it < items; it += kSearchWarps) {
-            const int cc = it_cc[it];
-            const int c = cc >> 8, ch = (cc >> 1) & 0x7f;
-            const bool edge = cc & 1;
-            const float Cx = it_C[it][0], Cy = it_C[it][1], Cz = it_C[it][2];
-            const int n = c_n[c], first = c_first[c];
-            const float reach2 = c_reach[c] * c_reach[c];
-            const int t = ch * 32 + lane;
-            const int sp = tbeg + t;
-            unsigned ms = 0, ml = 0, amb = 0;
-            if (t < tn && sp > first) {
-                float Dx = Cx - fx[t], Dy = Cy - fy[t], Dz = Cz - fz[t];
-                if (edge) {  // the sum of two minimum images need not be one
-                    Dx -= P.boxf[0] * rintf(Dx * P.inv_boxf[0]);
-                    Dy -= P.boxf[1] * rintf(Dy * P.inv_boxf[1]);
-                    Dz -= P.boxf[2] * rintf(Dz * P.inv_boxf[2]);
-                }
-                if (Dx * Dx + Dy * Dy + Dz * Dz <= reach2) {
-                    // branch-free classification of the W pairs; pairs inside a
-                    // band around a cutoff or near half a box edge are decided by
-                    // the exact FP64 test; pairs {i_k, j} with k < n and i_k
-                    // before j in sorted order
-                    const int nv = min(n, sp - first);
-                    const unsigned valid = (1u << nv) - 1u;
+                const float Cx = float(cdx), Cy = float(cdy), Cz = float(cdz);
+                // |C + i offset - j offset| per axis stays below |C| + both
+                // radii: when that is below half a box edge, the sum is the
+                // minimum image of every member pair
+                const bool edge = P.boundary && !(fabsf(Cx) + span < limx && fabsf(Cy) + span < limy &&
+                                                  fabsf(Cz) + span < limz);
 #pragma unroll
+                for (int m = 0; m < W; ++m) {
+                    float Dx = Cx - o[m].x, Dy = Cy - o[m].y, Dz = Cz - o[m].z;
+                    if (edge) {  // the sum of two minimum images need not be one
+                        Dx -= P.boxf[0] * rintf(Dx * P.inv_boxf[0]);
+                        Dy -= P.boxf[1] * rintf(Dy * P.inv_boxf[1]);
+                        Dz -= P.boxf[2] * rintf(Dz * P.inv_boxf[2]);
+                    }
+                    const int flags = (m < n_j ? 1 : 0) | (edge ? 2 : 0);
+                    q_d[w][lane * W + m] = make_float4(Dx, Dy, Dz, __int_as_float(flags));
+                }
+            }
+            __syncwarp();
+            for (int p0 = 0; p0 < nq; p0 += kPer) {
+                const int q = p0 + lane / W, m = lane % W;
+                unsigned ms = 0, ml = 0, amb = 0;
+                int jc = 0;
+                if (q < nq) {
+                    jc = q_jc[w][q];
+                    const float4 D = q_d[w][q * W + m];
+                    const int flags = __float_as_int(D.w);
+                    if (flags & 1) {
+                        const bool edge = flags & 2;
+                        // pairs {i_k, j_m} with k < n_i and i_k before j_m in sorted order
+                        unsigned valid = (1u << n_i) - 1u;
+                        if (jc == ci) valid &= (1u << m) - 1u;
+#pragma unroll
+                        for (int k = 0; k < W; ++k) {
+                            const float kx = ex[k] + D.x, ky = ey[k] + D.y, kz = ez[k] + D.z;
+                            const float d2 = kx * kx + ky * ky + kz * kz;
+                            ms |= unsigned(d2 < s_lo) << k;
+                            ml |= unsigned(d2 > s_hi && d2 < l_lo) << k;
+                            amb |= unsigned((d2 >= s_lo && d2 <= s_hi) || (d2 >= l_lo && d2 <= l_hi)) << k;
+                            if (edge) {
+                                const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
+                                amb |= unsigned(!inbox) << k;
+                            }
+                        }
+                        ms &= valid & ~amb;
+                        ml &= valid & ~amb;
+                        amb &= valid;
+                    }
+                }
+                // the rare ambiguous pairs: the exact FP64 decision
+                // (nearest_image_exact + len2_exact, box from the kernel
+                // parameters) for the lanes that have some
+                if (__any_sync(0xffffffffu, amb != 0u) && amb) {
+                    const int sp = s.clus_first[jc] + m;
+                    const double tjx = sref[sp], tjy = sref[stride + sp], tjz = sref[2 * stride + sp];
+#pragma unroll 1
                     for (int k = 0; k < W; ++k) {
-                        const float kx = cex[c][0][k] + Dx, ky = cex[c][1][k] + Dy, kz = cex[c][2][k] + Dz;
-                        const float d2 = kx * kx + ky * ky + kz * kz;
-                        ms |= unsigned(d2 < s_lo) << k;
-                        ml |= unsigned(d2 > s_hi && d2 < l_lo) << k;
-                        amb |= unsigned((d2 >= s_lo && d2 <= s_hi) || (d2 >= l_lo && d2 <= l_hi)) << k;
-                        if (edge) {
-                            const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
-                            amb |= unsigned(!inbox) << k;
+                        if (!((amb >> k) & 1u)) continue;
+                        double rx = __dsub_rn(sref[first_i + k], tjx);
+                        double ry = __dsub_rn(sref[stride + first_i + k], tjy);
+                        double rz = __dsub_rn(sref[2 * stride + first_i + k], tjz);
+                        if (P.boundary) {
+                            rx = image_exact(rx, P.box[0], P.inv_box[0]);
+                            ry = image_exact(ry, P.box[1], P.inv_box[1]);
+                            rz = image_exact(rz, P.box[2], P.inv_box[2]);
+                        }
+                        const double e2 = len2_exact(rx, ry, rz);
+                        if (!(e2 > P.c2l)) {
+                            if (e2 > P.c2s)
+                                ml |= 1u << k;
+                            else
+                                ms |= 1u << k;
                         }
                     }
-                    ms &= valid & ~amb;
-                    ml &= valid & ~amb;
-                    amb &= valid;
                 }
-            }
-            // the rare ambiguous pairs: one warp-uniform test, then the exact
-            // FP64 decision (nearest_image_exact + len2_exact, box from the
-            // kernel parameters) for the lanes that have some
-            if (__any_sync(0xffffffffu, amb != 0u) && amb) {
-#pragma unroll 1
-                for (int k = 0; k < W; ++k) {
-                    if (!((amb >> k) & 1u)) continue;
-                    double rx = __dsub_rn(cxs[c][0][k], tx[t]);
-                    double ry = __dsub_rn(cxs[c][1][k], ty[t]);
-                    double rz = __dsub_rn(cxs[c][2][k], tz[t]);
-                    if (P.boundary) {
-                        rx = image_exact(rx, P.box[0], P.inv_box[0]);
-                        ry = image_exact(ry, P.box[1], P.inv_box[1]);
-                        rz = image_exact(rz, P.box[2], P.inv_box[2]);
-                    }
-                    const double e2 = len2_exact(rx, ry, rz);
-                    if (!(e2 > P.c2l)) {
-                        if (e2 > P.c2s)
-                            ml |= 1u << k;
-                        else
-                            ms |= 1u << k;
-                    }
-                }
-            }
-            res_s[c * kChunks + ch][lane] = static_cast<uint8_t>(ms);
-            res_l[c * kChunks + ch][lane] = static_cast<uint8_t>(ml);
-        }
-        __syncthreads();
-        // each cluster's warp appends its surviving chunks in chunk order
-        if (active) {
-            unsigned surv = c_surv[warp];
-            while (surv) {
-                const int ch = __ffs(surv) - 1;
-                surv &= surv - 1;
-                const unsigned ms = res_s[warp * kChunks + ch][lane], ml = res_l[warp * kChunks + ch][lane];
-                const uint32_t slot = static_cast<uint32_t>(slot0 + (tbeg + ch * 32 + lane - j0));
+                const uint32_t slot = static_cast<uint32_t>(jc * W + m);
                 const unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
                 const unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
                 if (ms) {
                     const int p = cnt_s + __popc(bs & below);
                     const uint32_t ent = (slot << 8) | ms;
                     if (p < kEntBuf)
-                        ebuf_s[warp][p] = ent;
+                        ebuf_s[w][p] = ent;
                     else if (p < P.wcap)
                         outs[p] = ent;
                 }
@@ -673,32 +598,35 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 3) k_water_search(const Sys
                     const int p = cnt_l + __popc(bl & below);
                     const uint32_t ent = (slot << 8) | ml;
                     if (p < kEntBuf)
-                        ebuf_l[warp][p] = ent;
+                        ebuf_l[w][p] = ent;
                     else if (p < P.wcap)
                         outl[p] = ent;
                 }
                 cnt_s += __popc(bs);
                 cnt_l += __popc(bl);
             }
+            // keep the survivors beyond the 32 just classified
+            const int rem = qn - nq;
+            const int keep = lane < rem ? q_jc[w][32 + lane] : 0;
+            __syncwarp();
+            if (lane < rem) q_jc[w][lane] = keep;
+            qn = rem;
+            __syncwarp();
         }
-        ic = nic;
-        t0 = nt0;
-        j0 = nj0;
-        j1 = nj1;
-    }
-    if (!active) return;
-    __syncwarp();
-    if (POPSORT) {
-        sort_write_entries_pop<W>(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
-        sort_write_entries_pop<W>(ebuf_l[warp], min(cnt_l, kEntBuf), outl, lane);
-    } else {
-        sort_write_entries(ebuf_s[warp], min(cnt_s, kEntBuf), outs, lane);
-        sort_write_entries(ebuf_l[warp], min(cnt_l, kEntBuf), outl, lane);
-    }
-    if (lane == 0) {
-        if (cnt_s > P.wcap || cnt_l > P.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
-        s.wn_s[ci] = min(cnt_s, P.wcap);
-        s.wn_l[ci] = min(cnt_l, P.wcap);
+        __syncwarp();
+        if (POPSORT) {
+            sort_write_entries_pop<W>(ebuf_s[w], min(cnt_s, kEntBuf), outs, lane);
+            sort_write_entries_pop<W>(ebuf_l[w], min(cnt_l, kEntBuf), outl, lane);
+        } else {
+            sort_write_entries(ebuf_s[w], min(cnt_s, kEntBuf), outs, lane);
+            sort_write_entries(ebuf_l[w], min(cnt_l, kEntBuf), outl, lane);
+        }
+        if (lane == 0) {
+            if (cnt_s > P.wcap || cnt_l > P.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
+            s.wn_s[ci] = min(cnt_s, P.wcap);
+            s.wn_l[ci] = min(cnt_l, P.wcap);
+        }
+        __syncwarp();  // the entry buffers and queues are reused by the next cluster
     }
 }
 
