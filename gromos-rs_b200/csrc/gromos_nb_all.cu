@@ -7,4 +7,5 @@
 #include "md.cu"
 #include "batch.cu"
 #include "server.cu"
+#include "frames.cu"
 #include "noalloc.cu"

@@ -13,7 +13,9 @@
 //    the cluster's atoms live in registers, i-forces are reduced across lanes;
 //  - k_water_force_it (layout 2, default, W = 4 or 8): each lane iterates over
 //    its own bits; the cluster's atoms are read from shared memory by bit
-//    index and i-forces accumulate in lane-private shared-memory rows.
+//    index and i-forces accumulate in lane-private shared-memory rows; the
+//    virial is assembled from per-atom force sums (j side per entry, i side
+//    per cluster) instead of per pair.
 // The CG-pair image comes from an FP64 difference of first oxygens; FP32
 // arithmetic for the pairs; forces are accumulated in 64-bit fixed point
 // (2^32 per kJ mol^-1 nm^-1) with fire-and-forget reductions.  A CG pair whose
@@ -581,8 +583,9 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                     const float4 p0 = sp[k * 3], p1 = sp[k * 3 + 1], p2 = sp[k * 3 + 2];
                     float pxk[3] = {p0.x, p1.x, p2.x}, pyk[3] = {p0.y, p1.y, p2.y}, pzk[3] = {p0.z, p1.z, p2.z};
                     float r0x = pxk[0] - qx[0], r0y = pyk[0] - qy[0], r0z = pzk[0] - qz[0];
+                    float shx = 0.f, shy = 0.f, shz = 0.f;
+                    bool shifted = false;
                     if (!(fabsf(r0x) < limx && fabsf(r0y) < limy && fabsf(r0z) < limz)) {
-                        float shx = 0.f, shy = 0.f, shz = 0.f;
                         if (wp.boundary) {
                             shx = -wp.boxf[0] * rintf(r0x * wp.inv_boxf[0]);
                             shy = -wp.boxf[1] * rintf(r0y * wp.inv_boxf[1]);
@@ -607,6 +610,7 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                             pyk[a] += shy;
                             pzk[a] += shz;
                         }
+                        shifted = true;
                     }
                     float fx[3] = {0.f, 0.f, 0.f}, fy[3] = {0.f, 0.f, 0.f}, fz[3] = {0.f, 0.f, 0.f};
 #pragma unroll
@@ -635,13 +639,20 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                             gx[b] -= fxx;
                             gy[b] -= fyy;
                             gz[b] -= fzz;
-                            v0s = fmaf(x, fxx, v0s);
-                            v1s = fmaf(x, fyy, v1s);
-                            v2s = fmaf(x, fzz, v2s);
-                            v3s = fmaf(y, fyy, v3s);
-                            v4s = fmaf(y, fzz, v4s);
-                            v5s = fmaf(z, fzz, v5s);
                         }
+                    // virial sum_ab x_ab (x) f_ab = sum_a P_a (x) fi_a + sum_b Q_b (x) g_b
+                    // (P, Q: positions relative to the cluster origin): the
+                    // i-part is taken once per cluster from the column sums of
+                    // the unshifted P; a shifted image adds shift (x) sum_a fi_a
+                    if (shifted) {
+                        const float sx = fx[0] + fx[1] + fx[2], sy = fy[0] + fy[1] + fy[2], sz = fz[0] + fz[1] + fz[2];
+                        v0s = fmaf(shx, sx, v0s);
+                        v1s = fmaf(shx, sy, v1s);
+                        v2s = fmaf(shx, sz, v2s);
+                        v3s = fmaf(shy, sy, v3s);
+                        v4s = fmaf(shy, sz, v4s);
+                        v5s = fmaf(shz, sz, v5s);
+                    }
 #pragma unroll
                     for (int a = 0; a < 3; ++a) {
                         float4 f = myrow[k * 3 + a];
@@ -650,6 +661,16 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                         f.z += fz[a];
                         myrow[k * 3 + a] = f;
                     }
+                }
+                // the j-part of the virial: Q_b (x) g_b, g_b = -sum_a f_ab
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    v0s = fmaf(qx[b], gx[b], v0s);
+                    v1s = fmaf(qx[b], gy[b], v1s);
+                    v2s = fmaf(qx[b], gz[b], v2s);
+                    v3s = fmaf(qy[b], gy[b], v3s);
+                    v4s = fmaf(qy[b], gz[b], v4s);
+                    v5s = fmaf(qz[b], gz[b], v5s);
                 }
                 long long* __restrict__ fj = FS + static_cast<size_t>(js) * 9;
 #pragma unroll
@@ -691,6 +712,14 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                 red_add(fo, to_fixed_f(sx, 4294967296.0f));
                 red_add(fo + 1, to_fixed_f(sy, 4294967296.0f));
                 red_add(fo + 2, to_fixed_f(sz, 4294967296.0f));
+                // the i-part of the virial: P (x) F for this i atom
+                const float4 P = sp[lane];
+                v0s = fmaf(P.x, sx, v0s);
+                v1s = fmaf(P.x, sy, v1s);
+                v2s = fmaf(P.x, sz, v2s);
+                v3s = fmaf(P.y, sy, v3s);
+                v4s = fmaf(P.y, sz, v4s);
+                v5s = fmaf(P.z, sz, v5s);
             }
         }
         __syncwarp();

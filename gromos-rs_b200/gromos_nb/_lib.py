@@ -150,6 +150,7 @@ _SIGNATURES = {
     "gr_batch_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_ctx_device_bytes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrAutotuneResult)]),
+    "gr_energy_frames": (C.c_int32, [C.c_void_p, C.c_int32, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]),
     "gr_server_create": (C.c_int32, [C.c_int, C.c_int64, C.c_int32, C.POINTER(C.c_void_p)]),
     "gr_server_destroy": (C.c_int32, [C.c_void_p]),
     "gr_server_submit": (C.c_int32, [C.c_void_p, C.POINTER(GrJobDesc), C.POINTER(C.c_int64)]),

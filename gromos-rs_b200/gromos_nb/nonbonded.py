@@ -194,6 +194,26 @@ class Forcefield:
             flags |= _lib.GR_EVAL_GRAPH
         check(self._L.gr_forces_eval(self._h, flags, None))
 
+    def energy_frames(self, frames: np.ndarray, boxes: Optional[np.ndarray] = None, groups: bool = False) -> dict:
+        """LJ and CRF energies of every configuration in ``frames`` (n_frames, n_atoms, 3), each with
+        a fresh pairlist (``gr_energy_frames``); ``boxes`` (n_frames, 3) or None for the current box.
+        With ``groups`` the (n_frames, G, G) energy-group matrices are returned too."""
+        n = self.system.topo.n_atoms
+        fr = np.ascontiguousarray(frames, dtype=np.float64).reshape(-1, n, 3)
+        nf = fr.shape[0]
+        bx = None if boxes is None else np.ascontiguousarray(boxes, dtype=np.float64).reshape(nf, 3)
+        e_lj, e_crf = np.zeros(nf), np.zeros(nf)
+        G = int(self.system.topo.n_egroups)
+        glj = np.zeros((nf, G, G)) if groups else None
+        gcrf = np.zeros((nf, G, G)) if groups else None
+        f64 = C.POINTER(C.c_double)
+        ptr = lambda a: None if a is None else a.ctypes.data_as(f64)
+        check(self._L.gr_energy_frames(self._h, nf, ptr(fr), ptr(bx), ptr(e_lj), ptr(e_crf), ptr(glj), ptr(gcrf)))
+        out = {"e_lj": e_lj, "e_crf": e_crf}
+        if groups:
+            out["egroup_lj"], out["egroup_crf"] = glj, gcrf
+        return out
+
     def timings(self) -> List[float]:
         ms = (C.c_float * 5)()
         check(self._L.gr_last_timings(self._h, ms))

@@ -271,6 +271,20 @@ gr_status gr_batch_autotune(gr_batch* b, int32_t periods, gr_autotune_result* ou
 /* Device bytes held by a context (topology, lists, accumulators, MD state). */
 gr_status gr_ctx_device_bytes(gr_ctx* ctx, int64_t* bytes);
 
+/* ---- energies of many configurations (trajectory analysis) ---------------- */
+/* single_point_energy (crates/gromos-forces/src/energy.rs:96-239), nonbonded
+ * part, over n_frames configurations in one call (the frame loop of the ener
+ * tool, crates/gromos-analysis/src/bin/energy/ener.rs:106-124).  frames holds
+ * n_frames x n_atoms x 3 positions; boxes n_frames x 3 edge lengths, or NULL
+ * to keep the context's box.  Each frame gets a fresh pairlist built with the
+ * context's parameters (single_point_energy: rcutp = rcutl = cutoff, skin 0)
+ * and LJ + CRF energies including the RF-excluded and 1-4 terms: e_lj[f],
+ * e_crf[f] and, if non-NULL, egroup_lj / egroup_crf (n_frames x G x G).
+ * Bonded terms are not computed here.  Afterwards the context holds the last
+ * frame's positions. */
+gr_status gr_energy_frames(gr_ctx* ctx, int32_t n_frames, const double* frames, const double* boxes,
+                           double* e_lj, double* e_crf, double* egroup_lj, double* egroup_crf);
+
 /* ---- job server: continuous batching of MD jobs on one GPU ---------------- */
 /* No gromos-rs counterpart (the reference runs one simulation per process).
  * Jobs are submitted with all their inputs (copied: the caller's buffers are

@@ -147,3 +147,22 @@ def test_server_entry_points_without_device():
     assert L.gr_server_submit(None, None, None) == _lib.GR_ERR_INVALID
     assert L.gr_server_release(None, 0) == _lib.GR_ERR_INVALID
     assert L.gr_server_destroy(None) == _lib.GR_OK
+
+
+def test_energy_params_mirror_reference_defaults():
+    """EnergyParams::default (crates/gromos-forces/src/energy.rs:52-66) and the single-cutoff list setup."""
+    from gromos_nb.energy import EnergyParams, SinglePointEnergy, _nonbonded_params
+    p = EnergyParams()
+    assert (p.cutoff, p.epsilon, p.rf_epsilon, p.rf_kappa, p.pairlist_freq, p.atoms_per_solvent) == \
+        (1.4, 1.0, 78.5, 0.0, 1, 3)
+    assert p.ntf == (True, True, True, True) and p.quartic_bonds
+    nb = _nonbonded_params(EnergyParams(cutoff=0.9, rf_epsilon=62.0), np.array([3.0, 3.0, 3.0]))
+    assert (nb.rcutp, nb.rcutl, nb.skin, nb.nsnb, nb.boundary, nb.epsrf) == (0.9, 0.9, 0.0, 1, 1, 62.0)
+    assert _nonbonded_params(EnergyParams(), np.zeros(3)).boundary == 0   # vacuum (energy.rs:108-117)
+    assert SinglePointEnergy().potential == 0.0
+
+
+def test_energy_frames_entry_rejects_null_context():
+    from gromos_nb import _lib
+    L = _lib.lib()
+    assert L.gr_energy_frames(None, 1, None, None, None, None, None, None) == _lib.GR_ERR_INVALID
