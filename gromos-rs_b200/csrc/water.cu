@@ -472,6 +472,12 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
     __shared__ float4 sp_all[kWaterWarps][W * 3];
     __shared__ float4 ibuf[kWaterWarps][2][W * 3];
     __shared__ float4 jbuf[kWaterWarps][2][32 * 3];
+    // long range: a chunk's j forces (fixed point, 9 per lane) and j slots,
+    // so that the reductions go out with consecutive lanes on consecutive
+    // components (fewer L2 sectors per reduction instruction); the short
+    // range, with mostly partial chunks, reduces straight from registers
+    __shared__ long long jst[LONG ? kWaterWarps : 1][LONG ? 32 * 9 : 1];
+    __shared__ int jsl[LONG ? kWaterWarps : 1][32];
     float4* __restrict__ sp = sp_all[wid];
 #pragma unroll
     for (int c = 0; c < W * 3; ++c) myrow[c] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -564,6 +570,7 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
             __syncwarp();
             unsigned mask = e_cur & 0xffu;
             const int js = static_cast<int>(e_cur >> 8);
+            if (LONG) jsl[wid][lane] = mask ? js : -1;
             if (mask) {
                 const float4 r0 = jbuf[wid][jb][3 * lane], r1 = jbuf[wid][jb][3 * lane + 1], r2 = jbuf[wid][jb][3 * lane + 2];
                 double dx = x00 - rec_x(r0), dy = y00 - rec_y(r0), dz = z00 - rec_x(r1);
@@ -672,12 +679,34 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                     v4s = fmaf(qy[b], gz[b], v4s);
                     v5s = fmaf(qz[b], gz[b], v5s);
                 }
-                long long* __restrict__ fj = FS + static_cast<size_t>(js) * 9;
+                if (LONG) {
+                    long long* __restrict__ st = jst[wid] + lane * 9;
 #pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    red_add(fj + 3 * b, to_fixed_f(gx[b], 4294967296.0f));
-                    red_add(fj + 3 * b + 1, to_fixed_f(gy[b], 4294967296.0f));
-                    red_add(fj + 3 * b + 2, to_fixed_f(gz[b], 4294967296.0f));
+                    for (int b = 0; b < 3; ++b) {
+                        st[3 * b] = to_fixed_f(gx[b], 4294967296.0f);
+                        st[3 * b + 1] = to_fixed_f(gy[b], 4294967296.0f);
+                        st[3 * b + 2] = to_fixed_f(gz[b], 4294967296.0f);
+                    }
+                } else {
+                    long long* __restrict__ fj = FS + static_cast<size_t>(js) * 9;
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        red_add(fj + 3 * b, to_fixed_f(gx[b], 4294967296.0f));
+                        red_add(fj + 3 * b + 1, to_fixed_f(gy[b], 4294967296.0f));
+                        red_add(fj + 3 * b + 2, to_fixed_f(gz[b], 4294967296.0f));
+                    }
+                }
+            }
+            if (LONG) {
+                __syncwarp();
+                // element e = 32 r + lane is component e % 9 of lane e / 9's j
+                // water: the 9 components of a j water are contiguous in FS
+#pragma unroll
+                for (int r = 0; r < 9; ++r) {
+                    const int e = r * 32 + lane;
+                    const int src = e / 9;
+                    const int jw = jsl[wid][src];
+                    if (jw >= 0) red_add(FS + static_cast<size_t>(jw) * 9 + (e - 9 * src), jst[wid][e]);
                 }
             }
             e_cur = e_nx;
