@@ -685,9 +685,9 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
         (++launches, k_refpos<<<blocks_for(NCG, 256), 256, 0, s>>>(d_sys, d_cg_key));
         (++launches, k_scan_cells<<<1, 1024, 0, s>>>(d_sys));
         (++launches, k_scatter<<<blocks_for(NCG, 256), 256, 0, s>>>(d_sys, d_cg_key));
-        (++launches, k_cell_sort<<<h.n_cells, 1024, 0, s>>>(d_sys));
+        (++launches, k_cell_sort<<<h.n_cells, 256, 0, s>>>(d_sys));
         (++launches, k_scan_clusters<<<1, 1024, 0, s>>>(d_sys));
-        (++launches, k_cluster_setup<<<blocks_for(h.n_cells, 8), 256, 0, s>>>(d_sys));
+        (++launches, k_cluster_setup<<<h.n_cells, 128, 0, s>>>(d_sys));
         if (NCG > NSCG) {
             SearchParams P;
             for (int k = 0; k < 3; ++k) {
@@ -827,7 +827,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         WaterParams wp;
         if (NCG > NSCG) {
             wp = water_params();
-            (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 64), 64, 0, s>>>(d_sys));
+            (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 64), 64, 0, s>>>(d_sys));
             if ((st = launch_water(s, wp, false))) return st;
         }
         if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
@@ -846,7 +846,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         }
     } else {
         if (NCG > NSCG)  // per-step water data incl. the solvent excluded energies
-            (++launches, k_water_prep<<<blocks_for((long long)h.max_clusters * W, 64), 64, 0, s>>>(d_sys));
+            (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 64), 64, 0, s>>>(d_sys));
         (++launches, k_pos32<<<blocks_for(N, 256), 256, 0, s>>>(d_sys));
         GR_CUDA(cudaMemsetAsync(h.f32, 0, size_t(N) * 3 * sizeof(float), s));
         GR_CUDA(cudaMemsetAsync(h.e64, 0, 16 * sizeof(double), s));

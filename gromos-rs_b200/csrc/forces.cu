@@ -39,10 +39,12 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     // before the record is stored (a store through a descriptor pointer would
     // otherwise make every later field read wait for it).  Solvent molecules
     // are 3-site (checked at upload).
+    // One thread per solvent molecule in atom order (coalesced position
+    // reads); the record goes to the molecule's slot.
     const SysDev& s = sys[blockIdx.y];
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nslots = s.n_clusters[0] * s.W;
-    const int* __restrict__ slot_cg = s.slot_cg;
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nsolv = s.n_cg - s.n_solute_cg;
+    const int* __restrict__ cg_slot = s.cg_slot;
     const double* __restrict__ pos = s.pos;
     const double* __restrict__ charge = s.charge;
     WaterRec* __restrict__ wrec = s.wrec;
@@ -57,10 +59,10 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     const int G = s.n_egroups, gs = s.solvent_group < 0 ? 0 : s.solvent_group;
     double e_excl = 0.0;
     float m = 0.f;
-    if (slot < nslots) {
-        const int cg = slot_cg[slot];
-        if (cg >= 0) {
-            const int a0 = nsa + 3 * (cg - nscg);  // solvent CGs are whole 3-site molecules
+    if (w < nsolv) {
+        const int slot = cg_slot[nscg + w];
+        if (slot >= 0) {
+            const int a0 = nsa + 3 * w;  // solvent CGs are whole 3-site molecules
             double p[9];
 #pragma unroll
             for (int q = 0; q < 9; ++q) p[q] = pos[3 * a0 + q];

@@ -24,7 +24,7 @@ constexpr int kMaxCGAtoms = 8;        // generic (solute) kernel: atoms per CG
 constexpr int kMaxGroups = 16;        // energy groups
 constexpr double kForceScale = 4294967296.0;   // 2^32: force fixed point
 constexpr double kEnergyScale = 16777216.0;    // 2^24: energy / virial fixed point
-constexpr int kMaxCellCGs = 2048;     // bitonic per-cell sort capacity
+constexpr int kMaxCellCGs = 2048;     // per-cell sort capacity (charge groups in one grid cell)
 constexpr int kSearchWarps = 4;       // warps per block of the water search
 
 // Error flags (bitwise OR into SysDev::err[0]).

@@ -12,7 +12,7 @@
 //     d2 > (rcs+skin)^2 -> long range, else short range (strict '>').
 //
 // Stages: k_refpos (reference positions, cell keys) -> k_scan_cells ->
-// k_scatter -> k_cell_sort (bitonic, per cell, deterministic) ->
+// k_scatter -> k_cell_sort (rank sort, per cell, deterministic) ->
 // k_scan_clusters -> k_cluster_setup (solvent i-clusters of W CGs) ->
 // k_water_search (water-water j-lists with W-bit masks) and
 // k_solute_search (per solute CG j-lists with exclusion masks) ->
@@ -142,58 +142,52 @@ __global__ void k_scatter(const SysDev* __restrict__ sys, const unsigned long lo
     s.keys[p] = cg_key[c];
 }
 
-// One block (1024 threads) per cell: bitonic sort of the cell's keys.
-__global__ void k_cell_sort(const SysDev* __restrict__ sys) {
+// One block per cell: rank sort of the cell's keys (keys are unique: they
+// end in the CG index), one barrier; each key is then written at its rank
+// with the sorted CG maps and the sorted FP64 reference positions.
+__global__ void __launch_bounds__(256) k_cell_sort(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
     __shared__ unsigned long long sk[kMaxCellCGs];
-    int cell = blockIdx.x;
-    int start = s.cell_start[cell], n = s.cell_start[cell + 1] - start;
+    __shared__ int nsol;
+    const int cell = blockIdx.x;
+    const int start = s.cell_start[cell], n = s.cell_start[cell + 1] - start;
     if (n > kMaxCellCGs) {
         if (threadIdx.x == 0) atomicOr(&s.err[0], ERR_CELL_TOO_DENSE);
         return;
     }
-    int m = 1;
-    while (m < n) m <<= 1;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) sk[i] = i < n ? s.keys[start + i] : ~0ull;
-    __syncthreads();
-    for (int k = 2; k <= m; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < m; i += blockDim.x) {
-                int ixj = i ^ j;
-                if (ixj > i) {
-                    unsigned long long a = sk[i], b = sk[ixj];
-                    bool up = (i & k) == 0;
-                    if ((a > b) == up) {
-                        sk[i] = b;
-                        sk[ixj] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    __shared__ int nsol;
+    unsigned long long* __restrict__ keys = s.keys;
+    int* __restrict__ sorted_cg = s.sorted_cg;
+    int* __restrict__ cg_spos = s.cg_spos;
+    double* __restrict__ sref = s.sref;
+    const double* __restrict__ ref = s.ref;
+    const int stride = s.n_cg + 2;
     if (threadIdx.x == 0) nsol = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sk[i] = keys[start + i];
     __syncthreads();
     int local = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        unsigned long long key = sk[i];
-        int cg = static_cast<int>(key & 0xffffffffull);
-        s.keys[start + i] = key;
-        s.sorted_cg[start + i] = cg;
-        s.cg_spos[cg] = start + i;
-        const int stride = s.n_cg + 2;
-        s.sref[start + i] = s.ref[3 * cg];
-        s.sref[stride + start + i] = s.ref[3 * cg + 1];
-        s.sref[2 * stride + start + i] = s.ref[3 * cg + 2];
+        const unsigned long long key = sk[i];
+        int rank = 0;
+        int j = 0;
+        for (; j + 4 <= n; j += 4)
+            rank += int(sk[j] < key) + int(sk[j + 1] < key) + int(sk[j + 2] < key) + int(sk[j + 3] < key);
+        for (; j < n; ++j) rank += int(sk[j] < key);
+        const int cg = static_cast<int>(key & 0xffffffffull);
+        const int p = start + rank;
+        const double rx = ref[3 * cg], ry = ref[3 * cg + 1], rz = ref[3 * cg + 2];
+        keys[p] = key;
+        sorted_cg[p] = cg;
+        cg_spos[cg] = p;
+        sref[p] = rx;
+        sref[stride + p] = ry;
+        sref[2 * stride + p] = rz;
         if (((key >> 41) & 1ull) == 0ull) ++local;
     }
-    atomicAdd(&nsol, local);
+    if (local) atomicAdd(&nsol, local);
     __syncthreads();
     if (threadIdx.x == 0) {
         s.cell_nsolute[cell] = nsol;
-        int nsolv = n - nsol;
-        s.cell_nclus[cell] = (nsolv + s.W - 1) / s.W;
+        s.cell_nclus[cell] = (n - nsol + s.W - 1) / s.W;
     }
 }
 
@@ -212,62 +206,82 @@ __global__ void k_scan_clusters(const SysDev* __restrict__ sys) {
     }
 }
 
-// One warp per cell: write the cluster records and the slot <-> CG maps.
-__global__ void k_cluster_setup(const SysDev* __restrict__ sys) {
+// One block per cell, one thread per slot of the cell's clusters (the W
+// slots of a cluster are W consecutive lanes): the slot <-> CG maps, the
+// member offsets from the cluster's first atom and, reduced over the
+// cluster's lanes, its record and search geometry (FP64 first atom, bounding
+// box of the first atoms, radius of the offsets).
+__global__ void __launch_bounds__(256) k_cluster_setup(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
-    int cell = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    if (cell >= s.n_cells) return;
-    int c0 = s.cell_nclus[cell], c1 = s.cell_nclus[cell + 1];
-    int first_solv = s.cell_start[cell] + s.cell_nsolute[cell];
-    int nsolv = s.cell_start[cell + 1] - first_solv;
-    for (int k = c0 + lane; k < c1; k += 32) {
-        if (k >= s.max_clusters) break;
-        int local = k - c0;
-        int first = first_solv + local * s.W;
-        int n = min(s.W, nsolv - local * s.W);
-        s.clus_cell[k] = cell;
-        s.clus_first[k] = first;
-        s.clus_n[k] = n;
-        // search geometry: FP64 first atom, FP32 member offsets from it (one
-        // rounding of the FP64 difference), radius bounding the offsets
-        const int stride = s.n_cg + 2;
-        const double x0 = s.sref[first], y0 = s.sref[stride + first], z0 = s.sref[2 * stride + first];
-        float rad = 0.f;
-        for (int m = 0; m < s.W; ++m) {
-            int slot = k * s.W + m;
-            float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (m < n) {
-                int cg = s.sorted_cg[first + m];
-                s.slot_cg[slot] = cg;
-                s.cg_slot[cg] = slot;
-                o.x = float(s.sref[first + m] - x0);
-                o.y = float(s.sref[stride + first + m] - y0);
-                o.z = float(s.sref[2 * stride + first + m] - z0);
-                rad = fmaxf(rad, sqrtf(o.x * o.x + o.y * o.y + o.z * o.z));
-            } else {
-                s.slot_cg[slot] = -1;
-            }
-            s.slot_off[slot] = o;
+    const int cell = blockIdx.x;
+    const int W = s.W;  // 4 or 8: a cluster's lanes are an aligned group
+    const int c0 = s.cell_nclus[cell], c1 = s.cell_nclus[cell + 1];
+    const int first_solv = s.cell_start[cell] + s.cell_nsolute[cell];
+    const int nsolv = s.cell_start[cell + 1] - first_solv;
+    const int max_clusters = s.max_clusters;
+    const int stride = s.n_cg + 2;
+    const double* __restrict__ sref = s.sref;
+    const int* __restrict__ sorted_cg = s.sorted_cg;
+    const int nslots = (c1 - c0) * W;
+    for (int base = 0; base < nslots; base += blockDim.x) {  // block-uniform trip count
+        const int t = base + threadIdx.x;
+        const int local = t / W, m = t - local * W;
+        const int k = c0 + local;
+        const bool live = t < nslots && k < max_clusters;
+        const int first = first_solv + local * W;
+        const int n = live ? min(W, nsolv - local * W) : 0;
+        double x = 0.0, y = 0.0, z = 0.0;
+        int cg = -1;
+        if (m < n) {
+            cg = sorted_cg[first + m];
+            x = sref[first + m];
+            y = sref[stride + first + m];
+            z = sref[2 * stride + first + m];
         }
-        s.clus_x64[4 * k] = x0;
-        s.clus_x64[4 * k + 1] = y0;
-        s.clus_x64[4 * k + 2] = z0;
-        s.clus_x64[4 * k + 3] = 0.0;
-        // axis-aligned bounding box of the first atoms (FP64, then FP32 centre
-        // and slightly widened half extents)
-        double lo[3] = {x0, y0, z0}, hi[3] = {x0, y0, z0};
-        for (int m = 1; m < n; ++m)
-            for (int d = 0; d < 3; ++d) {
-                const double v = s.sref[d * stride + first + m];
-                lo[d] = fmin(lo[d], v);
-                hi[d] = fmax(hi[d], v);
+        // the group's first atom (lane m = 0 of the group)
+        const int g0 = (threadIdx.x & 31) & ~(W - 1);
+        const double x0 = __shfl_sync(0xffffffffu, x, g0), y0 = __shfl_sync(0xffffffffu, y, g0);
+        const double z0 = __shfl_sync(0xffffffffu, z, g0);
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+        double lx = x0, ly = y0, lz = z0, hx = x0, hy = y0, hz = z0;
+        if (m < n) {
+            o.x = float(x - x0);
+            o.y = float(y - y0);
+            o.z = float(z - z0);
+            lx = hx = x;
+            ly = hy = y;
+            lz = hz = z;
+        }
+        float rad = sqrtf(o.x * o.x + o.y * o.y + o.z * o.z);
+        for (int d = 1; d < W; d <<= 1) {
+            rad = fmaxf(rad, __shfl_xor_sync(0xffffffffu, rad, d));
+            lx = fmin(lx, __shfl_xor_sync(0xffffffffu, lx, d));
+            ly = fmin(ly, __shfl_xor_sync(0xffffffffu, ly, d));
+            lz = fmin(lz, __shfl_xor_sync(0xffffffffu, lz, d));
+            hx = fmax(hx, __shfl_xor_sync(0xffffffffu, hx, d));
+            hy = fmax(hy, __shfl_xor_sync(0xffffffffu, hy, d));
+            hz = fmax(hz, __shfl_xor_sync(0xffffffffu, hz, d));
+        }
+        if (live) {
+            const int slot = k * W + m;
+            s.slot_cg[slot] = cg;
+            if (cg >= 0) s.cg_slot[cg] = slot;
+            s.slot_off[slot] = o;
+            if (m == 0) {
+                s.clus_cell[k] = cell;
+                s.clus_first[k] = first;
+                s.clus_n[k] = n;
+                s.clus_x64[4 * k] = x0;
+                s.clus_x64[4 * k + 1] = y0;
+                s.clus_x64[4 * k + 2] = z0;
+                s.clus_x64[4 * k + 3] = 0.0;
+                s.clus_geo[k] = make_float4(float(0.5 * (lx + hx)), float(0.5 * (ly + hy)), float(0.5 * (lz + hz)),
+                                            rad * (1.f + 1e-5f) + 1e-5f);
+                s.clus_ext[k] = make_float4(float(0.5 * (hx - lx)) * (1.f + 1e-6f) + 1e-6f,
+                                            float(0.5 * (hy - ly)) * (1.f + 1e-6f) + 1e-6f,
+                                            float(0.5 * (hz - lz)) * (1.f + 1e-6f) + 1e-6f, 0.f);
             }
-        s.clus_geo[k] = make_float4(float(0.5 * (lo[0] + hi[0])), float(0.5 * (lo[1] + hi[1])),
-                                    float(0.5 * (lo[2] + hi[2])), rad * (1.f + 1e-5f) + 1e-5f);
-        s.clus_ext[k] = make_float4(float(0.5 * (hi[0] - lo[0])) * (1.f + 1e-6f) + 1e-6f,
-                                    float(0.5 * (hi[1] - lo[1])) * (1.f + 1e-6f) + 1e-6f,
-                                    float(0.5 * (hi[2] - lo[2])) * (1.f + 1e-6f) + 1e-6f, 0.f);
+        }
     }
 }
 
