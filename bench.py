@@ -183,7 +183,10 @@ def run_md(ff, s, args, generators):
     mass = generators.masses(s)
     vel = generators.maxwell_velocities(mass, 300.0, seed=2002)
     ff.upload_positions(s.pos)
-    ff.md_init(mass, vel, dt=DT_PS, settle=True, dist_oh=0.1, dist_hh=generators.SPC_DHH)
+    # Berendsen bath at 300 K (tau 0.1 ps): the synthetic start releases potential
+    # energy and would heat an NVE run far above 300 K
+    ff.md_init(mass, vel, dt=DT_PS, settle=True, dist_oh=0.1, dist_hh=generators.SPC_DHH, temperature=300.0,
+               tau=0.1)
     ff.md_run(max(args.warmup, 3) * 5)
     n = max(args.md_steps, 1)
     stream = torch.cuda.ExternalStream(ff.stream())
@@ -197,7 +200,12 @@ def run_md(ff, s, args, generators):
     ms = e0.elapsed_time(e1)
     return {"steps": n, "dt_ps": DT_PS, "ms_per_step": ms / n, "ns_per_day": ns_per_day(ms / n),
             "settle": True, "settle_failures": st["settle_failures"], "rollbacks": st["rollbacks"],
-            "e_kin_final": st["e_kin"], "start": "seeded Maxwell-Boltzmann velocities at 300 K"}
+            "e_kin_final": st["e_kin"],
+            # degrees of freedom as the bath counts them: 3N minus 3 SETTLE constraints per water
+            "t_final_k": 2.0 * st["e_kin"] / ((3 * s.topo.n_atoms - (s.topo.n_atoms - s.topo.n_solute_atoms))
+                                              * generators.BOLTZ),
+            "thermostat": "Berendsen 300 K, tau 0.1 ps",
+            "start": "seeded Maxwell-Boltzmann velocities at 300 K"}
 
 
 def run_gpu(args, rank, world, local_rank):

@@ -150,30 +150,42 @@ def box_for_waters(n_waters: int, density: float = 33.4) -> float:
 def solvated_solute_system(n_waters: int, n_solute_atoms: int, seed: int, rc: float = 1.4, epsrf: float = 61.0,
                            nsnb: int = 5, box: Optional[float] = None, perturbed: bool = False,
                            alpha_lj: float = 0.5, alpha_crf: float = 0.5, lam: float = 0.0,
-                           name: str = "") -> System:
+                           name: str = "", single_atom_cgs: bool = False) -> System:
     """A water box of ``n_waters`` SPC with a seeded ``n_solute_atoms`` solute.
 
-    The solute is built of CGs of 3-5 atoms; with ``perturbed`` every solute
-    atom gets independent state-A/B charges and C6/C12 (drawn as above) and
-    soft-core alphas.  Returned atom order: solute first, then waters.
+    The solute is built of CGs of 3-5 atoms (neutral CGs); with
+    ``single_atom_cgs`` every solute atom is its own CG (LJ ions with seeded
+    partial charges, neutral as a whole).  This library has no bonded terms,
+    so the atoms of a multi-atom CG are free to drift apart: over a few
+    hundred MD steps a CG spreads beyond what its centre-based cutoff test
+    covers and the run fails; single-atom CGs keep long MD runs stable.
+    With ``perturbed`` every solute atom gets independent state-A/B charges
+    and C6/C12 (drawn as above) and soft-core alphas.  Returned atom order:
+    solute first, then waters.
     """
     rng = np.random.default_rng(seed)
     if box is None:
         box = box_for_waters(n_waters + n_solute_atoms // 3)
-    # solute CG sizes: 3-5 atoms each
-    if n_solute_atoms < 3:
-        raise ValueError("a solute needs at least 3 atoms")
-    sizes = []
-    left = n_solute_atoms
-    while left >= 6:
-        s = int(rng.integers(3, 6))
-        if left - s < 3:
-            s = left - 3
-        sizes.append(s)
-        left -= s
-    sizes.append(left)
+    if single_atom_cgs:
+        if n_solute_atoms < 1:
+            raise ValueError("a solute needs at least 1 atom")
+        sizes = [1] * n_solute_atoms
+    else:
+        # solute CG sizes: 3-5 atoms each
+        if n_solute_atoms < 3:
+            raise ValueError("a solute needs at least 3 atoms")
+        sizes = []
+        left = n_solute_atoms
+        while left >= 6:
+            s = int(rng.integers(3, 6))
+            if left - s < 3:
+                s = left - 3
+            sizes.append(s)
+            left -= s
+        sizes.append(left)
     ncg = len(sizes)
-    # CG centres near the box centre, at least 0.55 nm apart as periodic
+    min_sep = 0.35 if single_atom_cgs else 0.55
+    # CG centres near the box centre, at least min_sep apart as periodic
     # minimum images (seeded rejection), so atoms of different CGs stay
     # >= 0.25 nm apart; the box grows when the solute does not fit
     spread = max(0.35, 0.42 * ncg ** (1.0 / 3.0))
@@ -189,7 +201,7 @@ def solvated_solute_system(n_waters: int, n_solute_atoms: int, seed: int, rc: fl
 
     while len(cg_centres) < ncg:
         c = box / 2 + rng.uniform(-min(spread, box / 2), min(spread, box / 2), size=3)
-        if min_dist(c) >= 0.55:
+        if min_dist(c) >= min_sep:
             cg_centres.append(c)
         tries += 1
         if tries > 200 * ncg:
@@ -199,12 +211,15 @@ def solvated_solute_system(n_waters: int, n_solute_atoms: int, seed: int, rc: fl
             spread *= 1.1
             tries = 0
     cg_centres = np.asarray(cg_centres)
-    sol_pos = []
-    for c, s in zip(cg_centres, sizes):
-        d = rng.normal(size=(s, 3))
-        d /= np.linalg.norm(d, axis=1, keepdims=True)
-        sol_pos.append(c + d * rng.uniform(0.05, 0.15, size=(s, 1)))
-    sol_pos = np.concatenate(sol_pos)
+    if single_atom_cgs:  # an atom at its centre: solute atoms stay >= min_sep apart
+        sol_pos = cg_centres.copy()
+    else:
+        sol_pos = []
+        for c, s in zip(cg_centres, sizes):
+            d = rng.normal(size=(s, 3))
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            sol_pos.append(c + d * rng.uniform(0.05, 0.15, size=(s, 1)))
+        sol_pos = np.concatenate(sol_pos)
     # waters: fill the box at liquid density, carve a cavity around the solute,
     # grow the box (seeded, 2% steps) until n_waters remain, keep a seeded subset
     from scipy.spatial import cKDTree
@@ -232,8 +247,11 @@ def solvated_solute_system(n_waters: int, n_solute_atoms: int, seed: int, rc: fl
 
     qa, f6a, f12a = draw_params(nsa)
     off = np.concatenate([[0], np.cumsum(sizes)])
-    for c in range(ncg):
-        qa[off[c]:off[c + 1]] -= qa[off[c]:off[c + 1]].mean()
+    if single_atom_cgs:
+        qa -= qa.mean()
+    else:
+        for c in range(ncg):
+            qa[off[c]:off[c + 1]] -= qa[off[c]:off[c + 1]].mean()
     # atom types: 0 = SPC O, 1 = H, 2.. = one type per solute atom (state A), then state B types
     ntypes = 2 + nsa * (2 if perturbed else 1)
     c6_of = np.zeros(ntypes)
@@ -243,8 +261,11 @@ def solvated_solute_system(n_waters: int, n_solute_atoms: int, seed: int, rc: fl
     c12_of[2:2 + nsa] = SPC_C12 * f12a
     if perturbed:
         qb, f6b, f12b = draw_params(nsa)
-        for c in range(ncg):
-            qb[off[c]:off[c + 1]] -= qb[off[c]:off[c + 1]].mean()
+        if single_atom_cgs:
+            qb -= qb.mean()
+        else:
+            for c in range(ncg):
+                qb[off[c]:off[c + 1]] -= qb[off[c]:off[c + 1]].mean()
         c6_of[2 + nsa:] = SPC_C6 * f6b
         c12_of[2 + nsa:] = SPC_C12 * f12b
     lj = np.zeros((ntypes, ntypes, 4))

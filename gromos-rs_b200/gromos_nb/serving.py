@@ -45,6 +45,8 @@ class Job:
     mass: np.ndarray
     vel: np.ndarray
     dt: float = 0.002
+    temperature: float = 300.0        # Berendsen bath (K)
+    tau: float = 0.1                  # bath coupling time (ps); < 0 runs NVE
     arrival: float = 0.0              # seconds since the server started
     # filled in by the server
     admitted: Optional[float] = None
@@ -105,7 +107,8 @@ class Server:
                 nsnb = max(1, job.system.params.nsnb)
                 job.pairs_per_step = r["n_pairs_short"] + r["n_pairs_long"] / nsnb
                 ff.upload_positions(job.system.pos)
-            ff.md_init(job.mass, job.vel, dt=job.dt, settle=True, dist_oh=0.1, dist_hh=generators.SPC_DHH)
+            ff.md_init(job.mass, job.vel, dt=job.dt, settle=True, dist_oh=0.1, dist_hh=generators.SPC_DHH,
+                       temperature=job.temperature, tau=job.tau)
             nbytes = ff.device_bytes()
             self.bytes_per_atom = max(self.bytes_per_atom if self.resident or self.done else 0.0,
                                       nbytes / max(1, job.system.topo.n_atoms))
@@ -192,9 +195,14 @@ class Server:
 
 def poisson_jobs(n_jobs: int, rate: float, seed: int, waters=(300, 20000), steps=(100, 2000),
                  solute_prob: float = 0.5, solute_atoms=(50, 500), rc: float = 1.4, nsnb: int = 5,
-                 T: float = 300.0) -> List[Job]:
+                 T: float = 300.0, tau: float = 0.1) -> List[Job]:
     """Seeded Poisson arrival stream of MD jobs: uniform water counts and
-    lengths, an optional seeded solute (as in the batched REMD replicas)."""
+    lengths, an optional seeded solute (as in the batched REMD replicas),
+    each coupled to a Berendsen bath at ``T`` with coupling time ``tau`` ps
+    (the synthetic starting structures release potential energy; without a
+    bath a job heats far above ``T`` within a picosecond).  The solutes are
+    single-atom charge groups, which stay consistent with the charge-group
+    cutoff over the jobs' up to 2,000 steps (see solvated_solute_system)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     jobs = []
@@ -204,14 +212,14 @@ def poisson_jobs(n_jobs: int, rate: float, seed: int, waters=(300, 20000), steps
         ns = int(rng.integers(solute_atoms[0], solute_atoms[1] + 1)) if rng.random() < solute_prob else 0
         sseed = seed * 1000 + k
         if ns >= 3:
-            s = generators.solvated_solute_system(nw, ns, seed=sseed, rc=rc, nsnb=nsnb)
+            s = generators.solvated_solute_system(nw, ns, seed=sseed, rc=rc, nsnb=nsnb, single_atom_cgs=True)
         else:
             s = generators.spc_water_system(nw, box=generators.box_for_waters(nw), seed=sseed, rcutp=rc,
                                             rcutl=rc, nsnb=nsnb)
         m = generators.masses(s)
         v = generators.maxwell_velocities(m, T, sseed + 7)
         jobs.append(Job(job_id=k, system=s, n_steps=int(rng.integers(steps[0], steps[1] + 1)), mass=m, vel=v,
-                        arrival=t))
+                        temperature=T, tau=tau, arrival=t))
     return jobs
 
 
@@ -231,7 +239,7 @@ class NativeServer:
         self.ids: Dict[int, int] = {}       # Job.job_id -> server job id
         self.jobs: Dict[int, Job] = {}
 
-    def submit(self, job: Job, tau: float = -1.0, temperature: float = 300.0, params=None) -> int:
+    def submit(self, job: Job, params=None) -> int:
         """Queue ``job``; ``params`` overrides the system's nonbonded parameters (a gr_nb_params)."""
         s = job.system
         topo = _TopologyStruct(s.topo)
@@ -240,7 +248,7 @@ class NativeServer:
         pos = np.ascontiguousarray(s.pos, dtype=np.float64)
         mass = np.ascontiguousarray(job.mass, dtype=np.float64)
         vel = np.ascontiguousarray(job.vel, dtype=np.float64)
-        md = _lib.GrMdParams(job.dt, 1, 0.1, generators.SPC_DHH, temperature, tau)
+        md = _lib.GrMdParams(job.dt, 1, 0.1, generators.SPC_DHH, job.temperature, job.tau)
         f64 = C.POINTER(C.c_double)
         desc = _lib.GrJobDesc(C.pointer(topo.struct), C.pointer(params), box.ctypes.data_as(f64),
                               pos.ctypes.data_as(f64), mass.ctypes.data_as(f64), vel.ctypes.data_as(f64),

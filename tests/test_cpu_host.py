@@ -166,3 +166,19 @@ def test_energy_frames_entry_rejects_null_context():
     from gromos_nb import _lib
     L = _lib.lib()
     assert L.gr_energy_frames(None, 1, None, None, None, None, None, None) == _lib.GR_ERR_INVALID
+
+
+def test_single_atom_solute_generator():
+    """Serving jobs use single-atom solute CGs: neutral, at least 0.35 nm apart; the default keeps 3-5 atom CGs."""
+    from gromos_nb import generators as gen
+    s = gen.solvated_solute_system(400, 60, seed=11, single_atom_cgs=True)
+    t = s.topo
+    assert t.n_solute_cg == t.n_solute_atoms == 60
+    assert abs(t.charge[:60].sum()) < 1e-12 and np.abs(t.charge[:60]).max() > 0.1
+    d = s.pos[:60, None, :] - s.pos[None, :60, :]
+    d -= s.box * np.round(d / s.box)
+    r = np.sqrt((d * d).sum(-1)) + np.eye(60) * 9
+    assert r.min() >= 0.35 - 1e-9
+    m = gen.solvated_solute_system(400, 60, seed=11)
+    sizes = np.diff(m.topo.cg_offsets[:m.topo.n_solute_cg + 1])
+    assert sizes.min() >= 3 and sizes.max() <= 5

@@ -16,7 +16,8 @@ pytestmark = pytest.mark.gpu
 def standalone(job):
     ff = Forcefield(job.system)
     ff.upload_positions(job.system.pos)
-    ff.md_init(job.mass, job.vel, dt=job.dt, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    ff.md_init(job.mass, job.vel, dt=job.dt, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH,
+               temperature=job.temperature, tau=job.tau)
     ff.md_run(job.n_steps)
     x, v = ff.md_state()
     ff.close()
