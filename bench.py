@@ -42,7 +42,7 @@ WORKLOAD = "spc30000_twinrange_0.8_1.4_nsnb5"
 # DRAM bytes (read + write) of one short-range water-kernel launch on this
 # workload, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum;
 # profiles/water_force_it_spc30000_short.md)
-SHORT_KERNEL_DRAM_BYTES = 6.75e6
+SHORT_KERNEL_DRAM_BYTES = 6.951424e6
 
 
 def ns_per_day(ms_per_step: float) -> float:
@@ -310,7 +310,7 @@ def run_gpu(args, rank, world, local_rank):
                           "parallelism": "replicas" if world > 1 else "single system"},
                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "roofline": {"bound": "fp32",
-                            "kernel": "short-range window: k_water_prep + k_water_force_it + k_water_deferred",
+                            "kernel": "short-range window: k_water_prep + k_water_force_it (deferred pairs in its last block)",
                             "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s (FP32 pipe)",
                             "frac": achieved / peak, "traffic": SHORT_KERNEL_DRAM_BYTES,
                             "peak_source": "measured FFMA-chain kernel (gr_ffma_peak), one FFMA = one op",
