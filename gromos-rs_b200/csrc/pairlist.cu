@@ -365,8 +365,9 @@ __device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ 
     }
 }
 
-// Stable counting sort of a cluster's entries by popcount of the mask (lanes of
-// a warp chunk then iterate over the same number of bits).
+// Stable counting sort of a cluster's entries by popcount of the mask, most
+// bits first: lanes of a warp chunk then iterate over the same number of bits,
+// and the last, partly filled chunk holds the cheapest entries.
 template <int W>
 __device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restrict__ buf, int nbuf,
                                                        uint32_t* __restrict__ out, int lane) {
@@ -380,9 +381,9 @@ __device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restric
 #pragma unroll
         for (int v = 1; v <= W; ++v) hist[v] += __popc(__ballot_sync(0xffffffffu, m == v));
     }
-    off[0] = 0;
+    off[W] = 0;
 #pragma unroll
-    for (int v = 1; v <= W; ++v) off[v] = off[v - 1] + hist[v - 1];
+    for (int v = W - 1; v >= 0; --v) off[v] = off[v + 1] + hist[v + 1];
     const unsigned lt = (1u << lane) - 1u;
     for (int c = 0; c < nbuf; c += 32) {
         const int e = c + lane;
