@@ -106,6 +106,11 @@ void NbSystem::release() {
     drop_graphs();
     if (err_step_host) cudaFreeHost(err_step_host);
     err_step_host = nullptr;
+    if (err_dl_host) cudaFreeHost(err_dl_host);
+    err_dl_host = nullptr;
+    if (e_dl_host) cudaFreeHost(e_dl_host);
+    e_dl_host = nullptr;
+    e_dl_n = 0;
     if (ev_step) cudaEventDestroy(ev_step);
     ev_step = nullptr;
     step_check = false;
@@ -1126,11 +1131,23 @@ gr_status NbSystem::pair_counts(cudaStream_t s, long long* n_short, long long* n
     return GR_OK;
 }
 
+// Energies, the error flags and (if requested) the forces are copied in
+// stream order -- the flags and energies into pinned buffers -- and read
+// after one synchronisation.
 gr_status NbSystem::download(cudaStream_t s, gr_result* out) {
     if (!out) return GR_OK;
     const int NA = acc_size(G);
-    std::vector<double> e(NA);
-    GR_CUDA(cudaMemcpyAsync(e.data(), h.e_out, NA * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (e_dl_n < NA) {
+        if (e_dl_host) cudaFreeHost(e_dl_host);
+        e_dl_host = nullptr;
+        e_dl_n = 0;
+        GR_CUDA(cudaMallocHost(&e_dl_host, size_t(NA) * sizeof(double)));
+        e_dl_n = NA;
+    }
+    if (!err_dl_host) GR_CUDA(cudaMallocHost(&err_dl_host, 4 * sizeof(int)));
+    const double* e = e_dl_host;
+    GR_CUDA(cudaMemcpyAsync(e_dl_host, h.e_out, NA * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GR_CUDA(cudaMemcpyAsync(err_dl_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (out->forces)
         GR_CUDA(cudaMemcpyAsync(out->forces, h.f_out, size_t(N) * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     GR_CUDA(cudaStreamSynchronize(s));
@@ -1417,12 +1434,10 @@ gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out) {
         if (st) return st;
         if (!download) return GR_OK;  // overflow (if any) is reported by the next call
         if ((st = S.download(ctx->stream, out))) return st;
-        S.step_check = false;  // the flags are checked here, synchronously
-        int errs[4] = {0, 0, 0, 0};
-        if (cudaMemcpy(errs, S.h.err, sizeof(errs), cudaMemcpyDeviceToHost) == cudaSuccess &&
-            (errs[0] & gnb::ERR_DEFER_OVERFLOW)) {
+        S.step_check = false;  // the flags are checked here, read with the download
+        if (S.err_dl_host[0] & gnb::ERR_DEFER_OVERFLOW) {
             // grow the deferred-pair list and redo this evaluation (long range too)
-            cudaMemset(S.h.err, 0, sizeof(errs));
+            cudaMemset(S.h.err, 0, 4 * sizeof(int));
             if (attempt >= 8) {
                 set_error("water kernel: deferred-pair list could not be grown far enough");
                 return GR_ERR_OVERFLOW;

@@ -95,6 +95,9 @@ class NbSystem {
     long long g_step_launches[2] = {0, 0};
     long long g_gen = -1;
     int* err_step_host = nullptr;  // pinned: device error flags after the last graph step
+    int* err_dl_host = nullptr;    // pinned: device error flags read with the last download
+    double* e_dl_host = nullptr;   // pinned: energies / virial of the last download
+    int e_dl_n = 0;
     cudaEvent_t ev_step = nullptr;
     bool step_check = false;
     bool in_capture = false;  // recording a CUDA graph: the device descriptor is already current
