@@ -493,6 +493,7 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
         return __shfl_sync(0xffffffffu, c, 0);
     };
     int ci = fetch();
+    int n_cur = ci < nclus ? clus_n[ci] : 0;
     int ib = 0, jb = 0;
     int cnt = 0;
     uint32_t e_cur = 0u, e_nx = 0u;
@@ -511,19 +512,28 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
     cp_async_commit();
 
     while (ci < nclus) {
-        const int n = clus_n[ci];
+        const int n = n_cur;
         const int base = ci * W;
         const uint32_t* __restrict__ list = wl + static_cast<size_t>(ci) * wcap;
-        // the next cluster: index now, list head in flight during this cluster
-        const int cn = fetch();
-        int cnt_n = 0;
+        const int nch = (cnt + 31) >> 5;
+        // the next cluster: asked for now, its index, size and list head read
+        // at chunk max(nch - 2, 0), one chunk before they are needed
+        int cn_raw = 0;
+        if (lane == 0) cn_raw = atomicAdd(ctr, 1);
+        int cn = nclus, cnt_n = 0, n_next = 0;
         uint32_t raw0 = 0u, raw1 = 0u;
-        if (cn < nclus) {
-            cnt_n = wn[cn];
-            const uint32_t* __restrict__ ln = wl + static_cast<size_t>(cn) * wcap;
-            raw0 = __ldg(ln + lane);
-            if (32 + lane < wcap) raw1 = __ldg(ln + 32 + lane);
-        }
+        const int c_take = nch >= 2 ? nch - 2 : 0;
+        auto take_next = [&]() {
+            cn = __shfl_sync(0xffffffffu, cn_raw, 0);
+            if (cn < nclus) {
+                cnt_n = wn[cn];
+                n_next = clus_n[cn];
+                const uint32_t* __restrict__ ln = wl + static_cast<size_t>(cn) * wcap;
+                raw0 = __ldg(ln + lane);
+                if (32 + lane < wcap) raw1 = __ldg(ln + 32 + lane);
+            }
+        };
+        if (nch == 0) take_next();
         cp_async_wait<0>();
         __syncwarp();
         const double x00 = rec_x(ibuf[wid][ib][0]), y00 = rec_y(ibuf[wid][ib][0]);
@@ -543,9 +553,9 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
             sp[lane] = p;
         }
         float elj = 0.f, ecrf = 0.f, v0s = 0.f, v1s = 0.f, v2s = 0.f, v3s = 0.f, v4s = 0.f, v5s = 0.f;
-        const int nch = (cnt + 31) >> 5;
         uint32_t e_cur_n = 0u, e_nx_n = 0u;
         for (int c = 0; c < nch; ++c) {
+            if (c == c_take) take_next();
             if (c + 1 < nch) {
                 if (e_nx & 0xffu) {
                     const int js = static_cast<int>(e_nx >> 8);
@@ -764,6 +774,7 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
         acc[7] += to_fixed_f(v5s, 16777216.0f);
         ib ^= 1;
         ci = cn;
+        n_cur = n_next;
         cnt = cnt_n;
         e_cur = e_cur_n;
         e_nx = e_nx_n;
