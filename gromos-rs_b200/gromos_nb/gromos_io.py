@@ -1,7 +1,10 @@
-"""Readers for the GROMOS file subset the nonbonded path needs.
+"""Readers and writers for the GROMOS file subset the nonbonded path needs.
 
 Topology (.topo/.top), configuration (.conf/.cnf), input parameters (.in/.imd)
-and perturbation topology (.ptp).  The topology is assembled the way
+and perturbation topology (.ptp) are read; energy (.tre, ENERTRJ) and force
+(.trf, FREEFORCERED) trajectories are read and written in the layout of
+gromos-rs's EnergyWriter / ForceWriter, so trajectories of the device MD can be
+diffed against the reference's output.  The topology is assembled the way
 gromos-rs's ``build_topology`` + ``Topology::solvate`` do it
 (crates/gromos-io/src/topology.rs:1040-1298, crates/gromos-core/src/topology.rs:1204-1262):
 
@@ -15,8 +18,10 @@ gromos-rs's ``build_topology`` + ``Topology::solvate`` do it
 """
 from __future__ import annotations
 
+import dataclasses
+import math
 import re
-from typing import Dict, List, Optional, Tuple
+from typing import Dict, List, Optional, TextIO, Tuple
 
 import numpy as np
 
@@ -355,3 +360,162 @@ def read_forces_step(path: str, step: int = 0) -> np.ndarray:
             return np.asarray(rows)
         i += 1
     raise KeyError(f"step {step} not found in {path}")
+
+
+
+# ---- trajectory writers ------------------------------------------------------
+#
+# Number formats follow the Rust formatting the reference's writers use:
+# ``{:20.12e}`` (mantissa with 12 decimals, exponent without sign padding:
+# ``1.234560000000e2``, ``-1.000000000000e-3``) for energies and ``{:>18.9}``
+# / ``{:>15.9}`` fixed-point fields for forces and times.
+
+
+def rust_exp(x: float, prec: int = 12, width: int = 20) -> str:
+    """``format!("{:width.prec e}", x)`` as Rust prints an f64."""
+    x = float(x)
+    if math.isnan(x):
+        t = "NaN"
+    elif math.isinf(x):
+        t = "inf" if x > 0 else "-inf"
+    else:
+        mant, exp = f"{x:.{prec}e}".split("e")
+        t = f"{mant}e{int(exp)}"
+    return t.rjust(width)
+
+
+@dataclasses.dataclass
+class EnergyFrame:
+    """One energy-trajectory row (crates/gromos-io/src/energy.rs:97-121), kJ/mol, K, nm^3, ps."""
+
+    time: float = 0.0
+    kinetic: float = 0.0
+    potential: float = 0.0
+    total: float = 0.0
+    temperature: float = 0.0
+    volume: float = 0.0
+    pressure: float = 0.0
+    bond: float = 0.0
+    angle: float = 0.0
+    improper: float = 0.0
+    dihedral: float = 0.0
+    lj: float = 0.0
+    coul_real: float = 0.0
+    coul_recip: float = 0.0
+    coul_self: float = 0.0
+    shake: float = 0.0
+    restraint: float = 0.0
+
+    def values(self) -> List[float]:
+        return [getattr(self, f.name) for f in dataclasses.fields(self)]
+
+
+_ENE_HEADER = ["Time (ps)", "Kinetic energy (kJ/mol)", "Potential energy (kJ/mol)", "Total energy (kJ/mol)",
+               "Temperature (K)", "Volume (nm\u00b3)", "Pressure (bar)", "Bond energy", "Angle energy",
+               "Improper dihedral", "Proper dihedral", "Lennard-Jones", "Coulomb (real)", "Coulomb (reciprocal)",
+               "Coulomb (self)", "SHAKE constraint", "Distance restraint"]
+
+
+def md_energy_frame(time: float, e_kin: float, e_lj: float, e_crf: float, n_dof: float,
+                    volume: float = 0.0, e_bonded: float = 0.0) -> EnergyFrame:
+    """An ENERTRJ row from device MD statistics: nonbonded LJ and reaction-field
+    energies (Coulomb, real space), kinetic energy and the temperature
+    2 E_kin / (n_dof k_B); bonded terms, if the caller has them, in ``e_bonded``."""
+    boltz = 0.00831446261815324
+    pot = e_lj + e_crf + e_bonded
+    return EnergyFrame(time=time, kinetic=e_kin, potential=pot, total=e_kin + pot,
+                       temperature=2.0 * e_kin / (n_dof * boltz) if n_dof > 0 else 0.0, volume=volume,
+                       bond=e_bonded, lj=e_lj, coul_real=e_crf)
+
+
+class EnergyWriter:
+    """ENERTRJ energy trajectory: TITLE, then one row of 17 values per frame
+    (EnergyWriter, crates/gromos-io/src/energy.rs:181-316); ``close`` ends the block."""
+
+    def __init__(self, path: str, title: str):
+        self._f: TextIO = open(path, "w", encoding="utf-8")
+        self._f.write(f"TITLE\n  {title}\nEND\nENERTRJ\n")
+        self._header = True
+        self.frames = 0
+
+    def write_frame(self, frame: EnergyFrame) -> None:
+        if self._header:
+            self._f.write("# Block definitions (ENE format):\n")
+            for k, name in enumerate(_ENE_HEADER):
+                self._f.write(f"# {k:>3} = {name}\n")
+            self._header = False
+        self._f.write(" ".join(rust_exp(v) for v in frame.values()) + "\n")
+        self.frames += 1
+
+    def close(self) -> None:
+        if self._f:
+            self._f.write("END\n")
+            self._f.close()
+            self._f = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def read_energy_trajectory(path: str) -> List[EnergyFrame]:
+    """Frames of an ENERTRJ file (rows of at least 17 numbers; comments skipped)."""
+    frames = []
+    inside = False
+    for ln in open(path, encoding="utf-8"):
+        t = ln.strip()
+        if t == "ENERTRJ":
+            inside = True
+            continue
+        if not inside or not t or t.startswith("#"):
+            continue
+        if t == "END":
+            break
+        vals = [float(v) for v in t.split()]
+        if len(vals) < 17:
+            raise ValueError(f"{path}: energy row with {len(vals)} values, expected at least 17")
+        frames.append(EnergyFrame(*vals[:17]))
+    return frames
+
+
+class ForceWriter:
+    """Force trajectory: TITLE, then per frame TIMESTEP (``%15d%15.9f``) and
+    FREEFORCERED (three ``%18.9f`` fields per atom, a ``#`` count line every 10
+    atoms), optionally CONSFORCERED (ForceWriter, crates/gromos-io/src/force.rs:44-153)."""
+
+    def __init__(self, path: str, title: str, constraint_forces: bool = False):
+        self._f: TextIO = open(path, "w", encoding="utf-8")
+        self._f.write(f"TITLE\n  {title}\nEND\n")
+        self._cons = constraint_forces
+        self.frames = 0
+
+    def _block(self, name: str, f: np.ndarray) -> None:
+        out = [name]
+        for i, (x, y, z) in enumerate(np.asarray(f, dtype=np.float64).reshape(-1, 3)):
+            out.append(f"{x:18.9f}{y:18.9f}{z:18.9f}")
+            if (i + 1) % 10 == 0:
+                out.append(f"#{i + 1:>10}")
+        out.append("END")
+        self._f.write("\n".join(out) + "\n")
+
+    def write_frame(self, step: int, time: float, forces: np.ndarray,
+                    constraint_forces: Optional[np.ndarray] = None) -> None:
+        self._f.write(f"TIMESTEP\n{step:>15}{time:15.9f}\nEND\n")
+        self._block("FREEFORCERED", forces)
+        if self._cons:
+            cf = np.zeros_like(np.asarray(forces, dtype=np.float64)) if constraint_forces is None else constraint_forces
+            self._block("CONSFORCERED", cf)
+        self.frames += 1
+
+    def close(self) -> None:
+        if self._f:
+            self._f.close()
+            self._f = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -182,3 +182,36 @@ def test_single_atom_solute_generator():
     m = gen.solvated_solute_system(400, 60, seed=11)
     sizes = np.diff(m.topo.cg_offsets[:m.topo.n_solute_cg + 1])
     assert sizes.min() >= 3 and sizes.max() <= 5
+
+
+def test_trajectory_writers_round_trip(tmp_path):
+    """ENERTRJ and FREEFORCERED files in the reference writers' layout, read back."""
+    from gromos_nb import gromos_io as io
+    assert io.rust_exp(123.456) == "    1.234560000000e2"
+    assert io.rust_exp(-0.001) == "  -1.000000000000e-3"
+    assert io.rust_exp(0.0) == "    0.000000000000e0"
+    frames = [io.md_energy_frame(0.002 * k, 1000.0 + k, -5000.0 - 3.5 * k, -20000.25 + k, 600.0, volume=27.0)
+              for k in range(3)]
+    p = str(tmp_path / "e.tre")
+    with io.EnergyWriter(p, "device MD") as w:
+        for f in frames:
+            w.write_frame(f)
+    text = open(p, encoding="utf-8").read().splitlines()
+    assert text[:4] == ["TITLE", "  device MD", "END", "ENERTRJ"] and text[-1] == "END"
+    assert text[5] == "#   0 = Time (ps)"
+    back = io.read_energy_trajectory(p)
+    assert len(back) == 3
+    for a, b in zip(frames, back):
+        np.testing.assert_allclose(b.values(), a.values(), rtol=1e-12, atol=1e-300)
+    assert back[1].lj == -5003.5 and back[1].potential == back[1].lj + back[1].coul_real
+    forces = np.random.default_rng(1).normal(0.0, 300.0, size=(23, 3))
+    q = str(tmp_path / "f.trf")
+    with io.ForceWriter(q, "forces", constraint_forces=True) as w:
+        w.write_frame(0, 0.0, forces)
+        w.write_frame(5, 0.01, -forces)
+    lines = open(q, encoding="utf-8").read().splitlines()
+    assert lines[4] == "              0    0.000000000"
+    assert lines[7] == f"{forces[0, 0]:18.9f}{forces[0, 1]:18.9f}{forces[0, 2]:18.9f}"
+    assert "#        10" in lines and "CONSFORCERED" in lines
+    np.testing.assert_allclose(io.read_forces_step(q, 0), forces, atol=1e-9)
+    np.testing.assert_allclose(io.read_forces_step(q, 5), -forces, atol=1e-9)

@@ -95,3 +95,34 @@ def test_md_rollback_after_list_overflow():
     xo, vo, so = ob.OracleForcefield(s).md_run(s.pos, v, m, 12, dist_oh=0.1, dist_hh=g.SPC_DHH)
     assert np.abs(x - xo).max() <= 1e-5
     assert np.sqrt(((vg - vo) ** 2).sum() / (vo ** 2).sum()) <= 1e-4
+
+
+def test_md_trajectory_files(tmp_path):
+    """Device MD written as ENERTRJ / FREEFORCERED frames and read back unchanged."""
+    from gromos_nb import gromos_io as io
+    s = g.spc_water_system(500, box=g.box_for_waters(500), seed=41, rcutp=0.8, rcutl=1.2, nsnb=5)
+    m = g.masses(s)
+    ff = Forcefield(s)
+    ff.upload_positions(s.pos)
+    ff.md_init(m, g.maxwell_velocities(m, 300.0, 9), dt=0.002, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH,
+               temperature=300.0, tau=0.1)
+    dof = 3 * s.topo.n_atoms - (s.topo.n_atoms - s.topo.n_solute_atoms)
+    pe, pf = str(tmp_path / "md.tre"), str(tmp_path / "md.trf")
+    kept = []
+    with io.EnergyWriter(pe, "device MD") as we, io.ForceWriter(pf, "device MD") as wf:
+        for k in range(4):
+            st = ff.md_run(5)              # statistics of this call; the step count is kept here
+            step = 5 * (k + 1)
+            fr = io.md_energy_frame(0.002 * step, st["e_kin"], st["e_lj"], st["e_crf"], dof,
+                                    volume=float(np.prod(s.box)))
+            f = ff.result()["forces"]
+            we.write_frame(fr)
+            wf.write_frame(step, 0.002 * step, f)
+            kept.append((fr, f, step))
+    ff.close()
+    back = io.read_energy_trajectory(pe)
+    assert len(back) == 4
+    for (fr, f, step), b in zip(kept, back):
+        np.testing.assert_allclose(b.values(), fr.values(), rtol=1e-12)
+        assert 0.0 < b.temperature < 1e4 and np.isfinite(b.total)
+        np.testing.assert_allclose(io.read_forces_step(pf, step), f, atol=1e-9)
