@@ -927,6 +927,9 @@ gr_status NbSystem::eval_graph(cudaStream_t s, int flags) {
         if (!st) warm = true;
         return st;
     }
+    // capacities grown after an overflow are allocated before the rebuild
+    // graph runs; a reallocation records the graphs again
+    if (rebuild && (st = ensure_capacity())) return st;
     if (g_gen != alloc_gen) {
         drop_graphs();
         if ((st = ensure_capacity())) return st;

@@ -304,10 +304,17 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
         return GR_ERR_INVALID;
     }
     const size_t bytes3 = size_t(N) * 3 * sizeof(double);
+    // The error flags are sticky in device memory, so they are read once per
+    // block of whole pairlist periods (one host synchronisation per block);
+    // an overflow anywhere in the block rolls the whole block back.  Kernels
+    // are launched one by one: the host runs ahead of the device, and the
+    // recorded step graphs would add their per-step flag copy and timing
+    // events (measured slower here).
+    const int kblock = std::max(1, prm.nsnb) * 4;
     int done = 0, attempts = 0, rollbacks = 0;
     gr_status st;
     while (done < n_steps) {
-        // snapshot at the start of the period
+        // snapshot at the start of the block
         GR_CUDA(cudaMemcpyAsync(md_pos_snap, h.pos, bytes3, cudaMemcpyDeviceToDevice, s));
         GR_CUDA(cudaMemcpyAsync(md_vel_snap, md_vel, bytes3, cudaMemcpyDeviceToDevice, s));
         GR_CUDA(cudaMemcpyAsync(md_ke_snap, md_ke, sizeof(long long), cudaMemcpyDeviceToDevice, s));
@@ -326,15 +333,15 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
             if ((st = eval(s, 0, false))) return st;
             if ((st = md_step_launch(s))) return st;
             ++k;
-            if (done + k >= n_steps || steps_since_update >= prm.nsnb) break;
+            if (done + k >= n_steps || (steps_since_update >= prm.nsnb && k >= kblock)) break;
         }
         if (!overflow) {
-            // everything of this period (build and force kernels) has set its flags
+            // everything of this block (builds and force kernels) has set its flags
             GR_CUDA(cudaMemcpyAsync(md_err_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
             GR_CUDA(cudaEventRecord(ev_md, s));
             GR_CUDA(cudaEventSynchronize(ev_md));
             const int* e = reinterpret_cast<const int*>(md_err_host);
-            if (pending_check) {  // a rebuild at the period's last step: its flags are in e[0] too
+            if (pending_check) {  // a rebuild at the block's last step: its flags are in e[0] too
                 pending_check = false;
             }
             if (e[0]) {
@@ -364,7 +371,7 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
             GR_CUDA(cudaMemcpyAsync(md_vel, md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, s));
             GR_CUDA(cudaMemcpyAsync(md_ke, md_ke_snap, sizeof(long long), cudaMemcpyDeviceToDevice, s));
             steps_since_update = ssu0;
-            built = false;  // the period is re-run from a fresh build with the grown lists
+            built = false;  // the block is re-run from a fresh build with the grown lists
             lr_computed = false;
             ++rollbacks;
             continue;

@@ -241,6 +241,24 @@ def test_graph_replay_bit_identical(kind):
     b.close()
 
 
+def test_graph_replay_regrows_lists():
+    """Graph replay whose rebuild overflows (denser positions than the lists were sized for): the
+    lists are grown, the graphs recorded again, and forces equal the launch-by-launch path."""
+    s = generators.spc_water_system(1500, box=generators.box_for_waters(1500), seed=25, rcutp=0.8, rcutl=1.2,
+                                    nsnb=2)
+    a, b = Forcefield(s), Forcefield(s, list_capacity=16)
+    w = s.pos.reshape(-1, 3, 3)
+    dense = (w + (0.7 * w[:, 0] - w[:, 0])[:, None, :]).reshape(-1, 3)   # rigid waters, centres pulled in
+    for step, pos in enumerate([s.pos, s.pos, dense, dense, dense]):
+        ra = a.apply(pos, force_rebuild=True)
+        rb = b.apply(pos, force_rebuild=True, graph=True)
+        assert np.all(np.isfinite(ra["forces"]))
+        assert np.array_equal(ra["forces"], rb["forces"]), step
+        assert ra["e_lj"] == rb["e_lj"] and ra["e_crf"] == rb["e_crf"]
+    a.close()
+    b.close()
+
+
 def test_list_overflow_regrow():
     """Solvent lists far too small at the start: every overflow is grown and the step redone."""
     s = generators.spc_water_system(1500, box=generators.box_for_waters(1500), seed=24, rcutp=0.8, rcutl=1.2,
