@@ -9,10 +9,11 @@
 //
 // Overflow recovery: list overflows (pairlist capacity, deferred water pairs)
 // are detected after the fact from the device error flags.  The runner keeps
-// a device snapshot of (positions, velocities) at the start of every pairlist
-// period (the steps between two rebuilds), reads the flags at the end of the
-// period, and on overflow grows the lists, restores the snapshot and runs the
-// period again, so an overflow never leaks into the trajectory.
+// a device snapshot of (positions, velocities) at the start of every block of
+// pairlist periods (a period is the steps between two rebuilds), reads the
+// flags at the end of the block, and on overflow grows the lists, restores
+// the snapshot and runs the block again, so an overflow never leaks into the
+// trajectory.
 #include <cuda_runtime.h>
 
 namespace gnb {
@@ -24,8 +25,8 @@ struct MdDev {
     double dt, dt_i;
     int settle;               // SETTLE every solvent molecule
     double m_o, m_h, ra, rb, rc;  // canonical SETTLE triangle (constraints.rs:836-840)
-    long long* ke;            // [2]: [0] kinetic energy of the velocities entering the step, [1] accumulator
-                              // of the velocities leaving it (fixed point 2^24)
+    long long* ke;            // [3]: [0] kinetic energy of the velocities entering the step, [1] accumulator
+                              // of the velocities leaving it (fixed point 2^24), [2] blocks finished
     int* failures;            // [1] molecules SETTLE could not solve
     double t0, tau, dof;      // Berendsen bath (tau < 0: none)
 };
@@ -40,12 +41,6 @@ __device__ __forceinline__ double berendsen_lambda(const MdDev& md) {
     if (t < 1e-10) t = md.t0;
     if (t < 1e-10) return 1.0;
     return md.tau == 0.0 ? sqrt(md.t0 / t) : sqrt(1.0 + md.dt / md.tau * (md.t0 / t - 1.0));
-}
-
-// The accumulated kinetic energy becomes the next step's input.
-__global__ void k_ke_commit(long long* ke) {
-    ke[0] = ke[1];
-    ke[1] = 0;
 }
 
 // Velocities scaled by `f` (temperature exchange), kinetic energy with them.
@@ -168,6 +163,18 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
     ke = warp_sum_ll(ke);
     if ((threadIdx.x & 31) == 0 && ke) atomicAdd(reinterpret_cast<unsigned long long*>(md.ke + 1),
                                                   static_cast<unsigned long long>(ke));
+    // The last block to finish makes the accumulated kinetic energy the next
+    // step's input (every block read ke[0] for its bath factor before adding).
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        last = atomicAdd(reinterpret_cast<unsigned long long*>(md.ke + 2), 1ull) == gridDim.x - 1;
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        md.ke[0] = static_cast<long long>(atomicExch(reinterpret_cast<unsigned long long*>(md.ke + 1), 0ull));
+        md.ke[2] = 0;
+    }
 }
 
 }  // namespace gnb
@@ -215,14 +222,14 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
     gr_status st;
     if ((st = upload_array(&md_mass, mass, N)) || (st = upload_array(&md_inv_mass, inv.data(), N)) ||
         (st = upload_array(&md_vel, v0.data(), size_t(N) * 3)) || (st = alloc(&md_pos_snap, size_t(N) * 3)) ||
-        (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 2)) || (st = alloc(&md_ke_snap, 1)) ||
+        (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 3)) || (st = alloc(&md_ke_snap, 1)) ||
         (st = alloc(&md_fail, 1)))
         return st;
     {
         double ke0 = 0.0;
         for (int i = 0; i < N; ++i)
             ke0 += 0.5 * mass[i] * (v0[3 * i] * v0[3 * i] + v0[3 * i + 1] * v0[3 * i + 1] + v0[3 * i + 2] * v0[3 * i + 2]);
-        const long long k[2] = {static_cast<long long>(std::llround(ke0 * kEnergyScale)), 0};
+        const long long k[3] = {static_cast<long long>(std::llround(ke0 * kEnergyScale)), 0, 0};
         GR_CUDA(cudaMemcpy(md_ke, k, sizeof(k), cudaMemcpyHostToDevice));
     }
     GR_CUDA(cudaMemset(md_fail, 0, sizeof(int)));
@@ -268,7 +275,6 @@ gr_status NbSystem::md_step_launch(cudaStream_t s) {
     const int n_units = md_settle ? NSA + (N - NSA) / 3 : N;
     const unsigned grid = std::max(1u, std::min(unsigned((n_units + 255) / 256), unsigned(sm_count() * 8)));
     (++launches, k_md_step<<<grid, 256, 0, s>>>(d_sys, md));
-    (++launches, k_ke_commit<<<1, 1, 0, s>>>(md_ke));
     return GR_OK;
 }
 
