@@ -516,11 +516,14 @@ def main():
     ap.add_argument("--no-plain-md", action="store_true", help="skip the plain-kernel MD comparison")
     ap.add_argument("--workload", default="spc30000", choices=["spc30000", "remd", "fep", "serving"])
     ap.add_argument("--replicas", type=int, default=256)
-    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-steps", type=int, default=None,
+                    help="MD steps per batched run (default: 500 for fep, the FEP windows' length; 100 for remd)")
     ap.add_argument("--sample-members", type=int, default=8, help="members timed one by one for comparison")
     ap.add_argument("--jobs", type=int, default=40)
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
+    if args.batch_steps is None:
+        args.batch_steps = 500 if args.workload == "fep" else 100
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world = int(os.environ.get("WORLD_SIZE", "1"))
