@@ -835,7 +835,10 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 64), 64, 0, s>>>(d_sys));
             if ((st = launch_water(s, wp, false))) return st;
         }
-        if (NSCG > 0) (++launches, k_solute_force<false><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
+        // solute work items: (CG, chunk of list entries), 4 warps per block
+        const unsigned sgrid = std::max(1u, std::min(blocks_for((long long)NSCG * ((h.scap + kSoluteChunk - 1) / kSoluteChunk), 4),
+                                                     unsigned(sm * 8)));
+        if (NSCG > 0) (++launches, k_solute_force<false><<<sgrid, 128, shg, s>>>(d_sys));
         if (record_events) GR_CUDA(record_event(ev[2], s));
         if (do_long) {
             GR_CUDA(cudaMemsetAsync(h.f_long, 0, size_t(N) * 3 * sizeof(long long), s));
@@ -846,7 +849,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
                 WaterParams wpl = water_params(true);
                 if ((st = launch_water(s, wpl, true))) return st;
             }
-            if (NSCG > 0) (++launches, k_solute_force<true><<<blocks_for(NSCG, 4), 128, shg, s>>>(d_sys));
+            if (NSCG > 0) (++launches, k_solute_force<true><<<sgrid, 128, shg, s>>>(d_sys));
             lr_computed = true;
         }
     } else {

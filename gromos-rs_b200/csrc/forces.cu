@@ -158,6 +158,15 @@ __device__ __forceinline__ void solute_pair_vector(const SysDev& s, bool per_ato
 
 // Solute CG pairs (solute-solute, solute-solvent, intra-CG).  One warp per
 // solute CG i, one lane per j entry.  Entries of the other range are skipped.
+// Work items are (solute CG, chunk of kSoluteChunk list entries): a CG's list
+// is spread over several warps, each adding its share of the CG's forces with
+// fixed-point reductions.  Group energies are summed per lane in FP32 for the
+// current energy-group slot and the virial per lane in FP32; both go to
+// fixed point when the slot changes and at the end of every item, so every
+// FP32 sum covers pairs of one item only and the results do not depend on
+// the grid or on which warp took which item.
+constexpr int kSoluteChunk = 64;
+
 template <bool LONG>
 __global__ void __launch_bounds__(128) k_solute_force(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
@@ -169,7 +178,24 @@ __global__ void __launch_bounds__(128) k_solute_force(const SysDev* __restrict__
     for (int v = threadIdx.x; v < 2 * G * G; v += blockDim.x) shg[v] = 0ull;
     __syncthreads();
     float v6[6] = {0, 0, 0, 0, 0, 0};
-    for (int ci = blockIdx.x * wpb + (threadIdx.x >> 5); ci < s.n_solute_cg; ci += gridDim.x * wpb) {
+    long long vfix[6] = {0, 0, 0, 0, 0, 0};
+    int cur_slot = -1;
+    float e_lj = 0.f, e_cr = 0.f;
+    auto flush_slot = [&]() {
+        if (cur_slot >= 0) {
+            const long long fl = to_fixed_f(e_lj, kE), fc = to_fixed_f(e_cr, kE);
+            if (fl) atomicAdd(&shg[cur_slot], static_cast<unsigned long long>(fl));
+            if (fc) atomicAdd(&shg[G * G + cur_slot], static_cast<unsigned long long>(fc));
+        }
+        e_lj = e_cr = 0.f;
+    };
+    const int per = (s.scap + kSoluteChunk - 1) / kSoluteChunk;
+    const int nitems = s.n_solute_cg * per;
+    for (int it = blockIdx.x * wpb + (threadIdx.x >> 5); it < nitems; it += gridDim.x * wpb) {
+        const int ci = it / per;
+        const int e_beg = (it - ci * per) * kSoluteChunk;
+        const int cnt = min(s.sn[ci], e_beg + kSoluteChunk);
+        if (e_beg >= cnt) continue;  // warp-uniform
         const int i0 = s.cg_off[ci], ni = s.cg_off[ci + 1] - i0;
         const double xi0 = s.pos[3 * i0], yi0 = s.pos[3 * i0 + 1], zi0 = s.pos[3 * i0 + 2];
         float dix[kMaxCGAtoms], diy[kMaxCGAtoms], diz[kMaxCGAtoms];
@@ -185,10 +211,9 @@ __global__ void __launch_bounds__(128) k_solute_force(const SysDev* __restrict__
                 dix[a] = diy[a] = diz[a] = 0.f;
             }
         }
-        const int cnt = s.sn[ci];
         const int* __restrict__ list = s.sl + static_cast<size_t>(ci) * s.scap;
         const unsigned long long* __restrict__ xl = s.sl_excl + static_cast<size_t>(ci) * s.scap;
-        for (int e0 = 0; e0 < cnt; e0 += 32) {
+        for (int e0 = e_beg; e0 < cnt; e0 += 32) {
             const int e = e0 + lane;
             int entry = e < cnt ? list[e] : -1;
             if (entry >= 0 && (entry & 1) != (LONG ? 1 : 0)) entry = -1;
@@ -243,9 +268,12 @@ __global__ void __launch_bounds__(128) k_solute_force(const SysDev* __restrict__
                     v6[4] = fmaf(y, fzz, v6[4]);
                     v6[5] = fmaf(z, fzz, v6[5]);
                     const int sl = group_slot(G, s.egroup[ai], gj);
-                    long long fl = to_fixed_f(el, kE), fc = to_fixed_f(ec, kE);
-                    if (fl) atomicAdd(&shg[sl], static_cast<unsigned long long>(fl));
-                    if (fc) atomicAdd(&shg[G * G + sl], static_cast<unsigned long long>(fc));
+                    if (sl != cur_slot) {
+                        flush_slot();
+                        cur_slot = sl;
+                    }
+                    e_lj += el;
+                    e_cr += ec;
                 }
                 red_add(&F[3 * aj], to_fixed_f(gxs, kF));
                 red_add(&F[3 * aj + 1], to_fixed_f(gys, kF));
@@ -263,15 +291,22 @@ __global__ void __launch_bounds__(128) k_solute_force(const SysDev* __restrict__
                 red_add(&F[3 * (i0 + a) + 2], to_fixed_f(vz, kF));
             }
         }
+        flush_slot();
+        cur_slot = -1;
+#pragma unroll
+        for (int v = 0; v < 6; ++v) {
+            vfix[v] += to_fixed_f(v6[v], kE);
+            v6[v] = 0.f;
+        }
     }
     long long* dst = LONG ? s.acc_long : s.acc_short;
     __syncthreads();
     for (int v = threadIdx.x; v < 2 * G * G; v += blockDim.x)
         if (shg[v]) atomicAdd(reinterpret_cast<unsigned long long*>(dst + v), shg[v]);
     long long acc[9];
-    float vv[9] = {v6[0], v6[1], v6[2], v6[1], v6[3], v6[4], v6[2], v6[4], v6[5]};
+    const long long vv[9] = {vfix[0], vfix[1], vfix[2], vfix[1], vfix[3], vfix[4], vfix[2], vfix[4], vfix[5]};
 #pragma unroll
-    for (int v = 0; v < 9; ++v) acc[v] = to_fixed_f(warp_sum(vv[v]), kE);
+    for (int v = 0; v < 9; ++v) acc[v] = warp_sum_ll(vv[v]);
     int idx[9];
 #pragma unroll
     for (int v = 0; v < 9; ++v) idx[v] = 2 * G * G + v;
