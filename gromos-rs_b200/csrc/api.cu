@@ -873,7 +873,9 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     const size_t sha = size_t(NA) * sizeof(unsigned long long);
     if (h.excl_atoms > 0) (++launches, k_excluded_14<<<blocks_for(h.excl_atoms, 128), 128, sha, s>>>(d_sys));
     if (n_pert > 0) {
-        if (NSCG > 0) (++launches, k_pert_pairs_force<<<blocks_for(std::max(pcap_alloc, 1), 128), 128, sha, s>>>(d_sys));
+        if (NSCG > 0)
+            (++launches, k_pert_pairs_force<<<blocks_for((std::max(pcap_alloc, 1) + kPertRun - 1) / kPertRun, 128), 128, sha,
+                                              s>>>(d_sys));
         (++launches, k_pert_terms<<<blocks_for(std::max(N, h.n_pp), 128), 128, sha, s>>>(d_sys));
     }
     (++launches, k_finalize<<<blocks_for(std::max<long long>(3LL * N, NA), 256), 256, 0, s>>>(d_sys, prm.kernel == GR_KERNEL_PLAIN));

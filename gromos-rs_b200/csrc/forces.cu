@@ -415,13 +415,6 @@ __device__ __forceinline__ void shared_add(unsigned long long* sh, int idx, doub
     if (f) atomicAdd(&sh[idx], static_cast<unsigned long long>(f));
 }
 
-__device__ __forceinline__ void shared_virial(unsigned long long* sh, int vb, double rx, double ry, double rz,
-                                              double fx, double fy, double fz) {
-    double r[3] = {rx, ry, rz}, f[3] = {fx, fy, fz};
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) shared_add(sh, vb + a * 3 + b, r[a] * f[b]);
-}
-
 // rf_excluded_interactions (excluded.rs:25-112) + one_four_interaction_loop
 // (excluded.rs:131-206, coulomb scaling 1).  One thread per atom i.
 __global__ void k_excluded_14(const SysDev* __restrict__ sys) {
@@ -433,6 +426,32 @@ __global__ void k_excluded_14(const SysDev* __restrict__ sys) {
     __syncthreads();
     const int vb = 2 * G * G;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // a thread's virial and energies are summed in registers (energies per
+    // group slot, flushed when the slot changes) and added to the block's
+    // fixed-point sums once, not per pair
+    double vir[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int cur_sl = -1;
+    double e_l = 0.0, e_c = 0.0;
+    auto flush_e = [&]() {
+        if (cur_sl >= 0) {
+            shared_add(sh, cur_sl, e_l);
+            shared_add(sh, G * G + cur_sl, e_c);
+        }
+        e_l = e_c = 0.0;
+    };
+    auto to_slot = [&](int sl) {
+        if (sl != cur_sl) {
+            flush_e();
+            cur_sl = sl;
+        }
+    };
+    auto add_vir = [&](double rx, double ry, double rz, double fx, double fy, double fz) {
+        const double r[3] = {rx, ry, rz}, f[3] = {fx, fy, fz};
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int w = 0; w < 3; ++w) vir[u * 3 + w] += r[u] * f[w];
+    };
     if (i < s.excl_atoms) {
         const double qi = s.charge[i];
         const double xi = s.pos[3 * i], yi = s.pos[3 * i + 1], zi = s.pos[3 * i + 2];
@@ -440,7 +459,8 @@ __global__ void k_excluded_14(const SysDev* __restrict__ sys) {
         double fxi = 0, fyi = 0, fzi = 0;
         if (i < s.n_solute_atoms) {
             double term = -0.5 * qi * qi * s.fpe * s.crf_cut;
-            shared_add(sh, G * G + group_slot(G, gi, gi), term);
+            to_slot(group_slot(G, gi, gi));
+            e_c += term;
         }
         for (int k = s.excl_off[i]; k < s.excl_off[i + 1]; ++k) {
             const int j = s.excl[k];
@@ -449,18 +469,19 @@ __global__ void k_excluded_14(const SysDev* __restrict__ sys) {
             nearest_image_exact(s, xi, yi, zi, s.pos[3 * j], s.pos[3 * j + 1], s.pos[3 * j + 2], rx, ry, rz);
             const double r2 = len2_exact(rx, ry, rz);
             const int sl = group_slot(G, gi, s.egroup[j]);
+            to_slot(sl);
             if (i < s.n_solute_atoms) {
                 const double q = qi * s.charge[j] * s.fpe;
-                shared_add(sh, G * G + sl, q * (-s.crf_2cut3i * r2 - s.crf_cut));
+                e_c += q * (-s.crf_2cut3i * r2 - s.crf_cut);
                 const double fs = q * s.crf_cut3i;
                 const double fx = rx * fs, fy = ry * fs, fz = rz * fs;
                 fxi += fx;
                 fyi += fy;
                 fzi += fz;
                 add_force_fixed(s.f_short, j, -fx, -fy, -fz);
-                shared_virial(sh, vb, rx, ry, rz, fx, fy, fz);
+                add_vir(rx, ry, rz, fx, fy, fz);
             } else {
-                shared_add(sh, G * G + sl, -qi * s.charge[j] * s.fpe * s.crf_2cut3i * r2);
+                e_c += -qi * s.charge[j] * s.fpe * s.crf_2cut3i * r2;
             }
         }
         for (int k = s.o14_off[i]; k < s.o14_off[i + 1]; ++k) {
@@ -484,12 +505,15 @@ __global__ void k_excluded_14(const SysDev* __restrict__ sys) {
             fyi += fy;
             fzi += fz;
             add_force_fixed(s.f_short, j, -fx, -fy, -fz);
-            const int sl = group_slot(G, gi, s.egroup[j]);
-            shared_add(sh, sl, el);
-            shared_add(sh, G * G + sl, ec);
-            shared_virial(sh, vb, rx, ry, rz, fx, fy, fz);
+            to_slot(group_slot(G, gi, s.egroup[j]));
+            e_l += el;
+            e_c += ec;
+            add_vir(rx, ry, rz, fx, fy, fz);
         }
         if (fxi != 0.0 || fyi != 0.0 || fzi != 0.0) add_force_fixed(s.f_short, i, fxi, fyi, fzi);
+        flush_e();
+#pragma unroll
+        for (int u = 0; u < 9; ++u) shared_add(sh, vb + u, vir[u]);
     }
     __syncthreads();
     for (int v = threadIdx.x; v < NA; v += blockDim.x)
@@ -566,6 +590,15 @@ __device__ __forceinline__ PInfo pinfo(const SysDev& s, int a) {
 
 // perturbed_pairlist_correction (perturbed.rs:309-386) for the explicit list
 // of (i perturbed, j) pairs of all lists, every step, per-atom image.
+// Each thread takes kPertRun consecutive pairs of the list (pairs are listed
+// per perturbed atom, so i rarely changes within a run).  Every pair's
+// contribution goes to fixed point first and the integers are summed in
+// registers -- the i-force until i changes, the energies until their group
+// slot changes -- so far fewer same-address atomics are issued than one per
+// pair, and the totals do not depend on the list's order (which the atomic
+// appends of k_pert_pairs do not fix).
+constexpr int kPertRun = 16;
+
 __global__ void k_pert_pairs_force(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
     const int G = s.n_egroups;
@@ -573,9 +606,27 @@ __global__ void k_pert_pairs_force(const SysDev* __restrict__ sys) {
     extern __shared__ unsigned long long sh[];
     for (int v = threadIdx.x; v < NA; v += blockDim.x) sh[v] = 0ull;
     __syncthreads();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int np = min(s.n_pert_pairs[0], s.pcap);
-    if (p < np) {
+    const int p0 = (blockIdx.x * blockDim.x + threadIdx.x) * kPertRun;
+    const int p1 = min(np, p0 + kPertRun);
+    int cur_i = -1, cur_sl = -1;
+    long long fxi = 0, fyi = 0, fzi = 0, el = 0, ec = 0, dh = 0;
+    auto flush_i = [&]() {
+        if (cur_i >= 0) {
+            red_add(&s.f_short[3 * cur_i], fxi);
+            red_add(&s.f_short[3 * cur_i + 1], fyi);
+            red_add(&s.f_short[3 * cur_i + 2], fzi);
+        }
+        fxi = fyi = fzi = 0;
+    };
+    auto flush_e = [&]() {
+        if (cur_sl >= 0) {
+            if (el) atomicAdd(&sh[cur_sl], static_cast<unsigned long long>(el));
+            if (ec) atomicAdd(&sh[G * G + cur_sl], static_cast<unsigned long long>(ec));
+        }
+        el = ec = 0;
+    };
+    for (int p = p0; p < p1; ++p) {
         const int i = s.pert_pairs[3 * p], j = s.pert_pairs[3 * p + 1];
         const PInfo pi = pinfo(s, i), pj = pinfo(s, j);
         const double* lja = s.lj64 + 4 * (pi.a_iac * s.n_types + pj.a_iac);
@@ -598,13 +649,26 @@ __global__ void k_pert_pairs_force(const SysDev* __restrict__ sys) {
         double o[5];
         pert_interaction(s, rx, ry, rz, lja[0], lja[1], ljb[0], ljb[1], a_q, b_q, alj, acrf, o);
         const double df = o[0] - fa;
-        add_force_fixed(s.f_short, i, rx * df, ry * df, rz * df);
+        if (i != cur_i) {
+            flush_i();
+            cur_i = i;
+        }
+        fxi += to_fixed_d(rx * df, kForceScale);
+        fyi += to_fixed_d(ry * df, kForceScale);
+        fzi += to_fixed_d(rz * df, kForceScale);
         add_force_fixed(s.f_short, j, -rx * df, -ry * df, -rz * df);
         const int sl = group_slot(G, s.egroup[i], s.egroup[j]);
-        shared_add(sh, sl, o[1] - ela);
-        shared_add(sh, G * G + sl, o[2] - eca);
-        shared_add(sh, NA - 1, o[3] + o[4]);
+        if (sl != cur_sl) {
+            flush_e();
+            cur_sl = sl;
+        }
+        el += to_fixed_d(o[1] - ela, kEnergyScale);
+        ec += to_fixed_d(o[2] - eca, kEnergyScale);
+        dh += to_fixed_d(o[3] + o[4], kEnergyScale);
     }
+    flush_i();
+    flush_e();
+    if (dh) atomicAdd(&sh[NA - 1], static_cast<unsigned long long>(dh));
     __syncthreads();
     for (int v = threadIdx.x; v < NA; v += blockDim.x)
         if (sh[v]) atomicAdd(reinterpret_cast<unsigned long long*>(s.acc_short + v), sh[v]);
