@@ -685,6 +685,11 @@ __device__ unsigned long long excl_mask(const SysDev& s, int ci, int cj) {
 // solute CG.  Entry = (j << 1 | long); the first entry is the CG itself
 // (intra-CG pairs, pairlist.rs:239-249).
 __global__ void k_solute_search(const SysDev* __restrict__ sys) {
+    // Candidates are swept 32 at a time through the neighbour cells in z-y-x
+    // order; positions come from the sorted copy of the reference positions
+    // (sref: the same FP64 values, stored at the sorted position) and the next
+    // round's candidate is loaded while this round's is tested, so a round
+    // waits for one memory latency instead of two chained ones.
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31;
     const int ci = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -701,51 +706,93 @@ __global__ void k_solute_search(const SysDev* __restrict__ sys) {
         outx[0] = excl_mask(s, ci, ci);
     }
     cnt = 1;
-    double xi = s.ref[3 * ci], yi = s.ref[3 * ci + 1], zi = s.ref[3 * ci + 2];
-    int cell = s.cg_cell[ci];
-    int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
-    int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
+    const double xi = s.ref[3 * ci], yi = s.ref[3 * ci + 1], zi = s.ref[3 * ci + 2];
+    const int cell = s.cg_cell[ci];
+    const int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
+    const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
     int ox[3], oy[3], oz[3];
-    int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
+    const int nx = axis_offsets(gx, ox), ny = axis_offsets(gy, oy), nz = axis_offsets(gz, oz);
+    int ncl[27];
+    int nn = 0;
     for (int iz = 0; iz < nz; ++iz)
         for (int iy = 0; iy < ny; ++iy)
-            for (int ix = 0; ix < nx; ++ix) {
-                int nc = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
-                int j0 = s.cell_start[nc], j1 = s.cell_start[nc + 1];
-                for (int base = j0; base < j1; base += 32) {
-                    int sp = base + lane;
-                    int entry = -1;
-                    unsigned long long xm = 0;
-                    if (sp < j1) {
-                        int cj = s.sorted_cg[sp];
-                        bool solute_j = cj < s.n_solute_cg;
-                        if (!solute_j || cj > ci) {
-                            double rx, ry, rz;
-                            nearest_image_exact(s, xi, yi, zi, s.ref[3 * cj], s.ref[3 * cj + 1],
-                                                s.ref[3 * cj + 2], rx, ry, rz);
-                            double d2 = len2_exact(rx, ry, rz);
-                            if (!(d2 > s.c2l)) {
-                                int lr = d2 > s.c2s ? 1 : 0;
-                                if (solute_j && s.cg_off[cj + 1] - s.cg_off[cj] > kMaxCGAtoms) {
-                                    atomicOr(&s.err[0], ERR_CG_TOO_LARGE);
-                                } else {
-                                    entry = (cj << 1) | lr;
-                                    if (solute_j && !lr) xm = excl_mask(s, ci, cj);
-                                }
-                            }
-                        }
+            for (int ix = 0; ix < nx; ++ix)
+                ncl[nn++] = imod(cx + ox[ix], gx) + gx * (imod(cy + oy[iy], gy) + gy * imod(cz + oz[iz], gz));
+    const int stride = s.n_cg + 2;
+    const int* __restrict__ cell_start = s.cell_start;
+    const int* __restrict__ sorted_cg = s.sorted_cg;
+    const double* __restrict__ sref = s.sref;
+    // sweep state: neighbour k, round start base within [cell_start[ncl[k]], cell_start[ncl[k] + 1])
+    int k = 0, base = 0, end = 0;
+    auto seek = [&]() {  // first non-empty cell at or after k
+        while (k < nn) {
+            base = cell_start[ncl[k]];
+            end = cell_start[ncl[k] + 1];
+            if (base < end) return;
+            ++k;
+        }
+    };
+    struct Cand {
+        int cj;
+        double x, y, z;
+    };
+    auto load = [&](int b, int e) {
+        Cand c{-1, 0.0, 0.0, 0.0};
+        const int sp = b + lane;
+        if (sp < e) {
+            c.cj = sorted_cg[sp];
+            c.x = sref[sp];
+            c.y = sref[stride + sp];
+            c.z = sref[2 * stride + sp];
+        }
+        return c;
+    };
+    seek();
+    Cand cur = k < nn ? load(base, end) : Cand{-1, 0.0, 0.0, 0.0};
+    while (k < nn) {
+        // the next round: advance, then load it before this round is tested
+        int nb = base + 32, ne = end;
+        if (nb >= end) {
+            ++k;
+            seek();
+            nb = base;
+            ne = end;
+        }
+        const bool more = k < nn;
+        const Cand nxt = more ? load(nb, ne) : Cand{-1, 0.0, 0.0, 0.0};
+        int entry = -1;
+        unsigned long long xm = 0;
+        const int cj = cur.cj;
+        if (cj >= 0) {
+            const bool solute_j = cj < s.n_solute_cg;
+            if (!solute_j || cj > ci) {
+                double rx, ry, rz;
+                nearest_image_exact(s, xi, yi, zi, cur.x, cur.y, cur.z, rx, ry, rz);
+                const double d2 = len2_exact(rx, ry, rz);
+                if (!(d2 > s.c2l)) {
+                    const int lr = d2 > s.c2s ? 1 : 0;
+                    if (solute_j && s.cg_off[cj + 1] - s.cg_off[cj] > kMaxCGAtoms) {
+                        atomicOr(&s.err[0], ERR_CG_TOO_LARGE);
+                    } else {
+                        entry = (cj << 1) | lr;
+                        if (solute_j && !lr) xm = excl_mask(s, ci, cj);
                     }
-                    unsigned b = __ballot_sync(0xffffffffu, entry >= 0);
-                    if (entry >= 0) {
-                        int p = cnt + __popc(b & ((1u << lane) - 1u));
-                        if (p < s.scap) {
-                            out[p] = entry;
-                            outx[p] = xm;
-                        }
-                    }
-                    cnt += __popc(b);
                 }
             }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, entry >= 0);
+        if (entry >= 0) {
+            const int p = cnt + __popc(bal & ((1u << lane) - 1u));
+            if (p < s.scap) {
+                out[p] = entry;
+                outx[p] = xm;
+            }
+        }
+        cnt += __popc(bal);
+        cur = nxt;
+        base = nb;
+        end = ne;
+    }
     if (lane == 0) {
         if (cnt > s.scap) atomicOr(&s.err[0], ERR_SLIST_OVERFLOW);
         s.sn[ci] = min(cnt, s.scap);
