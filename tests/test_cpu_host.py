@@ -215,3 +215,16 @@ def test_trajectory_writers_round_trip(tmp_path):
     assert "#        10" in lines and "CONSFORCERED" in lines
     np.testing.assert_allclose(io.read_forces_step(q, 0), forces, atol=1e-9)
     np.testing.assert_allclose(io.read_forces_step(q, 5), -forces, atol=1e-9)
+
+
+def test_single_atom_solute_md_stays_stable():
+    """A serving-style system (single-atom solute CGs, Berendsen bath) runs 800 FP64 oracle MD steps
+    with no SETTLE failure; unbonded multi-atom CGs drifted apart within that many steps."""
+    from gromos_nb import generators as gen
+    s = gen.solvated_solute_system(500, 60, seed=77, rc=1.0, nsnb=5, single_atom_cgs=True)
+    m = gen.masses(s)
+    o = ob.OracleForcefield(s)
+    x, v, st = o.md_run(s.pos, gen.maxwell_velocities(m, 300.0, 5), m, 800, dist_oh=0.1, dist_hh=gen.SPC_DHH,
+                        temperature=300.0, tau=0.1)
+    assert st["settle_failures"] == 0
+    assert np.all(np.isfinite(x)) and np.all(np.isfinite(v))
