@@ -180,3 +180,58 @@ def test_member_close_leaves_batch():
     assert np.array_equal(x, xr) and np.array_equal(v, vr)
     b.close()
     c.close()
+
+
+def test_batch_graphs_across_joins_and_leaves():
+    """Batch graphs replayed over several pairlist periods, then recorded again after a join (the new
+    member mid-way through the others' periods) and after a leave; every member's trajectory is its
+    standalone one, bit for bit."""
+    sy = systems()
+    b = Batch()
+    a, c, d = member(sy[0], 11), member(sy[1], 12), member(sy[3], 13)
+    b.add(a)
+    b.add(c)
+    b.md_run(12)
+    b.add(d)                 # joins at batch step 12 with its own rebuild phase
+    b.md_run(13)
+    b.remove(a)
+    b.md_run(3)
+    for ff, (s, seed, n) in zip((a, c, d), [(sy[0], 11, 25), (sy[1], 12, 28), (sy[3], 13, 16)]):
+        x, v = ff.md_state()
+        xr, vr = standalone(s, seed, n)
+        assert np.array_equal(x, xr) and np.array_equal(v, vr), seed
+    b.close()
+    for ff in (a, c, d):
+        ff.close()
+
+
+def test_batch_member_rollback_after_list_overflow():
+    """A member's rebuild inside a batch step overflows its (deliberately tiny) lists: that member is
+    rolled back to its period start and re-run alone with grown lists, the other members go on; its
+    trajectory is the oracle's and the others' are their standalone ones."""
+    s = g.spc_water_system(1200, box=g.box_for_waters(1200), seed=33, rcutp=0.8, rcutl=1.2, nsnb=5)
+    m = g.masses(s)
+    v = g.maxwell_velocities(m, 300.0, 8)
+    small = Forcefield(s)
+    small.apply(s.pos)                   # lists sized from the density, built synchronously
+    small.set_params(list_capacity=16)   # later rebuilds run asynchronously with tiny lists
+    small.upload_positions(s.pos)
+    small.md_init(m, v, dt=0.002, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    sy = systems()[:2]
+    others = [member(x, 60 + k) for k, x in enumerate(sy)]
+    b = Batch()
+    for ff in [small] + others:
+        b.add(ff)
+    b.md_run(12)
+    assert small.md_stats()["rollbacks"] >= 1
+    x, vg = small.md_state()
+    xo, vo, _ = ob.OracleForcefield(s).md_run(s.pos, v, m, 12, dist_oh=0.1, dist_hh=g.SPC_DHH)
+    assert np.abs(x - xo).max() <= 1e-5
+    assert np.sqrt(((vg - vo) ** 2).sum() / (vo ** 2).sum()) <= 1e-4
+    for k, (sx, ff) in enumerate(zip(sy, others)):
+        xx, vv = ff.md_state()
+        xr, vr = standalone(sx, 60 + k, 12)
+        assert np.array_equal(xx, xr) and np.array_equal(vv, vr), k
+    b.close()
+    for ff in [small] + others:
+        ff.close()
