@@ -5,7 +5,7 @@
   (bit-exact; the reference's own cell-list-vs-standard check,
   pairlist.rs:1121-1302, compares the same sets).
 * Forces: RMS relative error sqrt(sum|dF|^2 / sum|F|^2) <= 1e-5 for the
-  fixed-point kernel (BASELINE target), <= 1e-4 for the plain FP32 kernel;
+  fixed-point kernel (the path's accuracy target), <= 1e-4 for the plain FP32 kernel;
   max relative error max|dF_i| / max(|F_i|, 1e-3 RMS|F|) <= 1e-3.
 * Energies (per group and totals) and the virial: relative 1e-5 of the
   largest magnitude in the set (FP32 pair arithmetic).
