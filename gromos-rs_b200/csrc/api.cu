@@ -1267,6 +1267,10 @@ gr_status gr_set_params(gr_ctx* ctx, const gr_nb_params* params) {
 
 gr_status gr_set_box(gr_ctx* ctx, const double box[3]) {
     CTX_GUARD(ctx);
+    if (!box) {
+        set_error("gr_set_box: null box");
+        return GR_ERR_INVALID;
+    }
     if (!ctx->sys.params_set) {
         set_error("gr_set_box before gr_set_params");
         return GR_ERR_STATE;
@@ -1366,6 +1370,10 @@ static gr_status build_reference_lists(gr_ctx* ctx, std::vector<std::pair<int, i
 
 gr_status gr_pairlist_counts(gr_ctx* ctx, int64_t counts[4]) {
     CTX_GUARD(ctx);
+    if (!counts) {
+        set_error("gr_pairlist_counts: null counts");
+        return GR_ERR_INVALID;
+    }
     std::vector<std::pair<int, int>> L[4];
     gr_status st = build_reference_lists(ctx, L);
     if (st) return st;
@@ -1532,6 +1540,10 @@ gr_status gr_ffma_peak(int device, double* ops_per_s) {
 
 gr_status gr_last_timings(gr_ctx* ctx, float ms[5]) {
     CTX_GUARD(ctx);
+    if (!ms) {
+        set_error("gr_last_timings: null ms");
+        return GR_ERR_INVALID;
+    }
     NbSystem& S = ctx->sys;
     if (cudaEventSynchronize(S.ev[4]) != cudaSuccess) {
         set_error("no timed evaluation");

@@ -298,3 +298,17 @@ def test_accuracy_report(kernel):
           f"CRF groups rms, max | virial rms, max | dH/dlambda rel")
     for row in rows:
         print(" | ".join([row[0]] + [f"{v:.2e}" for v in row[1:]]))
+
+
+def test_null_output_arguments_are_rejected():
+    """Entry points given a null output or input array return GR_ERR_INVALID instead of dereferencing it."""
+    from gromos_nb import _lib
+    s = generators.spc_water_system(216, box=generators.box_for_waters(216), seed=3, rcutp=0.8, rcutl=0.9)
+    ff = Forcefield(s)
+    ff.apply(s.pos)
+    L = _lib.lib()
+    for name in ("gr_set_box", "gr_pairlist_counts", "gr_last_timings", "gr_ctx_launches", "gr_forces_device"):
+        assert getattr(L, name)(ff.handle, None) == _lib.GR_ERR_INVALID, name
+    r = ff.apply(s.pos)                          # the context is still usable
+    assert np.isfinite(r["e_lj"])
+    ff.close()
