@@ -529,6 +529,11 @@ gr_status NbSystem::ensure_capacity() {
     }
     int nsolv = NCG - NSCG;
     int maxc = nsolv / W + h.n_cells + 1;
+    // solvent list entries pack (j slot << 8 | i mask) into 32 bits
+    if (static_cast<long long>(maxc) * W > (1LL << 24)) {
+        set_error("pairlist: more than 2^24 solvent cluster slots (about 16.7 M solvent molecules)");
+        return GR_ERR_UNSUPPORTED;
+    }
     if (maxc > clus_alloc) {
         if ((st = alloc(&h.clus_cell, size_t(maxc)))) return st;
         if ((st = alloc(&h.clus_first, size_t(maxc)))) return st;
