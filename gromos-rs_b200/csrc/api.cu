@@ -506,11 +506,17 @@ gr_status NbSystem::set_box(const double box[3]) {
     // within the cutoff lies in the same or an adjacent cell
     double minc = (prm.rcutl + prm.skin) * (1.0 + 1e-7) + 1e-12;
     for (int k = 0; k < 3; ++k) {
-        int g = 1;
-        if (prm.boundary == 1) g = std::max(1, int(std::floor(box[k] / minc)));
-        h.gdim[k] = g;
-        h.cell_size[k] = prm.boundary == 1 ? box[k] / double(g) : 1.0;
+        double g = 1.0;
+        if (prm.boundary == 1) g = std::max(1.0, std::min(std::floor(box[k] / minc), double(1 << 20)));
+        h.gdim[k] = int(g);
     }
+    // a sparse box far larger than the cutoff: coarser cells (still wider than
+    // the cutoff, so the lists are the same) keep the cell count in range
+    while (static_cast<long long>(h.gdim[0]) * h.gdim[1] * h.gdim[2] > (1LL << 24)) {
+        const int k = (h.gdim[0] >= h.gdim[1] && h.gdim[0] >= h.gdim[2]) ? 0 : (h.gdim[1] >= h.gdim[2] ? 1 : 2);
+        h.gdim[k] = (h.gdim[k] + 1) / 2;
+    }
+    for (int k = 0; k < 3; ++k) h.cell_size[k] = prm.boundary == 1 ? box[k] / double(h.gdim[k]) : 1.0;
     h.n_cells = h.gdim[0] * h.gdim[1] * h.gdim[2];
     box_set = true;
     return GR_OK;
