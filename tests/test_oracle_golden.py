@@ -74,3 +74,25 @@ def test_cell_list_matches_standard(name):
         sa = set(map(tuple, np.sort(a[k], axis=1).tolist()))
         sb = set(map(tuple, np.sort(b[k], axis=1).tolist()))
         assert sa == sb, (k, len(sa), len(sb))
+
+
+@pytest.mark.parametrize("case", ["spc1000_single_range", "solute_small_box", "twin_range_solute"])
+def test_cell_list_matches_standard_synthetic(case):
+    """The same set equality on the synthetic shapes the parity tests use: 2 cells per axis (the
+    de-duplicated neighbour path), a box below twice the cutoff with a solute (per-atom images),
+    and a twin-range solvated solute."""
+    from gromos_nb import generators
+    if case == "spc1000_single_range":
+        s = generators.config1_spc1000()
+    elif case == "solute_small_box":
+        s = generators.solvated_solute_system(300, 40, seed=1003, rc=1.4)
+    else:
+        s = generators.solvated_solute_system(900, 60, seed=1005, rc=0.9)
+        s.params.rcutp = 0.6
+    a = ob.pairlist(s, algorithm=0)
+    b = ob.pairlist(s, algorithm=2)
+    for k in range(4):
+        sa = set(map(tuple, np.sort(a[k], axis=1).tolist()))
+        sb = set(map(tuple, np.sort(b[k], axis=1).tolist()))
+        assert sa == sb, (case, k, len(sa), len(sb))
+    assert sum(len(x) for x in a) > 0
