@@ -96,3 +96,29 @@ def test_cell_list_matches_standard_synthetic(case):
         sb = set(map(tuple, np.sort(b[k], axis=1).tolist()))
         assert sa == sb, (case, k, len(sa), len(sb))
     assert sum(len(x) for x in a) > 0
+
+
+@pytest.mark.parametrize("case,lam,nlam", [("ch4_water_fep", 0.2, 1), ("ch4_water_fep", 0.5, 1),
+                                           ("ch4_water_fep", 0.8, 1), ("solute30", 0.1, 1),
+                                           ("solute30", 0.7, 2), ("solute30_twin", 0.4, 3)])
+def test_dhdl_is_the_lambda_derivative_of_the_energy(case, lam, nlam):
+    """The fixtures hold no dH/dlambda, but they pin the energy at lambda 0.5.  The oracle's analytic
+    dH/dlambda (perturbed.rs:123-266, 395-605) must equal the central difference of its own total
+    nonbonded energy in lambda, for NLAM 1-3, single and twin range."""
+    import copy
+    from gromos_nb import generators
+    if case == "ch4_water_fep":
+        s, _ = load_fixture(case)
+    else:
+        s = generators.solvated_solute_system(300, 30, seed=1004, perturbed=True, lam=0.5, rc=1.2)
+        if case == "solute30_twin":
+            s.params.rcutp = 0.8
+    s.params.nlam = nlam
+    h = 1e-5
+    res = []
+    for l in (lam - h, lam, lam + h):
+        t = copy.deepcopy(s)
+        t.params.lam = l
+        res.append(ob.OracleForcefield(t).apply(t.pos))
+    numeric = ((res[2]["e_lj"] + res[2]["e_crf"]) - (res[0]["e_lj"] + res[0]["e_crf"])) / (2 * h)
+    assert abs(res[1]["dhdl"] - numeric) <= 1e-6 * max(abs(numeric), 1.0), (res[1]["dhdl"], numeric)
