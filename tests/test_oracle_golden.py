@@ -122,3 +122,43 @@ def test_dhdl_is_the_lambda_derivative_of_the_energy(case, lam, nlam):
         res.append(ob.OracleForcefield(t).apply(t.pos))
     numeric = ((res[2]["e_lj"] + res[2]["e_crf"]) - (res[0]["e_lj"] + res[0]["e_crf"])) / (2 * h)
     assert abs(res[1]["dhdl"] - numeric) <= 1e-6 * max(abs(numeric), 1.0), (res[1]["dhdl"], numeric)
+
+
+def _strain_derivative(s, a, b, periodic, h=1e-6):
+    """-dE/d(eps_ab) by central differences: positions x -> (I + eps) x, the box scaled with them."""
+    import copy
+    e = []
+    for sign in (-1.0, 1.0):
+        m = np.eye(3)
+        m[a, b] += sign * h
+        t = copy.deepcopy(s)
+        t.pos = s.pos @ m.T
+        if periodic:
+            t.box = s.box * np.diag(m)
+        r = ob.OracleForcefield(t).apply(t.pos)
+        e.append(r["e_lj"] + r["e_crf"])
+    return -(e[1] - e[0]) / (2 * h)
+
+
+def test_virial_is_the_strain_derivative_in_vacuum():
+    """No fixture holds a virial, but the energy is pinned.  For pair forces the virial
+    sum r_a F_b (innerloops.rs:169-210, forcefield.rs:953-1000) is -dE/d(eps_ab) under a homogeneous
+    strain; in vacuum every component can be strained.  Solute-only fixture (the solvent's
+    intramolecular RF terms carry energy without force, excluded.rs:25-112)."""
+    import dataclasses
+    s, _ = load_fixture("water_216_box")
+    s.params = dataclasses.replace(s.params, boundary=0)
+    w = np.asarray(ob.OracleForcefield(s).apply(s.pos)["virial"]).reshape(3, 3)
+    d = np.array([[_strain_derivative(s, a, b, periodic=False) for b in range(3)] for a in range(3)])
+    assert np.abs(w - d).max() <= 1e-6 * np.abs(w).max(), (w, d)
+
+
+@pytest.mark.parametrize("name", ["water_216_box", "water_1000_spc_gridcell"])
+def test_virial_diagonal_is_the_box_strain_derivative(name):
+    """Periodic solute-only fixtures (single and twin range): scaling one box edge with the
+    positions gives the diagonal virial element."""
+    s, _ = load_fixture(name)
+    w = np.asarray(ob.OracleForcefield(s).apply(s.pos)["virial"]).reshape(3, 3)
+    for a in range(3):
+        d = _strain_derivative(s, a, a, periodic=True)
+        assert abs(w[a, a] - d) <= 1e-6 * abs(w[a, a]), (a, w[a, a], d)
