@@ -1456,7 +1456,6 @@ gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out) {
     const bool download = out && !(flags & GR_EVAL_NO_DOWNLOAD);
     gr_status st;
     for (int attempt = 0;; ++attempt) {
-        const bool had_pending = S.pending_check;
         st = (flags & GR_EVAL_GRAPH) ? S.eval_graph(ctx->stream, flags) : S.eval(ctx->stream, flags, true);
         if (st) return st;
         if (!download) return GR_OK;  // overflow (if any) is reported by the next call
@@ -1482,7 +1481,7 @@ gr_status gr_forces_eval(gr_ctx* ctx, int32_t flags, gr_result* out) {
             set_error("pairlist: list capacity could not be grown far enough");
             return GR_ERR_OVERFLOW;
         }
-        (void)had_pending;  // re-run this evaluation with the grown lists
+        // re-run this evaluation with the grown lists
     }
     if (S.last_rebuilt) S.pair_count_valid = false;
     long long ns = 0, nl = 0;
