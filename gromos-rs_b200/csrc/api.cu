@@ -857,8 +857,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             if (NCG > NSCG)
                 GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
             if (NCG > NSCG) {
-                WaterParams wpl = water_params(true);
-                if ((st = launch_water(s, wpl, true))) return st;
+                if ((st = launch_water(s, wp, true))) return st;
             }
             if (NSCG > 0) (++launches, k_solute_force<true><<<sgrid, 128, shg, s>>>(d_sys));
             lr_computed = true;
@@ -1007,11 +1006,12 @@ gr_status NbSystem::eval_graph(cudaStream_t s, int flags) {
     return GR_OK;
 }
 
-// Per-launch constants of the water kernel.  `lim` keeps the FP32 image
-// decision away from half a box edge: 1e-4 nm covers the FP32 rounding of the
-// first-atom vector (short list); per-atom images (long list) also need room
-// for both molecules' extents (0.6 nm covers any 3-site water geometry).
-WaterParams NbSystem::water_params(bool long_range) const {
+// Per-launch constants of the water kernels (both ranges).  `lim` keeps the
+// FP32 image decision away from half a box edge: 1e-4 nm covers the FP32
+// rounding of the first-atom vector (short list); the long-range kernel also
+// subtracts twice the largest molecule extent measured this step, since it
+// images every atom pair.
+WaterParams NbSystem::water_params() const {
     WaterParams wp;
     for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) {

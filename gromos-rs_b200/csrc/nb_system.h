@@ -34,7 +34,7 @@ class NbSystem {
     gr_status push_descriptor(cudaStream_t s);
     cudaError_t record_event(cudaEvent_t e, cudaStream_t s);
     int sm_count();
-    WaterParams water_params(bool long_range = false) const;
+    WaterParams water_params() const;
     gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
     gr_status md_init(const double* mass, const double* vel, const gr_md_params* p);
     gr_status md_run(cudaStream_t s, int n_steps, gr_md_stats* out);
