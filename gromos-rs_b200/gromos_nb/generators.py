@@ -16,7 +16,7 @@ all intra-CG pairs excluded.
 from __future__ import annotations
 
 import math
-from typing import Optional, Tuple
+from typing import Optional
 
 import numpy as np
 

@@ -20,7 +20,6 @@ from __future__ import annotations
 
 import dataclasses
 import math
-import re
 from typing import Dict, List, Optional, TextIO, Tuple
 
 import numpy as np

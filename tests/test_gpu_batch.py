@@ -164,7 +164,6 @@ def standalone_variant(s, seed, n, layout, width):
 
 def test_member_close_leaves_batch():
     """Closing a member removes it from its batch first; the C ABI refuses to destroy a member."""
-    import ctypes as C
     from gromos_nb import _lib
     sy = systems()[:2]
     b = Batch()

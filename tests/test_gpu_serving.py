@@ -8,7 +8,7 @@ import pytest
 
 from gromos_nb import generators as g
 from gromos_nb.nonbonded import Forcefield
-from gromos_nb.serving import Job, NativeServer, Server, poisson_jobs
+from gromos_nb.serving import NativeServer, Server, poisson_jobs
 
 pytestmark = pytest.mark.gpu
 
