@@ -5,7 +5,8 @@ Covers the Metropolis test delta = (beta_1 - beta_2)(E_2 - E_1), accepted
 when a uniform number is below min(1, exp(-delta)) (remd.rs:259-308), the
 odd-even pairing (remd.rs:211-226), the ladder bookkeeping of swapped
 temperatures and the velocity-rescale flag of accepted exchanges
-(replica.rs:355-371).
+(replica.rs:355-371), and the same exchanges with the replicas sharded over
+two gloo ranks.
 """
 import numpy as np
 import pytest
@@ -110,3 +111,60 @@ def test_bad_arguments_are_rejected():
         ReplicaExchange([FakeReplica(0.0), FakeReplica(0.0, n_atoms=6)], [300.0, 310.0], batch=FakeBatch())
     with pytest.raises(ValueError):
         ReplicaExchange([FakeReplica(0.0), FakeReplica(0.0)], [300.0, 310.0], scheme="random", batch=FakeBatch())
+
+
+ENERGIES = [-100.0, -300.0, -50.0, -400.0, -500.0, -20.0]
+LADDER = [300.0, 320.0, 340.0, 360.0, 380.0, 400.0]
+
+
+def _single_process_run():
+    reps = [FakeReplica(e) for e in ENERGIES]
+    rx = ReplicaExchange(reps, LADDER, exchange_interval=10, batch=FakeBatch(), seed=5)
+    rx.run(80)
+    return rx.statistics(), {g: r.set_calls for g, r in enumerate(reps)}
+
+
+def _rank_worker(rank, world, port, q):
+    import datetime
+    import os
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        mine = [g for g in range(len(ENERGIES)) if g % world == rank]     # non-contiguous shards
+        reps = [FakeReplica(ENERGIES[g]) for g in mine]
+        rx = ReplicaExchange(reps, LADDER, exchange_interval=10, batch=FakeBatch(), seed=5, global_ids=mine)
+        rx.run(80)
+        q.put((rank, rx.statistics(), {g: r.set_calls for g, r in zip(mine, reps)}))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_exchange_across_ranks_matches_one_process():
+    """Replicas sharded over two gloo ranks: the energies are summed over the ranks at each attempt,
+    every rank takes the same decisions, and each replica receives the temperatures it would get with
+    all replicas in one process."""
+    import socket
+
+    import torch.multiprocessing as mp
+    want_stats, want_calls = _single_process_run()
+    assert 0 < sum(want_stats["accepts"]) < sum(want_stats["attempts"])   # both outcomes occur
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    calls = {}
+    for _, stats, c in out:
+        assert stats == want_stats
+        calls.update(c)
+    assert calls == want_calls
