@@ -422,8 +422,9 @@ def md_energy_frame(time: float, e_kin: float, e_lj: float, e_crf: float, n_dof:
     2 E_kin / (n_dof k_B); bonded terms, if the caller has them, in ``e_bonded``."""
     boltz = 0.00831446261815324
     pot = e_lj + e_crf + e_bonded
+    denom = n_dof * boltz
     return EnergyFrame(time=time, kinetic=e_kin, potential=pot, total=e_kin + pot,
-                       temperature=2.0 * e_kin / (n_dof * boltz) if n_dof > 0 else 0.0, volume=volume,
+                       temperature=2.0 * e_kin / denom if denom > 0.0 else 0.0, volume=volume,
                        bond=e_bonded, lj=e_lj, coul_real=e_crf)
 
 
