@@ -102,8 +102,9 @@ class ClockSampler:
 
 
 def cpu_baseline_sample(seconds_budget: float = 20.0):
-    """FP64 oracle (threaded fold/reduce) on the host's cores: a bounded sample
-    of the same workload (one rebuild + short-range steps)."""
+    """FP64 oracle on the host's cores, bounded samples of the same workload:
+    threaded (fold/reduce over all cores; the reported value) and serial (one
+    core, one pairlist period; reported beside it)."""
     import oracle_binding as ob
     from gromos_nb import generators
 
@@ -127,10 +128,22 @@ def cpu_baseline_sample(seconds_budget: float = 20.0):
             break
     el = time.perf_counter() - t0 + t_build  # the first pairlist build is part of the work
     orc.close()
+    # the serial mode of the same restatement (one core): one pairlist period
+    t0 = time.perf_counter()
+    orc1 = ob.OracleForcefield(s, nthreads=1)
+    pairs1 = 0
+    for k in range(s.params.nsnb):
+        orc1.apply(s.pos)
+        pairs1 += n_short + (n_long if k == 0 else 0)
+    el1 = time.perf_counter() - t0
+    orc1.close()
     return {"value": pairs / el, "unit": METRIC, "cores": nth, "kind": "port",
-            "sample": f"{steps} Forcefield::apply steps of {WORKLOAD} incl. 1 cell-list pairlist build and "
-                      f"1 long-range refresh, FP64 C++ restatement, {nth} threads",
-            "ms_per_step": 1e3 * el / steps}
+            "sample": f"{steps} Forcefield::apply steps of {WORKLOAD} incl. {-(-steps // s.params.nsnb)} cell-list "
+                      f"pairlist builds and long-range refreshes, FP64 C++ restatement, {nth} threads",
+            "ms_per_step": 1e3 * el / steps,
+            "serial": {"value": pairs1 / el1, "unit": METRIC, "cores": 1, "ms_per_step": 1e3 * el1 / s.params.nsnb,
+                       "sample": f"{s.params.nsnb} Forcefield::apply steps (one pairlist period incl. its build "
+                                 f"and long-range refresh), one thread"}}
 
 
 def run_reference(args, rank, world):
