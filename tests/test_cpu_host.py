@@ -228,3 +228,28 @@ def test_single_atom_solute_md_stays_stable():
                         temperature=300.0, tau=0.1)
     assert st["settle_failures"] == 0
     assert np.all(np.isfinite(x)) and np.all(np.isfinite(v))
+
+
+def test_reference_arm_json_line_and_nonzero_ranks():
+    """`bench.py --impl reference` (the CPU reference arm) prints one JSON line with the bench
+    contract's keys; under torchrun a rank other than 0 exits 0 without work or output."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cmd = [sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "2", "--warmup", "3"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env, check=True).stdout
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in d, key
+    assert d["impl"] == "reference" and d["value"] > 0 and d["config"]["workload"]
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["cores"] >= 1 and d["cpu_baseline"]["kind"] == "port"
+    other = subprocess.run(cmd, capture_output=True, text=True, timeout=120, check=True,
+                           env=dict(env, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1"))
+    assert other.stdout.strip() == ""
