@@ -725,12 +725,8 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
             };
 #define GR_WATER_SEARCH(WW, POP)                                                                            \
     do {                                                                                                    \
-        static int occ = 0;                                                                                 \
-        if (!occ) {                                                                                         \
-            GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_water_search<WW, POP>,            \
-                                                                  kSearchWarps * 32, 0));                   \
-            if (occ < 1) occ = 1;                                                                           \
-        }                                                                                                   \
+        int occ = 1;                                                                                        \
+        GR_CUDA(occupancy(k_water_search<WW, POP>, kSearchWarps * 32, 0, &occ));                            \
         (++launches, k_water_search<WW, POP><<<search_grid(occ), kSearchWarps * 32, 0, s>>>(d_sys, P));     \
     } while (0)
             if (layout == 1)
@@ -1054,23 +1050,14 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
 #define GR_WATER_IT(WW, LJ, LL)                                                                          \
     do {                                                                                                 \
         const size_t smem = water_it_smem<WW>();                                                         \
-        static int occ = 0;                                                                              \
-        if (!occ) {                                                                                      \
-            GR_CUDA(cudaFuncSetAttribute(k_water_force_it<WW, LJ, LL>,                                   \
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));       \
-            GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_water_force_it<WW, LJ, LL>,    \
-                                                                  128, smem));                           \
-            if (occ < 1) occ = 1;                                                                        \
-        }                                                                                                \
+        int occ = 1;                                                                                     \
+        GR_CUDA(occupancy(k_water_force_it<WW, LJ, LL>, 128, smem, &occ));                               \
         (++launches, k_water_force_it<WW, LJ, LL><<<water_grid(sm * occ), 128, smem, s>>>(d_sys, wp));  \
     } while (0)
 #define GR_WATER_SHARED(LJ, LL)                                                                          \
     do {                                                                                                 \
-        static int occ = 0;                                                                              \
-        if (!occ) {                                                                                      \
-            GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_water_force<LJ, LL>, 128, 0)); \
-            if (occ < 1) occ = 1;                                                                        \
-        }                                                                                                \
+        int occ = 1;                                                                                     \
+        GR_CUDA(occupancy(k_water_force<LJ, LL>, 128, 0, &occ));                                         \
         (++launches, k_water_force<LJ, LL><<<water_grid(sm * occ), 128, 0, s>>>(d_sys, wp));            \
     } while (0)
     if (layout == 1) {
@@ -1105,6 +1092,25 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
     }
     GR_CUDA(cudaGetLastError());
     return GR_OK;
+}
+
+template <class K>
+cudaError_t NbSystem::occupancy(K* kernel, int threads, size_t smem, int* occ) {
+    const void* key = reinterpret_cast<const void*>(kernel);
+    for (const auto& e : occ_cache)
+        if (e.first == key) {
+            *occ = e.second;
+            return cudaSuccess;
+        }
+    cudaError_t e;
+    if (smem > 0 && (e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))))
+        return e;
+    int o = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, threads, smem))) return e;
+    if (o < 1) o = 1;
+    occ_cache.emplace_back(key, o);
+    *occ = o;
+    return cudaSuccess;
 }
 
 int NbSystem::sm_count() {
@@ -1655,4 +1661,16 @@ extern "C" gr_status gr_lj_crf_innerloop(const float* positions, const float* ch
     cudaFree(dlj);
     cudaFree(dE);
     return st;
+}
+
+// rust_lj_crf_innerloop_parallel (crates/gromos-core/src/ffi.rs:105-145)
+// delegates to the serial stub in gromos-rs; here both names run the same
+// device evaluation.
+extern "C" gr_status gr_lj_crf_innerloop_parallel(const float* positions, const float* charges, const uint32_t* iac,
+                                                  uint32_t n_atoms, const uint32_t* pairlist, uint32_t n_pairs,
+                                                  const double* lj_params, uint32_t n_types, const double* box_data,
+                                                  uint32_t boundary_type, double crf_cut, double crf_2cut3i,
+                                                  double crf_cut3i, float* forces, double* energies, double* virial) {
+    return gr_lj_crf_innerloop(positions, charges, iac, n_atoms, pairlist, n_pairs, lj_params, n_types, box_data,
+                               boundary_type, crf_cut, crf_2cut3i, crf_cut3i, forces, energies, virial);
 }

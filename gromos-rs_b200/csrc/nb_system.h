@@ -4,6 +4,7 @@
 
 #include <array>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/gromos_nb.h"
@@ -34,6 +35,12 @@ class NbSystem {
     gr_status push_descriptor(cudaStream_t s);
     cudaError_t record_event(cudaEvent_t e, cudaStream_t s);
     int sm_count();
+    // Resident blocks per SM of `kernel` at this launch shape, looked up once
+    // per context: function attributes (the dynamic shared-memory opt-in) and
+    // occupancy belong to the device, and a process may hold contexts on
+    // several GPUs.
+    template <class K>
+    cudaError_t occupancy(K* kernel, int threads, size_t smem, int* occ);
     WaterParams water_params() const;
     gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
     gr_status md_init(const double* mass, const double* vel, const gr_md_params* p);
@@ -110,6 +117,7 @@ class NbSystem {
     gr_status ensure_cgp_capacity();
     gr_status check_errors(cudaStream_t s, bool* retry);
     std::vector<void*> allocs;
+    std::vector<std::pair<const void*, int>> occ_cache;
     int sms_cached = 0;
 };
 

@@ -216,6 +216,13 @@ def read_imd(path: str) -> dict:
     t = _tokens(b["FORCE"])
     negr = int(t[6])
     out["energy_groups_last"] = [int(x) for x in t[7:7 + negr]]
+    if "STEP" in b:
+        t = _tokens(b["STEP"])
+        out["nstlim"], out["dt"] = int(t[0]), float(t[2])
+    if "MULTIBATH" in b:
+        # weak-coupling, NBATHS, then (TEMP0, TAU) of the first bath
+        t = _tokens(b["MULTIBATH"])
+        out["bath_temp0"], out["bath_tau"] = float(t[2]), float(t[3])
     if "PERTURBATION" in b:
         t = _tokens(b["PERTURBATION"])
         out["ntg"], out["rlam"] = int(t[0]), float(t[2])
@@ -359,6 +366,87 @@ def read_forces_step(path: str, step: int = 0) -> np.ndarray:
             return np.asarray(rows)
         i += 1
     raise KeyError(f"step {step} not found in {path}")
+
+
+def read_masses(path: str, nsm: int) -> np.ndarray:
+    """Atom masses: SOLUTEATOM MASS column, then SOLVENTATOM MASS for each of the
+    NSM solvent molecules (gromos-io topology.rs build order)."""
+    blocks = read_blocks(path)
+    masses: List[float] = []
+    if "SOLUTEATOM" in blocks:
+        lines = blocks["SOLUTEATOM"]
+        nrp = int(lines[0].split()[0])
+        k = 1
+        for _ in range(nrp):
+            parts = lines[k].split()
+            k += 1
+            masses.append(float(parts[4]))
+            ine = int(parts[7])
+            seen = len(parts) - 8
+            while seen < ine:
+                seen += len(lines[k].split())
+                k += 1
+            p14 = lines[k].split()
+            k += 1
+            n14, seen = int(p14[0]), len(p14) - 1
+            while seen < n14:
+                seen += len(lines[k].split())
+                k += 1
+    solv: List[float] = []
+    if "SOLVENTATOM" in blocks:
+        ls = blocks["SOLVENTATOM"]
+        for ln in ls[1:1 + int(ls[0].split()[0])]:
+            solv.append(float(ln.split()[3]))
+    return np.asarray(masses + solv * nsm, dtype=np.float64)
+
+
+def read_solvent_constraints(path: str) -> List[Tuple[int, int, float]]:
+    """SOLVENTCONSTR: (i, j, length) with 0-based solvent atom indices."""
+    blocks = read_blocks(path)
+    out: List[Tuple[int, int, float]] = []
+    if "SOLVENTCONSTR" in blocks:
+        ls = blocks["SOLVENTCONSTR"]
+        for ln in ls[1:1 + int(ls[0].split()[0])]:
+            p = ln.split()
+            out.append((int(p[0]) - 1, int(p[1]) - 1, float(p[2])))
+    return out
+
+
+def read_velocities(path: str) -> np.ndarray:
+    """VELOCITY (24 ignored characters per line) or VELOCITYRED block of a configuration."""
+    blocks = read_blocks(path)
+    if "VELOCITY" in blocks:
+        return np.asarray([[float(x) for x in ln[24:].split()[:3]] for ln in blocks["VELOCITY"]])
+    if "VELOCITYRED" in blocks:
+        return np.asarray([[float(x) for x in ln.split()[:3]] for ln in blocks["VELOCITYRED"]])
+    raise KeyError(f"{path}: no VELOCITY block")
+
+
+def read_position_trajectory(path: str) -> Tuple[List[int], List[np.ndarray]]:
+    """(steps, positions) of every TIMESTEP / POSITIONRED frame of a .trc file."""
+    lines = open(path).read().splitlines()
+    steps: List[int] = []
+    frames: List[np.ndarray] = []
+    cur = None
+    i = 0
+    while i < len(lines):
+        s = lines[i].strip()
+        if s == "TIMESTEP":
+            cur = int(lines[i + 1].split()[0])
+            i += 2
+            continue
+        if s == "POSITIONRED":
+            rows = []
+            i += 1
+            while lines[i].strip() != "END":
+                t = lines[i].strip()
+                if t and not t.startswith("#"):
+                    rows.append([float(x) for x in t.split()[:3]])
+                i += 1
+            steps.append(cur)
+            frames.append(np.asarray(rows))
+        i += 1
+    return steps, frames
 
 
 

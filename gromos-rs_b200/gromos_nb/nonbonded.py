@@ -419,12 +419,15 @@ def ffma_peak(device: int = 0) -> float:
     return float(v.value)
 
 
-def lj_crf_innerloop(positions, charges, iac, pairlist, lj_params, crf: CRFParameters, box=None):
+def lj_crf_innerloop(positions, charges, iac, pairlist, lj_params, crf: CRFParameters, box=None,
+                     parallel: bool = False):
     """``lj_crf_innerloop`` over an explicit atom-pair list, on the GPU.
 
     Same arguments as the reference C-ABI stub (ffi.rs:55-103): FP32
     positions/charges, (c6, c12) per type pair, per-atom nearest image
-    (box=None -> vacuum).  Returns (forces (N,3) float32, e_lj, e_crf, virial 3x3).
+    (box=None -> vacuum).  ``parallel`` calls the ``rust_lj_crf_innerloop_parallel``
+    replacement (ffi.rs:105-145) instead.  Returns (forces (N,3) float32, e_lj,
+    e_crf, virial 3x3).
     """
     L = _lib.lib()
     pos = np.ascontiguousarray(positions, dtype=np.float32)
@@ -438,7 +441,7 @@ def lj_crf_innerloop(positions, charges, iac, pairlist, lj_params, crf: CRFParam
     e = np.zeros(2)
     v = np.zeros(9)
     bx = np.ascontiguousarray(box if box is not None else np.zeros(3), dtype=np.float64)
-    fn = L.gr_lj_crf_innerloop
+    fn = L.gr_lj_crf_innerloop_parallel if parallel else L.gr_lj_crf_innerloop
     fn.restype = C.c_int32
     u32 = C.POINTER(C.c_uint32)
     fn.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), u32, C.c_uint32, u32, C.c_uint32,

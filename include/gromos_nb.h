@@ -6,8 +6,7 @@
  * (LJ/CRF) force / energy / virial evaluation, with the soft-core FEP
  * corrections.  Every entry point names the gromos-rs interface it replaces
  * (paths relative to the gromos-rs repository).  A Rust `-sys` crate binds
- * these declarations one to one; ctypes does the same
- * from Python.
+ * these declarations one to one; ctypes does the same from Python.
  *
  * Conventions
  *  - Plain pointers and sizes only.  Host pointers unless a name says
@@ -348,8 +347,9 @@ gr_status gr_server_stats(gr_server* srv, gr_server_stats_t* out);
 /* ---- reference FFI stub replacement ------------------------------------ */
 /* Replaces `rust_lj_crf_innerloop` (crates/gromos-core/src/ffi.rs:55-103):
  * lj_crf_innerloop over an explicit atom-pair list with per-atom nearest
- * image (innerloops.rs:169-210), evaluated on device 0.  lj_params holds
- * (c6, c12) per type pair; q_i*q_j is scaled by four_pi_eps_i = 138.9354
+ * image (innerloops.rs:169-210), evaluated on the calling thread's current
+ * CUDA device (cudaSetDevice before the call selects another GPU).  lj_params
+ * holds (c6, c12) per type pair; q_i*q_j is scaled by four_pi_eps_i = 138.9354
  * (crates/gromos-core/src/units.rs:53); boundary_type 0 vacuum, 1
  * rectangular (2 = triclinic is rejected).  Outputs are overwritten.
  * Returns GR_OK or an error (the stub returned void). */
@@ -358,21 +358,34 @@ gr_status gr_lj_crf_innerloop(const float* positions, const float* charges, cons
                               const double* lj_params, uint32_t n_types, const double* box_data,
                               uint32_t boundary_type, double crf_cut, double crf_2cut3i,
                               double crf_cut3i, float* forces, double* energies, double* virial);
+/* Replaces `rust_lj_crf_innerloop_parallel` (crates/gromos-core/src/ffi.rs:105-145),
+ * which delegates to the serial stub: the same call as gr_lj_crf_innerloop
+ * (the GPU evaluation is parallel either way), same arguments and results. */
+gr_status gr_lj_crf_innerloop_parallel(const float* positions, const float* charges, const uint32_t* iac,
+                                       uint32_t n_atoms, const uint32_t* pairlist, uint32_t n_pairs,
+                                       const double* lj_params, uint32_t n_types, const double* box_data,
+                                       uint32_t boundary_type, double crf_cut, double crf_2cut3i,
+                                       double crf_cut3i, float* forces, double* energies, double* virial);
 
 /* ---- allocation-free variant (no counterpart in gromos-rs) -------------- */
 /* gr_lj_crf_innerloop on DEVICE buffers, enqueued on `stream` (a
  * cudaStream_t; NULL = legacy default stream) of the calling thread's current
  * device, without allocating device memory: for callers that cannot call
- * cudaMalloc while forces are computed (an integrator recorded into a CUDA
- * graph, a loop that must not wait on the allocator, a host program whose
- * device memory belongs to another allocator).  All inputs and outputs are
+ * cudaMalloc while forces are computed (a loop that must not wait on the
+ * allocator's implicit device synchronisation, a host program whose device
+ * memory belongs to another allocator that has reserved the GPU's free
+ * memory).  All inputs and outputs are
  * device pointers with the meaning of gr_lj_crf_innerloop (lj_params is the
  * double (c6, c12) table), except box_data: 3 doubles of host memory, read
  * during the call and passed to the kernel by value.  Its scratch (the FP32 table and the energy /
  * virial accumulators) is one static device array per GPU, sized for at most
  * 64 atom types: n_types > 64 returns GR_ERR_INVALID.  The first call on a
  * device looks the array's address up (cudaGetSymbolAddress) and must come
- * before any stream capture on that device.  forces are cleared by the call;
+ * before any stream capture on that device.  The address is kept for the
+ * life of the process: do not use this entry point on a device after
+ * cudaDeviceReset (or any other destruction of its primary context).  The box
+ * and the CRF constants are taken by value at each call, so a caller whose box
+ * changes passes the new box on every call.  forces are cleared by the call;
  * energies[2] and virial[9] are overwritten.  Pair indices (< n_atoms) and
  * iac values (< n_types) are the caller's to guarantee: they stay on the
  * device and are not checked.  Calls whose work may overlap on the GPU share

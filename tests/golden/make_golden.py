@@ -8,8 +8,12 @@ lines 11-12), the per-energy-group '# nonbonded' block and the step-0
 FREEFORCERED forces.  Step 0 depends only on the input configuration, so
 these are known-answer tests for the nonbonded path.
 
-Usage (only where the reference repository is mounted):
-    python tests/golden/make_golden.py /root/reference
+The MD fixture (nacl_1water_settle: leap-frog + SETTLE, no bath coupling)
+also carries the masses, the initial velocities, the SETTLE lengths, the time
+step and every frame of expected/trajectory.trc plus the final configuration.
+
+Usage (where a gromos-rs checkout is available; its path is required):
+    python tests/golden/make_golden.py <path to the gromos-rs repository>
 """
 from __future__ import annotations
 
@@ -39,7 +43,23 @@ FIXTURES = [
     ("pair_lj_mixed", None, None, None, None),
     ("nacl_pair", None, None, None, None),
     ("nacl_pair_box", None, None, None, None),
+    # 1-4 pairs (INE14) in vacuum; step-0 forces include the bonded terms
+    ("aladip_vacuum", "../shared/aladip.topo", "aladip_vacuum.conf", "aladip_vacuum.in", None),
+    ("butane_vacuum", "butane_vacuum.topo", "butane_vacuum.conf", "butane_vacuum.in", None),
+    # perturbed atoms + a PERTATOMPAIR at lambda 0.125 (input.toml names these inputs)
+    ("aladip_vacuum_fep", "../shared/aladip.topo", "../aladip_vacuum/aladip_vacuum.conf",
+     "aladip_vacuum_fep.in", "../shared/aladip.pttopo"),
+    # leap-frog + SETTLE trajectory (MD fixture)
+    ("nacl_1water_settle", "nacl_1water_settle.topo", "nacl_1water_settle.conf", "nacl_1water_settle.in", None),
 ]
+
+MD_FIXTURES = {"nacl_1water_settle"}
+
+# Fixtures that gromos-rs's own harness marks #[ignore] (the reason is recorded in the .npz)
+REFERENCE_IGNORES = {
+    "aladip_vacuum_fep": "crates/gromos-md/tests/test_gromosXX_references.rs:562 ignores this fixture "
+                         "(PLAN.md: known FEP mismatch with gromosXX)",
+}
 
 
 def _find(d, ext):
@@ -74,17 +94,32 @@ def convert(ref_root: str, name, topo, conf, imd, ptp):
         four_pi_eps_i=t.four_pi_eps_i, params=s.params.__dict__,
         expected_e_lj=ene["e_lj"], expected_e_crf=ene["e_crf"],
         expected_e_covalent=ene["totals"][3], source=f"gromosXX_references/{name}",
+        reference_ignores=REFERENCE_IGNORES.get(name),
     )
+    if name in MD_FIXTURES:
+        imd_d = gromos_io.read_imd(j(imd))
+        steps, frames = gromos_io.read_position_trajectory(os.path.join(base, "expected/trajectory.trc"))
+        fpos, _ = gromos_io.read_configuration(os.path.join(base, "expected/final.conf"))
+        cons = gromos_io.read_solvent_constraints(j(topo))
+        arrays.update(vel=gromos_io.read_velocities(j(conf)), mass=gromos_io.read_masses(j(topo), imd_d["nsm"]),
+                      traj_steps=np.asarray(steps, dtype=np.int32), traj_pos=np.stack(frames),
+                      final_pos=fpos, final_vel=gromos_io.read_velocities(os.path.join(base, "expected/final.conf")))
+        meta.update(dt=imd_d["dt"], nstlim=imd_d["nstlim"], bath_temp0=imd_d["bath_temp0"],
+                    bath_tau=imd_d["bath_tau"], solvent_constraints=cons)
     arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(out, **arrays)
     return out
 
 
-def main(ref_root: str):
+def main(ref_root: str, names=None):
     for fx in FIXTURES:
+        if names and fx[0] not in names:
+            continue
         print(convert(ref_root, *fx))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <gromos-rs repository> [fixture names...]")
+    main(sys.argv[1], set(sys.argv[2:]))

@@ -31,5 +31,10 @@ def load_fixture(name: str):
     s = System(topo=topo, pos=z["pos"].copy(), box=z["box"].copy(), params=params, name=name)
     expected = {"e_lj": meta["expected_e_lj"], "e_crf": meta["expected_e_crf"],
                 "e_covalent": meta["expected_e_covalent"], "forces": z["expected_forces"],
-                "nonbonded_groups": z["expected_nonbonded_groups"]}
+                "nonbonded_groups": z["expected_nonbonded_groups"],
+                "reference_ignores": meta.get("reference_ignores")}
+    if "vel" in z:   # MD fixture: initial velocities, masses, expected trajectory
+        expected["md"] = {k: z[k] for k in ("vel", "mass", "traj_steps", "traj_pos", "final_pos", "final_vel")}
+        expected["md"].update({k: meta[k] for k in ("dt", "nstlim", "bath_temp0", "bath_tau",
+                                                   "solvent_constraints")})
     return s, expected

@@ -60,6 +60,33 @@ def test_md_solvated_solute_vs_oracle():
     check(s, *run_both(s, 12))
 
 
+def test_md_settle_fixture_vs_gromosxx():
+    """nacl_1water_settle (gromosXX leap-frog + SETTLE, no bath, 10 steps of 2 fs) on the device:
+    every written frame and the final configuration within 2e-9 nm of the gromosXX output
+    (9 decimals), final velocities within 1e-8 nm/ps; the oracle reproduces the same file to
+    1e-9 (test_oracle_pins.py), so the device stays within FP32-pair-arithmetic noise of it."""
+    from golden_loader import load_fixture
+    s, ex = load_fixture("nacl_1water_settle")
+    md = ex["md"]
+    cons = {(i, j): d for i, j, d in md["solvent_constraints"]}
+    ff = Forcefield(s)
+    ff.upload_positions(s.pos)
+    ff.md_init(md["mass"], md["vel"], dt=md["dt"], settle=True, dist_oh=cons[(0, 1)], dist_hh=cons[(1, 2)],
+               tau=-1.0)
+    done = 0
+    for step, frame in zip(md["traj_steps"][1:], md["traj_pos"][1:]):
+        st = ff.md_run(int(step) - done)
+        done = int(step)
+        x, v = ff.md_state()
+        assert st["settle_failures"] == 0
+        assert np.abs(x - frame).max() <= 2e-9, (step, np.abs(x - frame).max())
+    ff.md_run(md["nstlim"] - done)
+    x, v = ff.md_state()
+    ff.close()
+    assert np.abs(x - md["final_pos"]).max() <= 2e-9
+    assert np.abs(v - md["final_vel"]).max() <= 1e-8
+
+
 def test_md_split_calls_bit_identical():
     """md_run(7) + md_run(13) == md_run(20) bit for bit (the rebuild cadence carries over)."""
     s = g.spc_water_system(500, box=g.box_for_waters(500), seed=32, rcutp=0.8, rcutl=1.0, nsnb=4)

@@ -22,7 +22,8 @@ from gromos_nb.nonbonded import Forcefield
 pytestmark = pytest.mark.gpu
 
 FIXTURES = ["water_216_box", "water_1000_spc_gridcell", "ch4_water_fep", "nacl_water_box",
-            "water_3_box_twinrange", "water_10_box", "nacl_3water_box", "nacl_pair_box"]
+            "water_3_box_twinrange", "water_10_box", "nacl_3water_box", "nacl_pair_box",
+            "aladip_vacuum", "butane_vacuum", "aladip_vacuum_fep", "nacl_1water_settle"]
 
 
 def sorted_pairs(a):
@@ -128,6 +129,32 @@ def test_spc1000_fixed_and_plain():
     compare_eval(s, "plain", tol_rms=1e-4, tol_e=1e-4)
 
 
+@pytest.mark.parametrize("variant", ["fixture", "charged_pair"])
+@pytest.mark.parametrize("lam", [0.0, 0.125, 0.6, 1.0])
+def test_fep_fixture_one_four_and_atom_pair(variant, lam):
+    """aladip_vacuum_fep: perturbed 1-4 pairs (perturbed.rs:517-605) and the PERTATOMPAIR
+    correction (perturbed.rs:624-707) on the device against the oracle, with the pair's first
+    atom uncharged (as converted) or charged (+0.15 e, so the pair's reaction-field term counts)."""
+    s, _ = load_fixture("aladip_vacuum_fep")
+    assert s.topo.n_pert_pairs == 1 and len(s.topo.normalized().o14) > 0
+    if variant == "charged_pair":
+        s.topo.charge = s.topo.charge.copy()
+        s.topo.charge[int(s.topo.pp_i[0])] = 0.15
+    s.params.lam = lam
+    compare_eval(s, "fixed")
+    compare_eval(s, "plain", tol_rms=1e-4, tol_e=1e-4)
+
+
+def test_spc30000_twin_range_forces_over_a_period():
+    """The bench workload (30,000 SPC waters, 9.65 nm, 0.8/1.4 nm, NSNB 5) against the FP64 oracle
+    over six steps with motion: a rebuild step with the long-range refresh, four short-range steps
+    on the cached long-range forces (forcefield.rs:620-697), and the next rebuild.  Forces RMS
+    <= 1e-5 relative, per-atom max <= 1e-3, energies, energy groups and virial as compare_eval."""
+    s = generators.config2_spc30000()
+    worst = compare_eval(s, "fixed", steps=6, move=0.001, seed=9)
+    assert worst <= 1e-5
+
+
 def test_twin_range_cache_over_steps():
     """Short range every step, long range refreshed every NSNB steps (forcefield.rs:620-697)."""
     s = generators.spc_water_system(2000, box=generators.box_for_waters(2000), seed=21, rcutp=0.8, rcutl=1.4,
@@ -186,35 +213,47 @@ def test_pair_counts_match_oracle_lists():
     ff.close()
 
 
-def test_innerloop_stub_replacement():
-    """gr_lj_crf_innerloop (ffi.rs:55-103 with a body) against the FP64 inner loop."""
+@pytest.mark.parametrize("entry", ["serial", "parallel"])
+def test_innerloop_stub_replacement(entry):
+    """gr_lj_crf_innerloop / gr_lj_crf_innerloop_parallel (ffi.rs:55-145 with a body) against an
+    FP64 loop over the same FP32-rounded inputs: forces RMS <= 1e-5 relative; each energy within
+    1e-5 of the sum of its per-pair magnitudes (the FP32 pair terms are summed in FP64); the
+    parallel name returns the serial name's results (the kernel's FP32 force atomics may differ
+    in order, so within 1e-6 RMS)."""
     from gromos_nb.nonbonded import CRFParameters, lj_crf_innerloop
     s, _ = load_fixture("nacl_water_box")
     lists = ob.pairlist(s, algorithm=0)
     pairs = np.concatenate([lists[0], lists[1], lists[3]])
     crf = CRFParameters.new(s.params.rcutl, 1.0, s.params.epsrf, 0.0)
     lj = s.topo.lj[:, :, :2].copy()
-    f, elj, ecrf, vir = lj_crf_innerloop(s.pos, s.topo.charge, s.topo.iac, pairs, lj, crf, box=s.box)
-    # FP64 reference over the same explicit pairs
+    f, elj, ecrf, vir = lj_crf_innerloop(s.pos, s.topo.charge, s.topo.iac, pairs, lj, crf, box=s.box,
+                                         parallel=(entry == "parallel"))
+    pos32 = s.pos.astype(np.float32).astype(np.float64)
+    q32 = s.topo.charge.astype(np.float32).astype(np.float64)
     fpe = 138.9354
     ref = np.zeros_like(s.pos)
-    e1 = e2 = 0.0
+    e1 = e2 = a1 = a2 = 0.0
     for i, j in pairs:
-        r = s.pos[i] - s.pos[j]
+        r = pos32[i] - pos32[j]
         r -= s.box * np.round(r / s.box)
         r2 = r @ r
         c6, c12 = s.topo.lj[s.topo.iac[i], s.topo.iac[j], :2]
-        q = s.topo.charge[i] * s.topo.charge[j] * fpe
+        q = q32[i] * q32[j] * fpe
         ir2 = 1 / r2
         ir6 = ir2 ** 3
-        e1 += (c12 * ir6 - c6) * ir6
-        e2 += q * (np.sqrt(ir2) - crf.crf_2cut3i * r2 - crf.crf_cut)
+        el = (c12 * ir6 - c6) * ir6
+        ec = q * (np.sqrt(ir2) - crf.crf_2cut3i * r2 - crf.crf_cut)
+        e1, e2, a1, a2 = e1 + el, e2 + ec, a1 + abs(el), a2 + abs(ec)
         fs = (12 * c12 * ir6 - 6 * c6) * ir6 * ir2 + q * (np.sqrt(ir2) * ir2 + crf.crf_cut3i)
         ref[i] += r * fs
         ref[j] -= r * fs
     rms, _ = force_errors(f.astype(np.float64), ref)
-    assert rms < 1e-4
-    assert rel(ecrf, e2) < 1e-4 and rel(elj, e1) < 1e-3
+    assert rms <= 1e-5, rms
+    assert abs(elj - e1) <= 1e-5 * a1 and abs(ecrf - e2) <= 1e-5 * a2, (elj, e1, a1, ecrf, e2, a2)
+    if entry == "parallel":
+        g, gl, gc, gv = lj_crf_innerloop(s.pos, s.topo.charge, s.topo.iac, pairs, lj, crf, box=s.box)
+        assert force_errors(f.astype(np.float64), g.astype(np.float64))[0] <= 1e-6
+        assert abs(gl - elj) <= 1e-6 * a1 and abs(gc - ecrf) <= 1e-6 * a2
 
 
 @pytest.mark.parametrize("kind", ["water", "solute_fep"])
@@ -276,12 +315,14 @@ def _rel_errors(got, ref):
 @pytest.mark.parametrize("kernel", ["fixed", "plain"])
 def test_accuracy_report(kernel):
     """RMS and max relative errors against the FP64 oracle for forces, energy groups, virial and
-    dH/dlambda (1000 SPC waters at 1.4 nm; a solvated perturbed solute at lambda 0.5), printed."""
+    dH/dlambda (1000 SPC waters at 1.4 nm; a solvated perturbed solute at lambda 0.5; the 30,000-water
+    twin-range bench workload at its rebuild step), printed."""
     rows = []
     s1 = generators.config1_spc1000()
     s2 = generators.solvated_solute_system(700, 30, seed=1004, perturbed=True, lam=0.5, rc=1.4)
     s2.params.lam = 0.5
-    for name, s in (("spc1000", s1), ("fep_solute30_lambda0.5", s2)):
+    s3 = generators.config2_spc30000()
+    for name, s in (("spc1000", s1), ("fep_solute30_lambda0.5", s2), ("spc30000_twin_range", s3)):
         ff = Forcefield(s, kernel=kernel)
         r = ff.apply(s.pos)
         o = ob.OracleForcefield(s).apply(s.pos)
