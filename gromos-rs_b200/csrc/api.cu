@@ -370,6 +370,9 @@ gr_status NbSystem::upload(const gr_topology* t) {
                 h.w_qq[a * 4 + b] = float(t->charge[f + a] * t->charge[f + b] * fpe);
                 if ((a || b) && (lj[0] != 0.0 || lj[1] != 0.0)) h.water_lj00_only = 0;
             }
+        double qs = 0.0;  // sum of the charges of one solvent molecule (zero for a neutral one)
+        for (int a = 0; a < aps; ++a) qs += t->charge[f + a];
+        w_qq_sum = qs * qs * fpe;
     }
     if ((st = alloc(&h.pos, size_t(N) * 3))) return st;
     if ((st = alloc(&h.ref, size_t(NCG) * 3))) return st;
@@ -446,9 +449,19 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
         return GR_ERR_INVALID;
     }
     prm = *p;
+    if (p->water_layout == 3 && p->cluster_size == 8) {
+        set_error("gr_nb_params: the pair-stream layout supports cluster_size 4 only");
+        return GR_ERR_INVALID;
+    }
+    if (p->water_layout < 0 || p->water_layout > 3) {
+        set_error("gr_nb_params: water_layout must be 0, 1, 2 or 3");
+        return GR_ERR_INVALID;
+    }
     // water kernel layout: 1 = lanes share the mask bits (width 4 only),
-    // 2 = each lane iterates over its own bits (width 4 or 8)
-    layout = p->water_layout == 1 ? 1 : 2;
+    // 2 = each lane iterates over its own bits (width 4 or 8), 3 = each lane
+    // streams its own water pairs over units of two clusters (width 4; short
+    // range, the long range runs layout 2)
+    layout = p->water_layout == 1 ? 1 : (p->water_layout == 3 ? 3 : 2);
     W = (layout == 2 && p->cluster_size == 8) ? 8 : 4;
     if (p->list_capacity < 0) {
         set_error("gr_nb_params: list_capacity must be >= 0");
@@ -1033,6 +1046,21 @@ WaterParams NbSystem::water_params() const {
     return wp;
 }
 
+// Force constants of the pair-stream kernel: the solvent table with the
+// fixed-point scale 2^32 folded in (a power of two: the scaling is exact).
+WaterScaled NbSystem::water_scaled(const WaterParams& wp) const {
+    WaterScaled pp;
+    const double sc = kForceScale;
+    for (int t = 0; t < 9; ++t) {
+        pp.qf[t] = float(double(wp.qq[t]) * sc);
+        pp.qcf[t] = float(double(wp.qq[t]) * double(h.crf_cut3i_f) * sc);
+        pp.c6f[t] = float(6.0 * double(wp.c6[t]) * sc);
+        pp.c12f[t] = float(12.0 * double(wp.c12[t]) * sc);
+    }
+    pp.crfc_sumq = float(h.crf_cut * w_qq_sum);
+    return pp;
+}
+
 // The water force kernel of the selected layout and width, then the
 // deferred-pair kernel.
 gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr) {
@@ -1052,7 +1080,7 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
         const size_t smem = water_it_smem<WW>();                                                         \
         int occ = 1;                                                                                     \
         GR_CUDA(occupancy(k_water_force_it<WW, LJ, LL>, 128, smem, &occ));                               \
-        (++launches, k_water_force_it<WW, LJ, LL><<<water_grid(sm * occ), 128, smem, s>>>(d_sys, wp));  \
+        (++launches, k_water_force_it<WW, LJ, LL><<<water_grid(sm * occ), 128, smem, s>>>(d_sys, wp, ws)); \
     } while (0)
 #define GR_WATER_SHARED(LJ, LL)                                                                          \
     do {                                                                                                 \
@@ -1060,7 +1088,23 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
         GR_CUDA(occupancy(k_water_force<LJ, LL>, 128, 0, &occ));                                         \
         (++launches, k_water_force<LJ, LL><<<water_grid(sm * occ), 128, 0, s>>>(d_sys, wp));            \
     } while (0)
-    if (layout == 1) {
+    const WaterScaled ws = water_scaled(wp);
+    if (layout == 3 && !lr) {
+        const WaterScaled& pp = ws;
+        const size_t smem = water_ps_smem();
+        int occ = 1;
+        if (lj00) {
+            GR_CUDA(occupancy(k_water_force_ps<true>, kPsWarps * 32, smem, &occ));
+            const long long need = (static_cast<long long>(h.max_clusters + 1) / 2 + kPsWarps - 1) / kPsWarps;
+            const unsigned grid = unsigned(std::max<long long>(1, std::min<long long>(sm * occ, need)));
+            (++launches, k_water_force_ps<true><<<grid, kPsWarps * 32, smem, s>>>(d_sys, wp, pp));
+        } else {
+            GR_CUDA(occupancy(k_water_force_ps<false>, kPsWarps * 32, smem, &occ));
+            const long long need = (static_cast<long long>(h.max_clusters + 1) / 2 + kPsWarps - 1) / kPsWarps;
+            const unsigned grid = unsigned(std::max<long long>(1, std::min<long long>(sm * occ, need)));
+            (++launches, k_water_force_ps<false><<<grid, kPsWarps * 32, smem, s>>>(d_sys, wp, pp));
+        }
+    } else if (layout == 1) {
         if (lj00) {
             if (lr) GR_WATER_SHARED(true, true); else GR_WATER_SHARED(true, false);
         } else {

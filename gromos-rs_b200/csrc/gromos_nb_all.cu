@@ -3,6 +3,7 @@
 #include "pairlist.cu"
 #include "forces.cu"
 #include "water.cu"
+#include "water_ps.cu"
 #include "api.cu"
 #include "md.cu"
 #include "batch.cu"

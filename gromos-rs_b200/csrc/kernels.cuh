@@ -19,12 +19,13 @@ __global__ void k_expand_cgpairs(const SysDev* __restrict__ sys, int long_range)
 
 __global__ void k_water_prep(const SysDev* __restrict__ sys);
 struct WaterParams;
+struct WaterScaled;
 template <bool LJ00, bool LONG>
 __global__ void k_water_force(const SysDev* __restrict__ sys, const WaterParams wp);
 template <bool LJ00, bool LONG>
 __global__ void k_water_deferred(const SysDev* __restrict__ sys, const WaterParams wp);
 template <int W, bool LJ00, bool LONG>
-__global__ void k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp);
+__global__ void k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp, const WaterScaled ws);
 template <bool LONG>
 __global__ void k_solute_force(const SysDev* __restrict__ sys);
 __global__ void k_pos32(const SysDev* __restrict__ sys);

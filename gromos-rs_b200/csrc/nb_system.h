@@ -13,6 +13,7 @@
 namespace gnb {
 
 struct WaterParams;
+struct WaterScaled;
 void set_error(const std::string& m);
 void crf_params(double cutoff, double epsilon, double rf_epsilon, double rf_kappa, double out[4]);
 void lambda_params(double lam, int n, double lp[17]);
@@ -42,6 +43,7 @@ class NbSystem {
     template <class K>
     cudaError_t occupancy(K* kernel, int threads, size_t smem, int* occ);
     WaterParams water_params() const;
+    WaterScaled water_scaled(const WaterParams& wp) const;
     gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
     gr_status md_init(const double* mass, const double* vel, const gr_md_params* p);
     gr_status md_run(cudaStream_t s, int n_steps, gr_md_stats* out);
@@ -53,6 +55,7 @@ class NbSystem {
     int N = 0, NCG = 0, NSCG = 0, NSA = 0, NT = 0, G = 1, aps = 3, W = 4, layout = 2;
     int n_pert = 0, solvent_group = -1;
     double fpe = 138.9354;
+    double w_qq_sum = 0.0;  // sum over a solvent molecule's atom pairs of q_a q_b fpe
     gr_nb_params prm{};
     // host copies needed for list expansion
     std::vector<int> h_cg_off, h_excl_off, h_excl, h_o14_off, h_o14, h_egroup;

@@ -42,10 +42,87 @@ struct WaterParams {
     int G;
 };
 
+// Force constants with the fixed-point scale 2^32 folded in (a power of two, so
+// the scaling is exact): FP32 force sums then convert to fixed point without
+// a multiply.  Energies keep the unscaled constants of WaterParams.
+struct WaterScaled {
+    float qf[9];     // q_a q_b fpe 2^32
+    float qcf[9];    // q_a q_b fpe crf_cut3i 2^32
+    float c6f[9];    // 6 c6 2^32
+    float c12f[9];   // 12 c12 2^32
+    float crfc_sumq; // crf_cut * sum over the 9 atom pairs of q_a q_b fpe (one water pair's constant CRF term)
+};
+
 __device__ __forceinline__ float rsqrt_fast(float x) {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
+}
+
+// The nine atom pairs of one water pair (lj_crf_interaction,
+// innerloops.rs:21-55): x/y/z/r2 hold the atom-pair vectors and squared
+// distances (t = 3 a + b); forces accumulate with FMAs into the i rows f[a]
+// and the j sums g*[b] (forces carry 2^32, energies do not).  The common case
+// is one branch-free block, so that the nine independent chains interleave;
+// an atom pair at r^2 < 1e-10 (zeros in the reference) takes the slow path,
+// which also cancels that pair's share of the CRF constant term.
+template <bool LJ00>
+__device__ __forceinline__ void water_pair_math(const float (&x)[9], const float (&y)[9], const float (&z)[9],
+                                                const float (&r2)[9], float4 (&f)[3], float (&gx)[3], float (&gy)[3],
+                                                float (&gz)[3], float& ecrf, float& elj, const WaterParams& wp,
+                                                const WaterScaled& ws) {
+    float m2 = r2[0];
+#pragma unroll
+    for (int t = 1; t < 9; ++t) m2 = fminf(m2, r2[t]);
+    if (m2 >= 1e-10f) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const int t = a * 3 + b;
+                const float ri = rsqrt_fast(r2[t]);
+                const float ri2 = ri * ri;
+                float fs = fmaf(ws.qf[t], ri2 * ri, ws.qcf[t]);
+                ecrf = fmaf(wp.qq[t], fmaf(-wp.crf2, r2[t], ri), ecrf);
+                if (!LJ00 || t == 0) {
+                    const float ri6 = ri2 * ri2 * ri2;
+                    elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, elj);
+                    fs = fmaf(fmaf(ws.c12f[t], ri6, -ws.c6f[t]), ri6 * ri2, fs);
+                }
+                f[a].x = fmaf(x[t], fs, f[a].x);
+                f[a].y = fmaf(y[t], fs, f[a].y);
+                f[a].z = fmaf(z[t], fs, f[a].z);
+                gx[b] = fmaf(-x[t], fs, gx[b]);
+                gy[b] = fmaf(-y[t], fs, gy[b]);
+                gz[b] = fmaf(-z[t], fs, gz[b]);
+            }
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const int t = a * 3 + b;
+                if (r2[t] < 1e-10f) {
+                    ecrf = fmaf(wp.qq[t], wp.crfc, ecrf);
+                    continue;
+                }
+                const float ri = rsqrt_fast(r2[t]);
+                const float ri2 = ri * ri;
+                float fs = fmaf(ws.qf[t], ri2 * ri, ws.qcf[t]);
+                ecrf = fmaf(wp.qq[t], fmaf(-wp.crf2, r2[t], ri), ecrf);
+                if (!LJ00 || t == 0) {
+                    const float ri6 = ri2 * ri2 * ri2;
+                    elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, elj);
+                    fs = fmaf(fmaf(ws.c12f[t], ri6, -ws.c6f[t]), ri6 * ri2, fs);
+                }
+                f[a].x = fmaf(x[t], fs, f[a].x);
+                f[a].y = fmaf(y[t], fs, f[a].y);
+                f[a].z = fmaf(z[t], fs, f[a].z);
+                gx[b] = fmaf(-x[t], fs, gx[b]);
+                gy[b] = fmaf(-y[t], fs, gy[b]);
+                gz[b] = fmaf(-z[t], fs, gz[b]);
+            }
+    }
 }
 
 struct PairAcc {
@@ -447,7 +524,8 @@ __device__ __forceinline__ void process_deferred(const SysDev& s, const WaterPar
 // shared-memory row (no atomics, so the result does not depend on the order
 // of lanes) and the rows are summed once per cluster.
 template <int W, bool LJ00, bool LONG>
-__global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp) {
+__global__ void __launch_bounds__(128, 3)
+    k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp, const WaterScaled pp) {
     constexpr int ROW = W * 3 + 1;  // float4 per lane row (+1 keeps 8 consecutive lanes on distinct banks)
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31;
@@ -553,6 +631,7 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
             sp[lane] = p;
         }
         float elj = 0.f, ecrf = 0.f, v0s = 0.f, v1s = 0.f, v2s = 0.f, v3s = 0.f, v4s = 0.f, v5s = 0.f;
+        int n_wp = 0;  // water pairs evaluated (the CRF constant term is added per pair at the end)
         uint32_t e_cur_n = 0u, e_nx_n = 0u;
         for (int c = 0; c < nch; ++c) {
             if (c == c_take) take_next();
@@ -629,54 +708,47 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                         }
                         shifted = true;
                     }
-                    float fx[3] = {0.f, 0.f, 0.f}, fy[3] = {0.f, 0.f, 0.f}, fz[3] = {0.f, 0.f, 0.f};
+                    // the i-force row is loaded now and the pair forces accumulate
+                    // into it with FMAs; j-forces likewise into g
+                    float4 f[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) f[a] = myrow[k * 3 + a];
+                    float gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
+                    if (shifted) {
+                        gs0 = gx[0] + gx[1] + gx[2];
+                        gs1 = gy[0] + gy[1] + gy[2];
+                        gs2 = gz[0] + gz[1] + gz[2];
+                    }
+                    float x[9], y[9], z[9], r2[9];
 #pragma unroll
                     for (int a = 0; a < 3; ++a)
 #pragma unroll
                         for (int b = 0; b < 3; ++b) {
                             const int t = a * 3 + b;
-                            const float x = (a == 0 && b == 0) ? r0x : pxk[a] - qx[b];
-                            const float y = (a == 0 && b == 0) ? r0y : pyk[a] - qy[b];
-                            const float z = (a == 0 && b == 0) ? r0z : pzk[a] - qz[b];
-                            const float r2 = fmaf(x, x, fmaf(y, y, z * z));
-                            const float ri = r2 < 1e-10f ? 0.f : rsqrt_fast(r2);
-                            const float ri2 = ri * ri;
-                            const float q = wp.qq[t];
-                            ecrf = fmaf(q, fmaf(-wp.crf2, r2, ri) - wp.crfc, ecrf);
-                            float fs = q * fmaf(ri, ri2, wp.crf3);
-                            if (!LJ00 || t == 0) {
-                                const float ri6 = ri2 * ri2 * ri2;
-                                elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, elj);
-                                fs = fmaf(fmaf(12.f * wp.c12[t], ri6, -6.f * wp.c6[t]), ri6 * ri2, fs);
-                            }
-                            const float fxx = x * fs, fyy = y * fs, fzz = z * fs;
-                            fx[a] += fxx;
-                            fy[a] += fyy;
-                            fz[a] += fzz;
-                            gx[b] -= fxx;
-                            gy[b] -= fyy;
-                            gz[b] -= fzz;
+                            x[t] = (t == 0) ? r0x : pxk[a] - qx[b];
+                            y[t] = (t == 0) ? r0y : pyk[a] - qy[b];
+                            z[t] = (t == 0) ? r0z : pzk[a] - qz[b];
+                            r2[t] = fmaf(x[t], x[t], fmaf(y[t], y[t], z[t] * z[t]));
                         }
+                    water_pair_math<LJ00>(x, y, z, r2, f, gx, gy, gz, ecrf, elj, wp, pp);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) myrow[k * 3 + a] = f[a];
+                    ++n_wp;
                     // virial sum_ab x_ab (x) f_ab = sum_a P_a (x) fi_a + sum_b Q_b (x) g_b
                     // (P, Q: positions relative to the cluster origin): the
                     // i-part is taken once per cluster from the column sums of
-                    // the unshifted P; a shifted image adds shift (x) sum_a fi_a
+                    // the unshifted P; a shifted image adds shift (x) sum_a fi_a,
+                    // which is minus the change of the j sums
                     if (shifted) {
-                        const float sx = fx[0] + fx[1] + fx[2], sy = fy[0] + fy[1] + fy[2], sz = fz[0] + fz[1] + fz[2];
+                        const float sx = gs0 - (gx[0] + gx[1] + gx[2]);
+                        const float sy = gs1 - (gy[0] + gy[1] + gy[2]);
+                        const float sz = gs2 - (gz[0] + gz[1] + gz[2]);
                         v0s = fmaf(shx, sx, v0s);
                         v1s = fmaf(shx, sy, v1s);
                         v2s = fmaf(shx, sz, v2s);
                         v3s = fmaf(shy, sy, v3s);
                         v4s = fmaf(shy, sz, v4s);
                         v5s = fmaf(shz, sz, v5s);
-                    }
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        float4 f = myrow[k * 3 + a];
-                        f.x += fx[a];
-                        f.y += fy[a];
-                        f.z += fz[a];
-                        myrow[k * 3 + a] = f;
                     }
                 }
                 // the j-part of the virial: Q_b (x) g_b, g_b = -sum_a f_ab
@@ -692,18 +764,18 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
                 if (LONG) {
                     long long* __restrict__ st = jst[wid] + lane * 9;
 #pragma unroll
-                    for (int b = 0; b < 3; ++b) {
-                        st[3 * b] = to_fixed_f(gx[b], 4294967296.0f);
-                        st[3 * b + 1] = to_fixed_f(gy[b], 4294967296.0f);
-                        st[3 * b + 2] = to_fixed_f(gz[b], 4294967296.0f);
+                    for (int b = 0; b < 3; ++b) {  // the forces carry the 2^32 scale already
+                        st[3 * b] = __float2ll_rn(gx[b]);
+                        st[3 * b + 1] = __float2ll_rn(gy[b]);
+                        st[3 * b + 2] = __float2ll_rn(gz[b]);
                     }
                 } else {
                     long long* __restrict__ fj = FS + static_cast<size_t>(js) * 9;
 #pragma unroll
                     for (int b = 0; b < 3; ++b) {
-                        red_add(fj + 3 * b, to_fixed_f(gx[b], 4294967296.0f));
-                        red_add(fj + 3 * b + 1, to_fixed_f(gy[b], 4294967296.0f));
-                        red_add(fj + 3 * b + 2, to_fixed_f(gz[b], 4294967296.0f));
+                        red_add(fj + 3 * b, __float2ll_rn(gx[b]));
+                        red_add(fj + 3 * b + 1, __float2ll_rn(gy[b]));
+                        red_add(fj + 3 * b + 2, __float2ll_rn(gz[b]));
                     }
                 }
             }
@@ -748,9 +820,9 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
             }
             if (lane / 3 < n) {
                 long long* __restrict__ fo = FS + static_cast<size_t>(base) * 9 + 3 * lane;
-                red_add(fo, to_fixed_f(sx, 4294967296.0f));
-                red_add(fo + 1, to_fixed_f(sy, 4294967296.0f));
-                red_add(fo + 2, to_fixed_f(sz, 4294967296.0f));
+                red_add(fo, __float2ll_rn(sx));
+                red_add(fo + 1, __float2ll_rn(sy));
+                red_add(fo + 2, __float2ll_rn(sz));
                 // the i-part of the virial: P (x) F for this i atom
                 const float4 P = sp[lane];
                 v0s = fmaf(P.x, sx, v0s);
@@ -765,13 +837,14 @@ __global__ void __launch_bounds__(128, 3) k_water_force_it(const SysDev* __restr
 #pragma unroll
         for (int cc = 0; cc < W * 3; ++cc) myrow[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
         acc[0] += to_fixed_f(elj, 16777216.0f);
-        acc[1] += to_fixed_f(ecrf, 16777216.0f);
-        acc[2] += to_fixed_f(v0s, 16777216.0f);
-        acc[3] += to_fixed_f(v1s, 16777216.0f);
-        acc[4] += to_fixed_f(v2s, 16777216.0f);
-        acc[5] += to_fixed_f(v3s, 16777216.0f);
-        acc[6] += to_fixed_f(v4s, 16777216.0f);
-        acc[7] += to_fixed_f(v5s, 16777216.0f);
+        acc[1] += to_fixed_f(fmaf(-pp.crfc_sumq, float(n_wp), ecrf), 16777216.0f);
+        // the virial sums carry the forces' 2^32; its fixed point is 2^24
+        acc[2] += to_fixed_f(v0s, 0.00390625f);
+        acc[3] += to_fixed_f(v1s, 0.00390625f);
+        acc[4] += to_fixed_f(v2s, 0.00390625f);
+        acc[5] += to_fixed_f(v3s, 0.00390625f);
+        acc[6] += to_fixed_f(v4s, 0.00390625f);
+        acc[7] += to_fixed_f(v5s, 0.00390625f);
         ib ^= 1;
         ci = cn;
         n_cur = n_next;
@@ -834,12 +907,12 @@ template __global__ void k_water_force<false, true>(const SysDev*, const WaterPa
 }  // namespace gnb
 
 namespace gnb {
-template __global__ void k_water_force_it<4, true, false>(const SysDev*, const WaterParams);
-template __global__ void k_water_force_it<4, true, true>(const SysDev*, const WaterParams);
-template __global__ void k_water_force_it<4, false, false>(const SysDev*, const WaterParams);
-template __global__ void k_water_force_it<4, false, true>(const SysDev*, const WaterParams);
-template __global__ void k_water_force_it<8, true, false>(const SysDev*, const WaterParams);
-template __global__ void k_water_force_it<8, true, true>(const SysDev*, const WaterParams);
-template __global__ void k_water_force_it<8, false, false>(const SysDev*, const WaterParams);
-template __global__ void k_water_force_it<8, false, true>(const SysDev*, const WaterParams);
+template __global__ void k_water_force_it<4, true, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, true, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, false, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, false, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, true, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, true, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, false, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, false, true>(const SysDev*, const WaterParams, const WaterScaled);
 }  // namespace gnb

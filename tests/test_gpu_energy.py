@@ -28,7 +28,12 @@ def rel(a, b):
     return abs(a - b) / max(abs(b), 1e-9)
 
 
-@pytest.mark.parametrize("name", [n for n in FIXTURE_NAMES if n != "ch4_water_fep"])
+# single_point_energy has no lambda (crates/gromos-forces/src/energy.rs:96-239): it evaluates the
+# topology's regular charges and types, so the perturbed fixtures are left out
+UNPERTURBED_FIXTURES = [n for n in FIXTURE_NAMES if n not in ("ch4_water_fep", "aladip_vacuum_fep")]
+
+
+@pytest.mark.parametrize("name", UNPERTURBED_FIXTURES)
 def test_single_point_energy_fixtures(name):
     s, ex = load_fixture(name)
     p = s.params
