@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/gromos_nb.h"
@@ -839,7 +840,6 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             GR_CUDA(cudaMemsetAsync(h.n_deferred, 0, 8 * sizeof(int), s));
         }
     }
-    if (NCG > NSCG) GR_CUDA(cudaMemsetAsync(h.fs_short, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
     if (NCG > NSCG && !fs_long_zeroed) {
         // the slot layout changes at rebuilds; keep the long cache consistent
         GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
@@ -852,7 +852,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         WaterParams wp;
         if (NCG > NSCG) {
             wp = water_params();
-            (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 64), 64, 0, s>>>(d_sys));
+            (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 128), 128, 0, s>>>(d_sys));
             if ((st = launch_water(s, wp, false))) return st;
         }
         // solute work items: (CG, chunk of list entries), 4 warps per block
@@ -873,7 +873,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         }
     } else {
         if (NCG > NSCG)  // per-step water data incl. the solvent excluded energies
-            (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 64), 64, 0, s>>>(d_sys));
+            (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 128), 128, 0, s>>>(d_sys));
         (++launches, k_pos32<<<blocks_for(N, 256), 256, 0, s>>>(d_sys));
         GR_CUDA(cudaMemsetAsync(h.f32, 0, size_t(N) * 3 * sizeof(float), s));
         GR_CUDA(cudaMemsetAsync(h.e64, 0, 16 * sizeof(double), s));

@@ -17,7 +17,8 @@
 // the image choice is always the reference's.
 //
 // Kernels:
-//   k_water_prep        per step: FP64 first-atom position + FP32 offsets, slot order
+//   k_water_prep        per step: FP64 first-atom position + FP32 offsets, slot order;
+//                       zeroes the slot force sums, pulls the short lists into L2
 //   (water-water clusters: water.cu)
 //   k_solute_force<..>  solute CG pairs (any CG size <= 8, LJ type table)
 //   k_plain_force       baseline: thread per CG pair, absolute FP32, FP32 atomics
@@ -48,6 +49,9 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     const double* __restrict__ pos = s.pos;
     const double* __restrict__ charge = s.charge;
     WaterRec* __restrict__ wrec = s.wrec;
+    long long* __restrict__ fs_short = s.fs_short;
+    const uint32_t* __restrict__ wl_s = s.wl_s;
+    const int W = s.W, wcap = s.wcap;
     const int nsa = s.n_solute_atoms, nscg = s.n_solute_cg;
     const bool excl = s.excl_atoms < s.n_atoms;
     const bool rect = s.boundary == 1;
@@ -101,6 +105,18 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
                         e_excl += -q3[a] * q3[b] * fpe * crf2 * len2_exact(rx, ry, rz);
                     }
             wrec[slot] = w;
+            // the slot's short-range force sums start at zero for this evaluation
+            // (only slots that hold a water are ever added to or read)
+            long long* __restrict__ fz = fs_short + static_cast<size_t>(slot) * 9;
+#pragma unroll
+            for (int c = 0; c < 9; ++c) fz[c] = 0;
+            // the member k of a cluster pulls line k of the cluster's short list
+            // into L2 for the force kernel (the list was written at the last rebuild)
+            const int k = slot % W;
+            if (32 * k < wcap) {
+                const uint32_t* line = wl_s + static_cast<size_t>(slot / W) * wcap + 32 * k;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+            }
         }
     }
     // one atomicMax per warp (the extents are >= 0, so their bit patterns order like the values)
