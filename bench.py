@@ -184,6 +184,34 @@ def run_reference(args, rank, world):
     return 0
 
 
+def hbm_peak_gbs():
+    """Measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), else the fallback figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def pairlist_summary(s, n_short, n_long, build_ms, total_ms, steps):
+    """The pairlist build on the rebuild steps of the timed region: device time per rebuild
+    (CUDA events around the build, inside the step graph) and its algorithmic bytes per
+    rebuild: the FP64 reference position of every CG read (24 B), cell key and permutation
+    written and read (16 B), CSR offsets (8 B), and one 4-byte j entry per listed CG pair."""
+    ncg = s.topo.n_cg
+    cg_pairs = (n_short + n_long) / 9.0    # water-water CG pairs: 9 atom pairs each
+    nbytes = 48.0 * ncg + 4.0 * cg_pairs
+    peak, src = hbm_peak_gbs()
+    if not build_ms:
+        return None
+    t = statistics.median(build_ms)
+    gbs = nbytes / (t * 1e-3) / 1e9
+    return {"build_us_per_rebuild": 1e3 * t, "rebuilds_timed": len(build_ms),
+            "algorithmic_bytes_per_rebuild": nbytes, "achieved_gbs": gbs, "hbm_peak_gbs": peak,
+            "peak_source": src, "frac_of_hbm": gbs / peak, "traffic": None,
+            "share_of_timed_steps": sum(build_ms) / total_ms if total_ms > 0 else None}
+
+
 def run_md(ff, s, args, generators):
     """MD steps (force evaluation + leap-frog + SETTLE, device resident) for ns/day.
 
@@ -251,7 +279,7 @@ def run_gpu(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    step_ms, short_ms, long_ms = [], [], []
+    step_ms, short_ms, long_ms, build_ms = [], [], [], []
     pairs = 0
     rebuilds = 0
     for k in range(args.steps):
@@ -265,6 +293,7 @@ def run_gpu(args, rank, world, local_rank):
         if rebuild:
             rebuilds += 1
             long_ms.append(t[2])
+            build_ms.append(t[0])
         else:
             short_ms.append(t[1])
         pairs += n_short + (n_long if rebuild else 0)
@@ -331,10 +360,10 @@ def run_gpu(args, rank, world, local_rank):
                             "peak_source": "measured FFMA-chain kernel (gr_ffma_peak), one FFMA = one op",
                             "ops_per_pair": OPS_PER_PAIR, "short_kernel_ms": t_short,
                             "long_kernel_ms": statistics.median(long_ms) if long_ms else None},
+               "pairlist": pairlist_summary(s, n_short, n_long, build_ms, total_ms, args.steps),
                "md": md, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
-        print(json.dumps(out), flush=True)
     ff.close()
-    return 0
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -398,6 +427,32 @@ def _one_by_one(systems, seeds, temps, steps, kernel):
         total_ms += e0.elapsed_time(e1)
         ff.close()
     return total_ms
+
+
+def _jobs_one_by_one(jobs, kernel):
+    """Each serving job alone, from its own start to its last step (device time summed, and wall)."""
+    import torch
+
+    from gromos_nb import generators
+    from gromos_nb.nonbonded import Forcefield
+
+    total_ms = 0.0
+    t0 = time.perf_counter()
+    for job in jobs:
+        ff = Forcefield(job.system, kernel=kernel)
+        ff.upload_positions(job.system.pos)
+        ff.md_init(job.mass, job.vel, dt=job.dt, settle=True, dist_oh=0.1, dist_hh=generators.SPC_DHH,
+                   temperature=job.temperature, tau=job.tau)
+        stream = torch.cuda.ExternalStream(ff.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ff.md_run(job.n_steps)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        ff.close()
+    return total_ms, time.perf_counter() - t0
 
 
 def run_batched(args, kind, rank=0, world=1, local_rank=0):
@@ -465,7 +520,7 @@ def run_batched(args, kind, rank=0, world=1, local_rank=0):
     ms_fixed = _one_by_one(sub, [seeds[i] for i in idx], [temps[i] for i in idx], steps_alone, "fixed")
     ms_plain = _one_by_one(sub, [seeds[i] for i in idx], [temps[i] for i in idx], steps_alone, "plain")
     if rank != 0:
-        return 0
+        return None
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.batch_steps,
             "warmup": 5, "ms_per_step": per_step,
             "ns_per_day": ns_per_day(per_step), "ns_per_day_aggregate": ns_per_day(per_step) * n_members,
@@ -485,8 +540,7 @@ def run_batched(args, kind, rank=0, world=1, local_rank=0):
                    "rollbacks": int(sum(s["rollbacks"] for s in stats))}}
     if out_fep:
         line["fep"] = out_fep
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_serving(args):
@@ -498,10 +552,8 @@ def run_serving(args):
     srv.run(jobs, timeout=1800)
     rep = srv.report()
     srv.close()
-    # the same jobs one by one on the plain kernel: a sample, extrapolated by pairs
-    k = min(len(jobs), args.sample_members)
-    ms_plain = _one_by_one([j.system for j in jobs[:k]], [7 for _ in range(k)], [300.0] * k, 20, "plain")
-    plain_rate = sum(j.pairs_per_step for j in jobs[:k]) * 20 / (ms_plain * 1e-3)
+    # the same jobs one by one on the plain FP32 kernel, every job in full (measured, not extrapolated)
+    ms_plain, wall_plain = _jobs_one_by_one(jobs, "plain")
     total_pairs = sum(j.pairs_per_step * j.n_steps for j in jobs)
     line = {"metric": METRIC, "value": rep["pair_int_per_s"], "unit": METRIC, "n_gpus": 1,
             "steps": rep["batch_steps"], "warmup": 0, "ms_per_step": rep["gpu_ms"] / max(1, rep["batch_steps"]),
@@ -510,10 +562,36 @@ def run_serving(args):
             "config": {"workload": f"serving_{len(jobs)}_jobs_poisson20_spc300-20000_steps100-2000",
                        "hbm_budget_gb": args.hbm_budget_gb, "chunk_steps": 5},
             "serving": rep,
-            "one_by_one_plain": {"sample_jobs": k, "pair_int_per_s": plain_rate,
-                                 "makespan_s_extrapolated": total_pairs / plain_rate}}
-    print(json.dumps(line), flush=True)
-    return 0
+            "one_by_one_plain": {"jobs": len(jobs), "device_s": ms_plain * 1e-3, "wall_s": wall_plain,
+                                 "pair_int_per_s": total_pairs / (ms_plain * 1e-3)}}
+    return line
+
+
+_LINE_KEYS = ("metric", "unit", "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "n_gpus", "warmup")
+
+
+def batched_summary(args):
+    """The batched workloads at bounded size for the default line (one GPU): the 21 FEP
+    lambda windows, 32 of the 256 REMD replicas (same generator and size range), and the
+    serving stream with its one-by-one plain-kernel baseline measured in full."""
+    out = {}
+    t0 = time.perf_counter()
+    a = argparse.Namespace(**vars(args))
+    a.batch_steps, a.sample_members = 100, 4
+    fep = run_batched(a, "fep")
+    a.replicas = 32
+    remd = run_batched(a, "remd")
+    srv = run_serving(args)
+    for name, line in (("fep_21_windows", fep), ("remd_32_replicas", remd), ("serving", srv)):
+        out[name] = {k: v for k, v in line.items() if k not in _LINE_KEYS}
+    for name in ("fep_21_windows", "remd_32_replicas"):
+        o = out[name]
+        o["speedup_vs_plain_one_by_one"] = o["value"] / o["one_by_one"]["plain_pair_int_per_s"]
+        o["speedup_vs_fixed_one_by_one"] = o["value"] / o["one_by_one"]["fixed_pair_int_per_s"]
+    sv = out["serving"]
+    sv["makespan_speedup_vs_plain_one_by_one"] = sv["one_by_one_plain"]["wall_s"] / sv["serving"]["wall_s"]
+    out["seconds"] = time.perf_counter() - t0
+    return out
 
 
 def main():
@@ -536,6 +614,8 @@ def main():
     ap.add_argument("--sample-members", type=int, default=8, help="members timed one by one for comparison")
     ap.add_argument("--jobs", type=int, default=40)
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
+    ap.add_argument("--no-batched", action="store_true",
+                    help="default workload: leave out the batched FEP / REMD / serving sub-object")
     args = ap.parse_args()
     if args.batch_steps is None:
         args.batch_steps = 500 if args.workload == "fep" else 100
@@ -555,12 +635,18 @@ def main():
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
             try:
-                return run_batched(args, args.workload, rank, world, local_rank)
+                line = run_batched(args, args.workload, rank, world, local_rank)
             finally:
                 dist.destroy_process_group()
-        return run_batched(args, args.workload)
+        else:
+            line = run_batched(args, args.workload)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
     if args.workload == "serving":
-        return run_serving(args) if rank == 0 else 0
+        if rank == 0:
+            print(json.dumps(run_serving(args)), flush=True)
+        return 0
     if world > 1:
         import datetime
 
@@ -569,11 +655,16 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        return run_gpu(args, rank, world, local_rank)
+        out = run_gpu(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
+    if out is not None:
+        if world == 1 and not args.no_batched:
+            out["batched"] = batched_summary(args)
+        print(json.dumps(out), flush=True)
+    return 0
 
 
 if __name__ == "__main__":

@@ -119,6 +119,9 @@ void NbSystem::release() {
     md_vel = md_mass = md_inv_mass = md_pos_snap = md_vel_snap = nullptr;
     md_ke = nullptr;
     md_ke_snap = nullptr;
+    md_psnap_pos = md_psnap_vel = nullptr;
+    md_psnap_ke = nullptr;
+    md_psnap_valid = false;
     md_fail = nullptr;
     if (md_err_host) cudaFreeHost(md_err_host);
     md_err_host = nullptr;
@@ -449,7 +452,6 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
         set_error("gr_nb_params: the shared-bit layout supports cluster_size 4 only");
         return GR_ERR_INVALID;
     }
-    prm = *p;
     if (p->water_layout == 3 && p->cluster_size == 8) {
         set_error("gr_nb_params: the pair-stream layout supports cluster_size 4 only");
         return GR_ERR_INVALID;
@@ -458,16 +460,32 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
         set_error("gr_nb_params: water_layout must be 0, 1, 2 or 3");
         return GR_ERR_INVALID;
     }
+    if (p->list_capacity < 0) {
+        set_error("gr_nb_params: list_capacity must be >= 0");
+        return GR_ERR_INVALID;
+    }
+    if (params_set) {
+        // a change of list_capacity alone only re-sizes the list storage at the
+        // next rebuild: the current lists and the rebuild schedule stay
+        const gr_nb_params& o = prm;
+        const bool same = p->rcutp == o.rcutp && p->rcutl == o.rcutl && p->skin == o.skin &&
+                          p->epsilon == o.epsilon && p->epsrf == o.epsrf && p->kappa == o.kappa &&
+                          p->nsnb == o.nsnb && p->boundary == o.boundary && p->lambda == o.lambda &&
+                          p->nlam == o.nlam && p->kernel == o.kernel && p->cluster_size == o.cluster_size &&
+                          p->water_layout == o.water_layout;
+        if (same) {
+            if (p->list_capacity != prm.list_capacity) relist = true;
+            prm.list_capacity = p->list_capacity;
+            return GR_OK;
+        }
+    }
+    prm = *p;
     // water kernel layout: 1 = lanes share the mask bits (width 4 only),
     // 2 = each lane iterates over its own bits (width 4 or 8), 3 = each lane
     // streams its own water pairs over units of two clusters (width 4; short
     // range, the long range runs layout 2)
     layout = p->water_layout == 1 ? 1 : (p->water_layout == 3 ? 3 : 2);
     W = (layout == 2 && p->cluster_size == 8) ? 8 : 4;
-    if (p->list_capacity < 0) {
-        set_error("gr_nb_params: list_capacity must be >= 0");
-        return GR_ERR_INVALID;
-    }
     h.W = W;
     clus_alloc = 0;  // cluster arrays depend on W
     wcap_want = 0;   // list capacity from the (new) parameters
@@ -706,6 +724,11 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
         return GR_ERR_STATE;
     }
     regrow_count = 0;
+    if (relist) {  // list storage sized afresh from the requested capacity
+        wcap_alloc = 0;
+        wcap_want = 0;
+        relist = false;
+    }
     for (;;) {
         gr_status st = ensure_capacity();
         if (st) return st;
@@ -953,6 +976,11 @@ gr_status NbSystem::eval_graph(cudaStream_t s, int flags) {
     }
     // capacities grown after an overflow are allocated before the rebuild
     // graph runs; a reallocation records the graphs again
+    if (rebuild && relist) {  // a list_capacity change: the lists are re-sized (graphs recorded again)
+        wcap_alloc = 0;
+        wcap_want = 0;
+        relist = false;
+    }
     if (rebuild && (st = ensure_capacity())) return st;
     if (g_gen != alloc_gen) {
         drop_graphs();

@@ -488,7 +488,7 @@ namespace {
 struct Variant {
     int layout, width;
 };
-constexpr Variant kVariants[] = {{2, 4}, {2, 8}, {1, 4}};
+constexpr Variant kVariants[] = {{2, 4}, {2, 8}, {1, 4}, {3, 4}};
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
 // `periods` timed pairlist periods of every member, concurrently on their
@@ -601,6 +601,22 @@ gr_status gr_autotune(gr_ctx* ctx, int32_t periods, gr_autotune_result* out) {
     cudaStreamDestroy(s0);
     for (cudaEvent_t e : {fork, join, t0, t1}) cudaEventDestroy(e);
     return st;
+}
+
+gr_status gr_batch_set_variant(gr_batch* b, int32_t water_layout, int32_t cluster_size) {
+    BATCH_GUARD(b);
+    gr_status st;
+    for (auto& mb : b->m) {
+        NbSystem& S = mb.ctx->sys;
+        gr_nb_params p = S.prm;
+        p.water_layout = water_layout;
+        p.cluster_size = cluster_size;
+        if ((st = S.set_params(&p))) return st;
+        S.steps_since_update = S.prm.nsnb;  // the next step rebuilds
+    }
+    for (auto& mb : b->m) mb.offset = int((b->nsnb - b->t % b->nsnb) % b->nsnb);  // every member rebuilds next
+    b->valid = false;
+    return GR_OK;
 }
 
 gr_status gr_batch_autotune(gr_batch* b, int32_t periods, gr_autotune_result* out) {

@@ -223,7 +223,8 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
     if ((st = upload_array(&md_mass, mass, N)) || (st = upload_array(&md_inv_mass, inv.data(), N)) ||
         (st = upload_array(&md_vel, v0.data(), size_t(N) * 3)) || (st = alloc(&md_pos_snap, size_t(N) * 3)) ||
         (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 3)) || (st = alloc(&md_ke_snap, 1)) ||
-        (st = alloc(&md_fail, 1)))
+        (st = alloc(&md_psnap_pos, size_t(N) * 3)) || (st = alloc(&md_psnap_vel, size_t(N) * 3)) ||
+        (st = alloc(&md_psnap_ke, 1)) || (st = alloc(&md_fail, 1)))
         return st;
     {
         double ke0 = 0.0;
@@ -235,6 +236,11 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
     GR_CUDA(cudaMemset(md_fail, 0, sizeof(int)));
     md_steps_total = 0;
     md_rollbacks = 0;
+    md_step_idx = 0;
+    md_psnap_valid = false;
+    // an MD run starts a pairlist period with a build at its first step
+    built = false;
+    lr_computed = false;
     if (!md_err_host) GR_CUDA(cudaMallocHost(&md_err_host, 8 * sizeof(long long)));
     if (!ev_md) GR_CUDA(cudaEventCreateWithFlags(&ev_md, cudaEventDisableTiming));
     mdp = *p;
@@ -316,59 +322,82 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
     // are launched one by one: the host runs ahead of the device, and the
     // recorded step graphs would add their per-step flag copy and timing
     // events (measured slower here).
+    //
+    // The rollback point of a block is its start when the block starts a
+    // pairlist period.  A block that starts inside a period (the previous
+    // call ended there) rolls back to that period's start, kept in md_psnap,
+    // and replays the steps up to the block start: the lists are rebuilt at
+    // the period's own first step, so the rebuild and long-range schedule is
+    // that of a run without overflow, and (the sums being fixed point) the
+    // replayed steps reproduce the block's starting state bit for bit.
     const int kblock = std::max(1, prm.nsnb) * 4;
     int done = 0, attempts = 0, rollbacks = 0;
     gr_status st;
     while (done < n_steps) {
-        // snapshot at the start of the block
-        GR_CUDA(cudaMemcpyAsync(md_pos_snap, h.pos, bytes3, cudaMemcpyDeviceToDevice, s));
-        GR_CUDA(cudaMemcpyAsync(md_vel_snap, md_vel, bytes3, cudaMemcpyDeviceToDevice, s));
-        GR_CUDA(cudaMemcpyAsync(md_ke_snap, md_ke, sizeof(long long), cudaMemcpyDeviceToDevice, s));
         const int ssu0 = steps_since_update;
-        bool overflow = false;
+        const bool from_period = built && ssu0 < prm.nsnb && md_psnap_valid && md_step_idx - md_psnap_step == ssu0;
+        GR_CUDA(cudaMemcpyAsync(md_pos_snap, from_period ? md_psnap_pos : h.pos, bytes3, cudaMemcpyDeviceToDevice, s));
+        GR_CUDA(cudaMemcpyAsync(md_vel_snap, from_period ? md_psnap_vel : md_vel, bytes3, cudaMemcpyDeviceToDevice, s));
+        GR_CUDA(cudaMemcpyAsync(md_ke_snap, from_period ? md_psnap_ke : md_ke, sizeof(long long),
+                                cudaMemcpyDeviceToDevice, s));
+        const long long idx0 = from_period ? md_psnap_step : md_step_idx;
+        int replay = 0;  // steps re-run before the block's own steps (after a rollback)
         int k = 0;
-        for (;;) {
-            if (pending_check) {  // the flags of this period's rebuild
-                bool of = false;
-                if ((st = resolve_pending(&of))) return st;
-                if (of) {
+        for (;;) {  // attempts at this block
+            bool overflow = false;
+            k = 0;
+            for (int r = 0;;) {
+                if (pending_check) {  // the flags of this period's rebuild
+                    bool of = false;
+                    if ((st = resolve_pending(&of))) return st;
+                    if (of) {
+                        overflow = true;
+                        break;
+                    }
+                }
+                if (!built || steps_since_update >= prm.nsnb) {  // this step starts a pairlist period
+                    GR_CUDA(cudaMemcpyAsync(md_psnap_pos, h.pos, bytes3, cudaMemcpyDeviceToDevice, s));
+                    GR_CUDA(cudaMemcpyAsync(md_psnap_vel, md_vel, bytes3, cudaMemcpyDeviceToDevice, s));
+                    GR_CUDA(cudaMemcpyAsync(md_psnap_ke, md_ke, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+                    md_psnap_step = md_step_idx;
+                    md_psnap_valid = true;
+                }
+                if ((st = eval(s, 0, false))) return st;
+                if ((st = md_step_launch(s))) return st;
+                ++md_step_idx;
+                if (r < replay) {
+                    ++r;
+                    continue;
+                }
+                ++k;
+                if (done + k >= n_steps || (steps_since_update >= prm.nsnb && k >= kblock)) break;
+            }
+            if (!overflow) {
+                // everything of this block (builds and force kernels) has set its flags
+                GR_CUDA(cudaMemcpyAsync(md_err_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+                GR_CUDA(cudaEventRecord(ev_md, s));
+                GR_CUDA(cudaEventSynchronize(ev_md));
+                const int* e = reinterpret_cast<const int*>(md_err_host);
+                pending_check = false;  // a rebuild at the block's last step: its flags are in e[0] too
+                if (e[0]) {
+                    const int f = e[0];
+                    GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
+                    if (f & (ERR_CELL_TOO_DENSE | ERR_CG_TOO_LARGE)) {
+                        set_error(f & ERR_CELL_TOO_DENSE ? "pairlist: a grid cell holds more than 2048 charge groups"
+                                                         : "pairlist: solute charge group larger than 8 atoms");
+                        return GR_ERR_UNSUPPORTED;
+                    }
+                    if (f & ERR_WLIST_OVERFLOW) wcap_want = std::max(wcap_want, wcap_alloc) * 2;
+                    if (f & ERR_SLIST_OVERFLOW) scap_want = std::max(scap_want, scap_alloc) * 2;
+                    if (f & ERR_PERT_OVERFLOW) pcap_want = std::max(pcap_want, pcap_alloc) * 2;
+                    if (f & ERR_DEFER_OVERFLOW) {
+                        defer_want = std::max(defer_want, h.defer_cap) * 4;
+                        clus_alloc = 0;
+                    }
                     overflow = true;
-                    break;
                 }
             }
-            if ((st = eval(s, 0, false))) return st;
-            if ((st = md_step_launch(s))) return st;
-            ++k;
-            if (done + k >= n_steps || (steps_since_update >= prm.nsnb && k >= kblock)) break;
-        }
-        if (!overflow) {
-            // everything of this block (builds and force kernels) has set its flags
-            GR_CUDA(cudaMemcpyAsync(md_err_host, h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
-            GR_CUDA(cudaEventRecord(ev_md, s));
-            GR_CUDA(cudaEventSynchronize(ev_md));
-            const int* e = reinterpret_cast<const int*>(md_err_host);
-            if (pending_check) {  // a rebuild at the block's last step: its flags are in e[0] too
-                pending_check = false;
-            }
-            if (e[0]) {
-                const int f = e[0];
-                GR_CUDA(cudaMemset(h.err, 0, 4 * sizeof(int)));
-                if (f & (ERR_CELL_TOO_DENSE | ERR_CG_TOO_LARGE)) {
-                    set_error(f & ERR_CELL_TOO_DENSE ? "pairlist: a grid cell holds more than 2048 charge groups"
-                                                     : "pairlist: solute charge group larger than 8 atoms");
-                    return GR_ERR_UNSUPPORTED;
-                }
-                if (f & ERR_WLIST_OVERFLOW) wcap_want = std::max(wcap_want, wcap_alloc) * 2;
-                if (f & ERR_SLIST_OVERFLOW) scap_want = std::max(scap_want, scap_alloc) * 2;
-                if (f & ERR_PERT_OVERFLOW) pcap_want = std::max(pcap_want, pcap_alloc) * 2;
-                if (f & ERR_DEFER_OVERFLOW) {
-                    defer_want = std::max(defer_want, h.defer_cap) * 4;
-                    clus_alloc = 0;
-                }
-                overflow = true;
-            }
-        }
-        if (overflow) {
+            if (!overflow) break;
             if (++attempts > 8) {
                 set_error("md: list capacity could not be grown far enough");
                 return GR_ERR_OVERFLOW;
@@ -376,11 +405,12 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
             GR_CUDA(cudaMemcpyAsync(h.pos, md_pos_snap, bytes3, cudaMemcpyDeviceToDevice, s));
             GR_CUDA(cudaMemcpyAsync(md_vel, md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, s));
             GR_CUDA(cudaMemcpyAsync(md_ke, md_ke_snap, sizeof(long long), cudaMemcpyDeviceToDevice, s));
-            steps_since_update = ssu0;
-            built = false;  // the block is re-run from a fresh build with the grown lists
+            md_step_idx = idx0;
+            steps_since_update = prm.nsnb;
+            built = false;  // the rollback point starts a period: rebuilt there with the grown lists
             lr_computed = false;
+            replay = from_period ? ssu0 : 0;
             ++rollbacks;
-            continue;
         }
         attempts = 0;
         done += k;

@@ -96,6 +96,13 @@ class NbSystem {
     long long* md_err_host = nullptr;  // pinned
     cudaEvent_t ev_md = nullptr;
     long long md_steps_total = 0, md_rollbacks = 0;
+    // state at the start of the current pairlist period (a rollback point for
+    // a block that starts inside the period) and its MD step index
+    double *md_psnap_pos = nullptr, *md_psnap_vel = nullptr;
+    long long* md_psnap_ke = nullptr;
+    long long md_step_idx = 0, md_psnap_step = 0;
+    bool md_psnap_valid = false;
+    bool relist = false;  // list storage re-sized at the next rebuild (a list_capacity change)
     bool warm = false;        // evaluated at least once with the current parameters
     bool acc_clean = false;   // short-range accumulators and per-step counters are zero
     bool batch_member = false;  // held by a gr_batch (its graphs point at this system)

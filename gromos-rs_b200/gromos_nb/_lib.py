@@ -160,6 +160,7 @@ _SIGNATURES = {
     "gr_server_release": (C.c_int32, [C.c_void_p, C.c_int64]),
     "gr_server_stats": (C.c_int32, [C.c_void_p, C.POINTER(GrServerStats)]),
     "gr_batch_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrAutotuneResult)]),
+    "gr_batch_set_variant": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32]),
     "gr_lj_crf_innerloop_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                                 C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                                 C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,

@@ -127,6 +127,7 @@ class Forcefield:
         self._L = L
         self.system = system
         self.kernel = kernel
+        self.device = device
         h = C.c_void_p()
         check(L.gr_ctx_create(device, C.byref(h)))
         self._h = h
@@ -144,7 +145,8 @@ class Forcefield:
 
     # ---- set-up
     def set_params(self, **changes) -> None:
-        """Change parameters (e.g. ``list_capacity``, ``water_layout``); the next step rebuilds."""
+        """Change parameters (e.g. ``list_capacity``, ``water_layout``); the next step rebuilds,
+        except when only ``list_capacity`` changes (then the new size applies from the next rebuild)."""
         for k, v in changes.items():
             setattr(self._params, k, v)
         check(self._L.gr_set_params(self._h, C.byref(self._params)))
@@ -282,11 +284,22 @@ class Forcefield:
         return {"forces": f, "e_lj": r.e_lj, "e_crf": r.e_crf, "dhdl": r.dhdl,
                 "virial": np.asarray(list(r.virial)).reshape(3, 3), "egroup_lj": glj, "egroup_crf": gcrf}
 
-    def autotune(self, periods: int = 2) -> Dict:
-        """Pick the fastest solvent kernel variant by timing pairlist periods (forces only)."""
-        r = _lib.GrAutotuneResult()
-        check(self._L.gr_autotune(self._h, int(periods), C.byref(r)))
-        return _autotune_dict(r)
+    def autotune(self, periods: int = 2, cache: Optional[str] = None) -> Dict:
+        """Pick the fastest solvent kernel variant by timing pairlist periods (forces only).
+        With ``cache`` (a JSON file path) a choice made earlier for the same system shape on the
+        same kind of GPU is applied without timing, and a new choice is stored."""
+        from . import tuning
+
+        def tune():
+            r = _lib.GrAutotuneResult()
+            check(self._L.gr_autotune(self._h, int(periods), C.byref(r)))
+            return _autotune_dict(r)
+
+        if cache is None:
+            return dict(tune(), cached=False)
+        key = tuning.cache_key(tuning.device_signature(self.device), [tuning.system_signature(self.system)])
+        return tuning.tune_cached(tuning.TuningCache(cache), key, tune,
+                                  lambda layout, width: self.set_params(water_layout=layout, cluster_size=width))
 
     def device_bytes(self) -> int:
         n = C.c_int64(0)
@@ -354,6 +367,7 @@ class Batch:
 
     def __init__(self, device: int = 0):
         self._L = _lib.lib()
+        self.device = device
         h = C.c_void_p()
         check(self._L.gr_batch_create(device, C.byref(h)))
         self._h = h
@@ -382,10 +396,22 @@ class Batch:
         check(self._L.gr_batch_eval(self._h, _lib.GR_EVAL_VIRIAL if virial else 0))
         return self.last_ms()
 
-    def autotune(self, periods: int = 2) -> Dict:
-        r = _lib.GrAutotuneResult()
-        check(self._L.gr_batch_autotune(self._h, int(periods), C.byref(r)))
-        return _autotune_dict(r)
+    def autotune(self, periods: int = 2, cache: Optional[str] = None) -> Dict:
+        """gr_batch_autotune over the members; ``cache`` as in Forcefield.autotune, keyed by the
+        members' system shapes in order."""
+        from . import tuning
+
+        def tune():
+            r = _lib.GrAutotuneResult()
+            check(self._L.gr_batch_autotune(self._h, int(periods), C.byref(r)))
+            return _autotune_dict(r)
+
+        if cache is None:
+            return dict(tune(), cached=False)
+        key = tuning.cache_key(tuning.device_signature(self.device),
+                               [tuning.system_signature(m.system) for m in self.members])
+        return tuning.tune_cached(tuning.TuningCache(cache), key, tune,
+                                  lambda layout, width: check(self._L.gr_batch_set_variant(self._h, layout, width)))
 
     def last_ms(self) -> float:
         ms = C.c_float(0.0)

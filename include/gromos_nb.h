@@ -110,9 +110,12 @@ typedef struct {
     int32_t nlam;                /* NLAM */
     int32_t kernel;              /* GR_KERNEL_* */
     int32_t cluster_size;        /* solvent i-cluster width 4 or 8 (0 = 4) */
-    int32_t water_layout;        /* 0 default, 1 lanes share mask bits (width 4), 2 lanes iterate own bits */
+    int32_t water_layout;        /* 0 default, 1 lanes share mask bits (width 4), 2 lanes iterate own bits,
+                                    3 lanes stream their own water pairs (width 4, short range) */
     int32_t list_capacity;       /* entries per solvent i-cluster list, 0 = sized from the density; a list
-                                    that overflows is grown (doubling) and its step evaluated again */
+                                    that overflows is grown (doubling) and its step evaluated again.  A
+                                    gr_set_params call that changes only this field keeps the current
+                                    lists and rebuild schedule; the new size applies from the next rebuild */
 } gr_nb_params;
 
 /* Results of one evaluation (ForceStorage + Energy, params.rs:100-138). */
@@ -143,7 +146,9 @@ void* gr_ctx_stream(gr_ctx* ctx);
 /* Topology upload: `Forcefield::init` (forcefield.rs:210-223) + LJ matrix
  * conversion (forcefield.rs:173-178) + build_pert_info (:146-170). */
 gr_status gr_system_upload(gr_ctx* ctx, const gr_topology* topo);
-/* CRFParameters::new + PairlistContainer::new + NSNB (md.rs:326-330, 815, 836-841). */
+/* CRFParameters::new + PairlistContainer::new + NSNB (md.rs:326-330, 815, 836-841).
+ * The next evaluation rebuilds the pairlist, unless no field other than
+ * list_capacity changed (then the lists and their schedule stay). */
 gr_status gr_set_params(gr_ctx* ctx, const gr_nb_params* params);
 /* Periodicity refresh from the box (forcefield.rs:243-265); box = 3 edge lengths. */
 gr_status gr_set_box(gr_ctx* ctx, const double box[3]);
@@ -214,9 +219,15 @@ typedef struct {
 } gr_md_stats;
 
 /* masses: n_atoms (all > 0); vel: n_atoms*3 initial v(-dt/2) or NULL (zero).
- * Positions are those of the last gr_positions_upload. */
+ * Positions are those of the last gr_positions_upload.  The run starts a
+ * pairlist period: its first step builds the lists (as the md binary's first
+ * step does). */
 gr_status gr_md_init(gr_ctx* ctx, const double* mass, const double* vel, const gr_md_params* params);
-/* Runs n_steps MD steps on the context's stream; out may be NULL. */
+/* Runs n_steps MD steps on the context's stream; out may be NULL.  A list
+ * overflow rolls the steps back to the start of the affected pairlist period
+ * and re-runs them with grown lists, so the rebuild and long-range schedule
+ * (every NSNB steps from gr_md_init) and the results are those of a run
+ * without overflow, also when a call starts inside a period. */
 gr_status gr_md_run(gr_ctx* ctx, int32_t n_steps, gr_md_stats* out);
 /* New Berendsen reference temperature (an accepted replica exchange); with
  * rescale_velocities the velocities are scaled to t0 from the instantaneous
@@ -255,8 +266,8 @@ gr_status gr_batch_last_ms(gr_batch* b, float* ms);
 gr_status gr_batch_launches(gr_batch* b, int64_t* n);
 /* Autotuner (no counterpart in gromos-rs): times full pairlist periods
  * (rebuild + long-range refresh + NSNB short-range steps) of the system(s)
- * for every solvent kernel variant -- lane layout x i-cluster width -- and
- * keeps the fastest.  NSNB is not tuned: in the reference's twin-range
+ * for every solvent kernel variant -- lane layout x i-cluster width: (2, 4),
+ * (2, 8), (1, 4), (3, 4) -- and keeps the fastest.  NSNB is not tuned: in the reference's twin-range
  * scheme it decides which pairs are evaluated.  Tuning evaluates forces only
  * (positions and velocities are untouched); the next step rebuilds. */
 typedef struct {
@@ -267,6 +278,9 @@ typedef struct {
 } gr_autotune_result;
 gr_status gr_autotune(gr_ctx* ctx, int32_t periods, gr_autotune_result* out);
 gr_status gr_batch_autotune(gr_batch* b, int32_t periods, gr_autotune_result* out);
+/* Applies a solvent kernel variant (e.g. an earlier gr_batch_autotune result kept by the
+ * caller) to every member without timing; every member rebuilds at the next step. */
+gr_status gr_batch_set_variant(gr_batch* b, int32_t water_layout, int32_t cluster_size);
 /* Device bytes held by a context (topology, lists, accumulators, MD state). */
 gr_status gr_ctx_device_bytes(gr_ctx* ctx, int64_t* bytes);
 

@@ -128,7 +128,7 @@ def test_autotune_picks_a_variant_and_keeps_results():
     ff = Forcefield(s)
     ff.upload_positions(s.pos)
     r = ff.autotune(periods=1)
-    assert (r["water_layout"], r["cluster_size"]) in [(2, 4), (2, 8), (1, 4)]
+    assert (r["water_layout"], r["cluster_size"]) in [(2, 4), (2, 8), (1, 4), (3, 4)]
     assert all(c["ms_per_step"] > 0 for c in r["candidates"])
     a = ff.apply(s.pos)
     o = ob.OracleForcefield(s).apply(s.pos)
@@ -140,11 +140,48 @@ def test_autotune_picks_a_variant_and_keeps_results():
     for f in ffs:
         b.add(f)
     rb = b.autotune(periods=1)
-    assert len(rb["candidates"]) == 3
+    assert len(rb["candidates"]) == 4
     b.md_run(6)
     for k, f in enumerate(ffs):
         x, v = f.md_state()
         xr, vr = standalone_variant(systems()[k], 50 + k, 6, rb["water_layout"], rb["cluster_size"])
+        assert np.array_equal(x, xr) and np.array_equal(v, vr)
+    b.close()
+    for f in ffs:
+        f.close()
+
+
+def test_autotune_cache_reuses_the_choice(tmp_path):
+    """A second autotune of the same system shape with the same cache file applies the stored
+    variant without timing (no candidate times), and the forces still match the oracle."""
+    cache = str(tmp_path / "tuning.json")
+    s = g.spc_water_system(1500, box=g.box_for_waters(1500), seed=46, rcutp=0.8, rcutl=1.2, nsnb=5)
+    ff = Forcefield(s)
+    ff.upload_positions(s.pos)
+    r1 = ff.autotune(periods=1, cache=cache)
+    ff.close()
+    s2 = g.spc_water_system(1500, box=g.box_for_waters(1500), seed=47, rcutp=0.8, rcutl=1.2, nsnb=5)
+    ff = Forcefield(s2)
+    ff.upload_positions(s2.pos)
+    r2 = ff.autotune(periods=1, cache=cache)
+    assert r1["cached"] is False and r2["cached"] is True
+    assert (r2["water_layout"], r2["cluster_size"]) == (r1["water_layout"], r1["cluster_size"])
+    a = ff.apply(s2.pos)
+    o = ob.OracleForcefield(s2).apply(s2.pos)
+    d = a["forces"] - o["forces"]
+    assert np.sqrt((d * d).sum() / (o["forces"] ** 2).sum()) <= 1e-5
+    ff.close()
+    b = Batch()
+    ffs = [member(x, 60 + k) for k, x in enumerate(systems()[:2])]
+    for f in ffs:
+        b.add(f)
+    rb1 = b.autotune(periods=1, cache=cache)
+    rb2 = b.autotune(periods=1, cache=cache)
+    assert rb1["cached"] is False and rb2["cached"] is True
+    b.md_run(5)
+    for k, f in enumerate(ffs):
+        x, v = f.md_state()
+        xr, vr = standalone_variant(systems()[k], 60 + k, 5, rb2["water_layout"], rb2["cluster_size"])
         assert np.array_equal(x, xr) and np.array_equal(v, vr)
     b.close()
     for f in ffs:

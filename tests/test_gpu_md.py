@@ -124,6 +124,31 @@ def test_md_rollback_after_list_overflow():
     assert np.sqrt(((vg - vo) ** 2).sum() / (vo ** 2).sum()) <= 1e-4
 
 
+def test_md_rollback_mid_period_keeps_the_schedule():
+    """A call that starts inside a pairlist period (md_run(2), then md_run(11) with NSNB 4) whose
+    lists overflow at the period's next rebuild: the block goes back to the period start, replays
+    the two steps and runs again with grown lists.  Rebuilds stay at steps 1, 5, 9, ... from
+    gr_md_init, so the trajectory equals, bit for bit, the same calls on lists that never overflow."""
+    s = g.spc_water_system(1200, box=g.box_for_waters(1200), seed=33, rcutp=0.8, rcutl=1.2, nsnb=4)
+    m = g.masses(s)
+    v = g.maxwell_velocities(m, 300.0, 8)
+    out = []
+    for tiny in (False, True):
+        ff = Forcefield(s)
+        ff.upload_positions(s.pos)
+        ff.md_init(m, v, dt=0.002, settle=True, dist_oh=0.1, dist_hh=g.SPC_DHH)
+        ff.md_run(2)
+        if tiny:
+            ff.set_params(list_capacity=16)  # only the capacity: the current lists and schedule stay
+        st = ff.md_run(11)
+        out.append((ff.md_state(), st))
+        ff.close()
+    (xa, va), sa = out[0]
+    (xb, vb), sb = out[1]
+    assert sa["rollbacks"] == 0 and sb["rollbacks"] >= 1
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
 def test_md_trajectory_files(tmp_path):
     """Device MD written as ENERTRJ / FREEFORCERED frames and read back unchanged."""
     from gromos_nb import gromos_io as io
