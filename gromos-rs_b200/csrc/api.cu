@@ -836,6 +836,11 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     if ((st = resolve_pending(&overflowed))) return st;
     if (overflowed) lr_computed = false;
     bool rebuild = !built || steps_since_update >= prm.nsnb || (flags & GR_EVAL_FORCE_REBUILD);
+    // stage timing events are recorded kernel by kernel only: inside a recorded
+    // graph each event node adds its own latency to the step, so a graph holds
+    // just the first and last (the step's total device time)
+    const bool stage = record_events && !in_capture;
+    if (stage) last_staged = true;
     if (record_events) GR_CUDA(record_event(ev[0], s));
     if (rebuild) {
         // the first build of a system synchronises to size the list capacities
@@ -848,7 +853,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     }
     last_rebuilt = rebuild;
     steps_since_update += 1;
-    if (record_events) GR_CUDA(record_event(ev[1], s));
+    if (stage) GR_CUDA(record_event(ev[1], s));
     const int NA = acc_size(G);
     // The per-atom short-range accumulators (and the per-step counters) are
     // zeroed by the previous evaluation's k_finalize as it reads them; only
@@ -882,7 +887,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         const unsigned sgrid = std::max(1u, std::min(blocks_for((long long)NSCG * ((h.scap + kSoluteChunk - 1) / kSoluteChunk), 4),
                                                      unsigned(sm * 8)));
         if (NSCG > 0) (++launches, k_solute_force<false><<<sgrid, 128, shg, s>>>(d_sys));
-        if (record_events) GR_CUDA(record_event(ev[2], s));
+        if (stage) GR_CUDA(record_event(ev[2], s));
         if (do_long) {
             GR_CUDA(cudaMemsetAsync(h.f_long, 0, size_t(N) * 3 * sizeof(long long), s));
             GR_CUDA(cudaMemsetAsync(h.acc_long, 0, size_t(NA) * sizeof(long long), s));
@@ -902,7 +907,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         GR_CUDA(cudaMemsetAsync(h.e64, 0, 16 * sizeof(double), s));
         unsigned grid = std::max(1u, std::min(blocks_for(n_cgp_host[0], 256), unsigned(sm * 16)));
         (++launches, k_plain_force<<<grid, 256, 0, s>>>(d_sys, 0));
-        if (record_events) GR_CUDA(record_event(ev[2], s));
+        if (stage) GR_CUDA(record_event(ev[2], s));
         if (do_long) {
             GR_CUDA(cudaMemsetAsync(h.f32_long, 0, size_t(N) * 3 * sizeof(float), s));
             GR_CUDA(cudaMemsetAsync(h.e64_long, 0, 16 * sizeof(double), s));
@@ -911,7 +916,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             lr_computed = true;
         }
     }
-    if (record_events) GR_CUDA(record_event(ev[3], s));
+    if (stage) GR_CUDA(record_event(ev[3], s));
     const size_t sha = size_t(NA) * sizeof(unsigned long long);
     if (h.excl_atoms > 0) (++launches, k_excluded_14<<<blocks_for(h.excl_atoms, 128), 128, sha, s>>>(d_sys));
     if (n_pert > 0) {
@@ -1026,6 +1031,7 @@ gr_status NbSystem::eval_graph(cudaStream_t s, int flags) {
         g_gen = alloc_gen;
     }
     GR_CUDA(cudaGraphLaunch(g_step[rebuild ? 1 : 0], s));
+    last_staged = false;
     GR_CUDA(cudaEventRecord(ev_step, s));
     step_check = true;
     launches += g_step_launches[rebuild ? 1 : 0];
@@ -1637,10 +1643,14 @@ gr_status gr_last_timings(gr_ctx* ctx, float ms[5]) {
         set_error("no timed evaluation");
         return GR_ERR_STATE;
     }
-    cudaEventElapsedTime(&ms[0], S.ev[0], S.ev[1]);
-    cudaEventElapsedTime(&ms[1], S.ev[1], S.ev[2]);
-    cudaEventElapsedTime(&ms[2], S.ev[2], S.ev[3]);
-    cudaEventElapsedTime(&ms[3], S.ev[3], S.ev[4]);
+    if (S.last_staged) {
+        cudaEventElapsedTime(&ms[0], S.ev[0], S.ev[1]);
+        cudaEventElapsedTime(&ms[1], S.ev[1], S.ev[2]);
+        cudaEventElapsedTime(&ms[2], S.ev[2], S.ev[3]);
+        cudaEventElapsedTime(&ms[3], S.ev[3], S.ev[4]);
+    } else {
+        ms[0] = ms[1] = ms[2] = ms[3] = -1.f;  // a graph step: its total only
+    }
     cudaEventElapsedTime(&ms[4], S.ev[0], S.ev[4]);
     return GR_OK;
 }

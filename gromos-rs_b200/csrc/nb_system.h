@@ -118,6 +118,7 @@ class NbSystem {
     cudaEvent_t ev_step = nullptr;
     bool step_check = false;
     bool in_capture = false;  // recording a CUDA graph: the device descriptor is already current
+    bool last_staged = false; // the last timed evaluation recorded its stage events (kernel by kernel)
 
    private:
     template <class T>

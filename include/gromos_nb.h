@@ -184,7 +184,9 @@ gr_status gr_forces_device(gr_ctx* ctx, const double** dev_forces);
 gr_status gr_result_download(gr_ctx* ctx, gr_result* out);
 /* Device-event timing of the last evaluation's stages in ms:
  * [0] pairlist build, [1] short-range force kernels, [2] long-range force
- * kernels, [3] excluded/1-4/FEP terms, [4] total. */
+ * kernels, [3] excluded/1-4/FEP terms, [4] total.  A step replayed from a
+ * recorded graph (GR_EVAL_GRAPH) records only its first and last event (the
+ * step's device time, [4]); [0]-[3] read -1 for it. */
 gr_status gr_last_timings(gr_ctx* ctx, float ms[5]);
 
 /* ---- measurement utilities (no counterpart in gromos-rs) ---------------- */
