@@ -549,6 +549,9 @@ gr_status NbSystem::set_box(const double box[3]) {
         h.gdim[k] = (h.gdim[k] + 1) / 2;
     }
     for (int k = 0; k < 3; ++k) h.cell_size[k] = prm.boundary == 1 ? box[k] / double(h.gdim[k]) : 1.0;
+    // columns of about 0.5 nm (the edge of the volume of four waters) order
+    // the CGs inside a cell, so that W consecutive solvent CGs are compact
+    for (int k = 0; k < 2; ++k) h.ncol[k] = std::max(1, std::min(4, int(h.cell_size[k] / 0.5 + 0.5)));
     h.n_cells = h.gdim[0] * h.gdim[1] * h.gdim[2];
     box_set = true;
     return GR_OK;

@@ -7,7 +7,7 @@
 //   positions  : pos [N*3] f64 (gromos-rs DVec3 layout)
 //   pairlist   : ref [n_cg*3] f64 (COG for solute CGs, first atom for
 //                solvent CGs), cell keys, CGs sorted by (cell, solute-first,
-//                Morton sub-cell, index), solvent i-clusters of W CGs,
+//                column, z, index), solvent i-clusters of W CGs,
 //                per-cluster j-lists of packed (slot << 8 | mask) u32 entries
 //                (short and long separately), per-solute-CG j-lists
 //   per step   : water slots in cluster order: first-atom f64 position and
@@ -69,6 +69,7 @@ struct SysDev {
     // ---- cell grid
     int gdim[3], n_cells;
     double cell_size[3];
+    int ncol[2];         // columns per cell along x and y (order inside a cell)
     // ---- solvent 3x3 parameter table from the first solvent molecule
     //      (innerloops.rs:241-255): c6, c12, q_i q_j fpe
     float w_c6[16], w_c12[16], w_qq[16];

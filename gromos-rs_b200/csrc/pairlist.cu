@@ -36,10 +36,6 @@ __device__ __forceinline__ int cell_coord(double x, double cs, int g, double* fr
     return static_cast<int>(r);
 }
 
-__device__ __forceinline__ unsigned spread3(unsigned v) {  // 3-bit Morton spread
-    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
-}
-
 // Reference positions + cell keys (pairlist.rs:196-198, 577-585, 658-663).
 __global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __restrict__ cg_key) {
     const SysDev& s = sys[blockIdx.y];
@@ -75,13 +71,20 @@ __global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __r
         cz = cell_coord(rz, s.cell_size[2], s.gdim[2], &fz);
     }
     int cell = cx + s.gdim[0] * (cy + s.gdim[1] * cz);
-    unsigned sx3 = min(7u, static_cast<unsigned>(fx * 8.0));
-    unsigned sy3 = min(7u, static_cast<unsigned>(fy * 8.0));
-    unsigned sz3 = min(7u, static_cast<unsigned>(fz * 8.0));
-    unsigned morton = spread3(sx3) | (spread3(sy3) << 1) | (spread3(sz3) << 2);
+    // order inside the cell: ncol[0] x ncol[1] columns visited row by row,
+    // every other row backwards, and z along each column, every other column
+    // downwards (64 levels), so that W consecutive CGs are close together
+    const int ncx = s.ncol[0], ncy = s.ncol[1];
+    int kx = min(ncx - 1, static_cast<int>(fx * ncx));
+    const int ky = min(ncy - 1, static_cast<int>(fy * ncy));
+    if (ky & 1) kx = ncx - 1 - kx;
+    const unsigned col = static_cast<unsigned>(ky * ncx + kx);
+    const unsigned zq = min(63u, static_cast<unsigned>(((col & 1u) ? 1.0 - fz : fz) * 64.0));
+    const unsigned order = (col << 6) | zq;  // 10 bits
     unsigned long long solvent = c >= s.n_solute_cg ? 1ull : 0ull;
-    cg_key[c] = (static_cast<unsigned long long>(cell) << 42) | (solvent << 41) |
-                (static_cast<unsigned long long>(morton) << 32) | static_cast<unsigned>(c);
+    // the cell's bits only label the key (keys are sorted within a cell)
+    cg_key[c] = (static_cast<unsigned long long>(cell) << 43) | (solvent << 42) |
+                (static_cast<unsigned long long>(order) << 32) | static_cast<unsigned>(c);
     s.cg_cell[c] = cell;
     s.cg_slot[c] = -1;
     atomicAdd(&s.cell_count[cell], 1);
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(256) k_cell_sort(const SysDev* __restrict__ sy
         sref[p] = rx;
         sref[stride + p] = ry;
         sref[2 * stride + p] = rz;
-        if (((key >> 41) & 1ull) == 0ull) ++local;
+        if (((key >> 42) & 1ull) == 0ull) ++local;
     }
     if (local) atomicAdd(&nsol, local);
     __syncthreads();
