@@ -566,6 +566,8 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.cell_start, size_t(n) + 1))) return st;
         if ((st = alloc(&h.cell_nsolute, size_t(n)))) return st;
         if ((st = alloc(&h.cell_nclus, size_t(n) + 1))) return st;
+        if ((st = alloc(&h.cell_cand, 2 * size_t(n)))) return st;
+        if ((st = alloc(&h.cell_ncand, 2 * size_t(n)))) return st;
         cells_alloc = n;
     }
     int nsolv = NCG - NSCG;
@@ -582,6 +584,11 @@ gr_status NbSystem::ensure_capacity() {
         if ((st = alloc(&h.slot_cg, size_t(maxc) * W))) return st;
         if ((st = alloc(&h.clus_geo, size_t(maxc)))) return st;
         if ((st = alloc(&h.clus_ext, size_t(maxc)))) return st;
+        // each cluster is a candidate in both lists of its own cell and in one
+        // list of each of its at most 26 neighbour cells
+        h.cand_cap = int(std::min<long long>(28LL * maxc, (1LL << 31) - 1));
+        if ((st = alloc(&h.cand_geo, size_t(h.cand_cap)))) return st;
+        if ((st = alloc(&h.cand_ext, size_t(h.cand_cap)))) return st;
         if ((st = alloc(&h.clus_x64, size_t(maxc) * 4))) return st;
         if ((st = alloc(&h.slot_off, size_t(maxc) * W))) return st;
         if ((st = alloc(&h.wn_s, size_t(maxc)))) return st;
@@ -745,6 +752,7 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
         (++launches, k_scan_clusters<<<1, 1024, 0, s>>>(d_sys));
         (++launches, k_cluster_setup<<<h.n_cells, 128, 0, s>>>(d_sys));
         if (NCG > NSCG) {
+            (++launches, k_cell_candidates<<<dim3(h.n_cells, 2), 256, 0, s>>>(d_sys));
             SearchParams P;
             for (int k = 0; k < 3; ++k) {
                 P.box[k] = h.box[k];

@@ -10,6 +10,7 @@ __global__ void k_scatter(const SysDev* __restrict__ sys, const unsigned long lo
 __global__ void k_cell_sort(const SysDev* __restrict__ sys);
 __global__ void k_scan_clusters(const SysDev* __restrict__ sys);
 __global__ void k_cluster_setup(const SysDev* __restrict__ sys);
+__global__ void k_cell_candidates(const SysDev* __restrict__ sys);
 struct SearchParams;
 template <int W, bool POPSORT>
 __global__ void k_water_search(const SysDev* __restrict__ sys, const SearchParams P);

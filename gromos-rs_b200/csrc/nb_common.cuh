@@ -104,6 +104,11 @@ struct SysDev {
     int* cell_start;           // n_cells+1
     int* cell_nsolute;         // n_cells
     int* cell_nclus;           // n_cells+1 (scanned in place -> cluster start)
+    int* cell_cand;            // 2*n_cells: start of each cell's candidate list per cluster parity
+    int* cell_ncand;           // 2*n_cells: its length
+    float4* cand_geo;          // [cand_cap] candidate j-clusters of the stencil cells: clus_geo
+    float4* cand_ext;          // [cand_cap] clus_ext, .w = the j-cluster index (int bits)
+    int cand_cap;
     int* sorted_cg;            // n_cg: sorted position -> CG
     double* sref;              // [3][n_cg + 2] sorted reference positions (x, y, z planes)
     int* cg_spos;              // n_cg: CG -> sorted position

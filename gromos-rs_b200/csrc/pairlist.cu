@@ -14,6 +14,7 @@
 // Stages: k_refpos (reference positions, cell keys) -> k_scan_cells ->
 // k_scatter -> k_cell_sort (rank sort, per cell, deterministic) ->
 // k_scan_clusters -> k_cluster_setup (solvent i-clusters of W CGs) ->
+// k_cell_candidates (each cell's j-cluster candidates, contiguous) ->
 // k_water_search (water-water j-lists with W-bit masks) and
 // k_solute_search (per solute CG j-lists with exclusion masks) ->
 // k_pert_pairs (explicit perturbed atom pairs for the FEP correction).
@@ -24,6 +25,18 @@ namespace gnb {
 __device__ __forceinline__ int imod(int a, int m) {
     int r = a % m;
     return r < 0 ? r + m : r;
+}
+
+// Cell of stencil lane l (0..26, offsets in z-y-x order, -1..1 per axis;
+// grids of 1 or 2 cells along an axis use the de-duplicated offsets of
+// axis_offsets), -1 for a lane a small grid does not use.  The stencil is
+// symmetric: c is in the stencil of c' iff c' is in the stencil of c.
+__device__ __forceinline__ int stencil_cell(int cell, int l, int gx, int gy, int gz) {
+    const int ix = l % 3, iy = (l / 3) % 3, iz = l / 9;
+    if (ix >= (gx >= 3 ? 3 : gx) || iy >= (gy >= 3 ? 3 : gy) || iz >= (gz >= 3 ? 3 : gz)) return -1;
+    const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
+    const int ox = gx >= 3 ? ix - 1 : ix, oy = gy >= 3 ? iy - 1 : iy, oz = gz >= 3 ? iz - 1 : iz;
+    return imod(cx + ox, gx) + gx * (imod(cy + oy, gy) + gy * imod(cz + oz, gz));
 }
 
 __device__ __forceinline__ int cell_coord(double x, double cs, int g, double* frac) {
@@ -201,6 +214,7 @@ __global__ void k_scan_clusters(const SysDev* __restrict__ sys) {
     __syncthreads();
     if (threadIdx.x == 0) {
         s.n_deferred[6] = 0;  // the water search's cluster counter
+        s.n_deferred[7] = 0;  // the candidate lists' allocation counter
         if (total > s.max_clusters) {
             atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
             total = s.max_clusters;
@@ -288,6 +302,105 @@ __global__ void __launch_bounds__(256) k_cluster_setup(const SysDev* __restrict_
     }
 }
 
+// Grid (n_cells, 2): the candidate list of the water search for the
+// clusters of parity p = blockIdx.y of one cell, the geometry and index of
+// the j-clusters such a cluster can own.  A pair of clusters a < b belongs
+// to a when a + b is even and to b when it is odd.  The list holds the own
+// cell's clusters of parity p (run A; a cluster owns those from itself on),
+// those of parity 1 - p (run B; it owns those before itself), then the
+// owned clusters of the stencil cells: the clusters of another cell lie all
+// before or all after this cell's, so from a cell after this one those of
+// parity p, from a cell before it those of parity 1 - p.  Every cluster thus
+// owns about half of the pairs around it in every direction, and all lists
+// are about equally long.  The lists are placed by an atomic counter: where
+// a list lies does not change what it holds.
+__global__ void __launch_bounds__(256) k_cell_candidates(const SysDev* __restrict__ sys) {
+    const SysDev& s = sys[0];
+    const int cell = blockIdx.x, par = blockIdx.y;
+    constexpr int kSegs = 29;  // runs A and B, 27 stencil lanes
+    __shared__ int seg_lo[kSegs], seg_pre[kSegs + 1];
+    __shared__ int base_s;
+    const int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
+    const int max_clusters = s.max_clusters;
+    if (threadIdx.x < 32) {
+        const int l = threadIdx.x;
+        int lo = 0, len = 0, c0 = 0, c1 = 0, q = 0;
+        if (l < 2) {  // own cell: parity p (A), then 1 - p (B)
+            c0 = s.cell_nclus[cell];
+            c1 = min(s.cell_nclus[cell + 1], max_clusters);
+            q = par + l;
+        } else if (l < kSegs) {
+            const int nc = stencil_cell(cell, l - 2, gx, gy, gz);
+            if (nc >= 0 && nc != cell) {
+                c0 = s.cell_nclus[nc];
+                c1 = min(s.cell_nclus[nc + 1], max_clusters);
+                q = nc > cell ? par : par + 1;
+            }
+        }
+        if (c1 > c0) {
+            lo = c0 + ((c0 - q) & 1);
+            len = lo < c1 ? (c1 - lo + 1) >> 1 : 0;
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (l >= o) incl += y;
+        }
+        if (l < kSegs) {
+            seg_lo[l] = lo;
+            seg_pre[l] = incl - len;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (l == 0) {
+            int n = total;
+            int base = atomicAdd(s.n_deferred + 7, total);
+            if (base + total > s.cand_cap) {
+                atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
+                base = 0;
+                n = 0;
+            }
+            seg_pre[kSegs] = n;
+            base_s = base;
+            s.cell_cand[2 * cell + par] = base;
+            s.cell_ncand[2 * cell + par] = n;
+        }
+    }
+    __syncthreads();
+    const int total = seg_pre[kSegs], base = base_s;
+    const float4* __restrict__ geo = s.clus_geo;
+    const float4* __restrict__ ext = s.clus_ext;
+    float4* __restrict__ cgeo = s.cand_geo + base;
+    float4* __restrict__ cext = s.cand_ext + base;
+    // two entries per thread and pass, loads first
+    for (int v0 = threadIdx.x; v0 < total; v0 += 2 * blockDim.x) {
+        int jc[2];
+        float4 g[2], e[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int v = v0 + u * blockDim.x;
+            jc[u] = -1;
+            if (v < total) {
+                int lo = 0;  // run of v: binary search over the kSegs + 1 offsets
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1)
+                    if (lo + step <= kSegs && seg_pre[lo + step] <= v) lo += step;
+                jc[u] = seg_lo[lo] + 2 * (v - seg_pre[lo]);
+                g[u] = geo[jc[u]];
+                e[u] = ext[jc[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (jc[u] < 0) continue;
+            const int v = v0 + u * blockDim.x;
+            e[u].w = __int_as_float(jc[u]);
+            cgeo[v] = g[u];
+            cext[v] = e[u];
+        }
+    }
+}
+
 // Neighbour cell offsets along one axis, de-duplicated for grids of 1 or 2
 // cells (the reference de-duplicates with a HashSet, pairlist.rs:675-692).
 __device__ __forceinline__ int axis_offsets(int g, int* off) {
@@ -307,20 +420,28 @@ __device__ __forceinline__ int axis_offsets(int g, int* off) {
 }
 
 // Water-water search, one warp per i-cluster (clusters handed out by a
-// counter, so every warp stays busy to the end).  Pair {i_k, j} belongs to
-// this cluster iff j's sorted position is after i_k's, so every unordered CG
-// pair is listed once.  Bit k of the short (long) mask is set when the
+// counter, so every warp stays busy to the end).  Every unordered CG pair is
+// listed once: a pair of two clusters a < b belongs to a when a + b is even,
+// to b when it is odd; a pair inside one cluster to the member that comes
+// first in sorted order.  Each cluster owns about half of the pairs around
+// it in every direction, wherever it sits in its cell, so all lists (and the
+// search's and the force kernels' work per cluster) are about equally long.
+// (Listing a pair under the cluster that comes first in sorted order gives
+// lists of 0 to 2.3 times the mean length.)  Bit k of the short (long) mask is set when the
 // reference test puts (i_k, j) in the short (long) range; the solvent
 // reference point is the first atom for both CGs (pairlist.rs:359-368).
 //
-// The candidates are the j-clusters of the neighbour cells at or after this
-// one; their cluster ranges are concatenated and swept 32 at a time with a
+// The candidates are the owned j-clusters: in the own cell every second
+// cluster (two strided runs), in the stencil cells those of the cell's
+// candidate list for this cluster's parity (k_cell_candidates: geometry and
+// index, contiguous).  They are swept 32 at a time with a
 // conservative FP32 test of the gap between the two clusters' axis-aligned
-// bounding boxes (1e-3 nm margin).  Survivors queue in shared memory in candidate order; for
-// 32 of them at a time the cluster-to-cluster vector C is taken with the FP64
-// image of the two first atoms and rounded once, then lanes classify 32 / W
-// survivors x W members per pass: the pair vector is the i offset + C - the
-// j offset (offsets from the cluster's first atom, FP32).  A squared distance
+// bounding boxes (1e-3 nm margin).  Survivors queue in shared memory in
+// candidate order; lane q takes survivor q of the next 32: the
+// cluster-to-cluster vector C with the FP64 image of the two first atoms,
+// rounded once, then all W x W member pairs, the pair vector being the i
+// offset + C - the j offset (offsets from the cluster's first atom, FP32);
+// the lanes' entries are compacted member by member.  A squared distance
 // within a relative 1e-5 of either cutoff, or a vector near half a box edge
 // (image not certain in FP32), is decided by the exact FP64 test
 // (nearest_image_exact + len2_exact).  The FP32 error is below 1e-6
@@ -402,14 +523,12 @@ __device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restric
 }
 
 template <int W, bool POPSORT>
-__global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
+__global__ void __launch_bounds__(kSearchWarps * 32, W == 4 ? 6 : 4) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    constexpr int kPer = 32 / W;  // survivors per classification pass
     __shared__ uint32_t ebuf_s[kSearchWarps][kEntBuf], ebuf_l[kSearchWarps][kEntBuf];
     __shared__ int q_jc[kSearchWarps][64];          // surviving j-clusters, candidate order
-    __shared__ float4 q_d[kSearchWarps][32 * W];    // per survivor and member: i-first to j-member vector, flags
-    __shared__ int seg_lo[kSearchWarps][32], seg_pre[kSearchWarps][33];
+    __shared__ float q_sp[kSearchWarps][64];        // their offset radii (clus_geo .w)
     const int nclus = s.n_clusters[0];
     const float4* __restrict__ geo = s.clus_geo;
     const float4* __restrict__ ext = s.clus_ext;
@@ -424,7 +543,6 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const Sys
     const float limx = P.boundary ? P.half_boxf[0] - 1e-4f : 3e38f;
     const float limy = P.boundary ? P.half_boxf[1] - 1e-4f : 3e38f;
     const float limz = P.boundary ? P.half_boxf[2] - 1e-4f : 3e38f;
-    const int gx = s.gdim[0], gy = s.gdim[1], gz = s.gdim[2];
     const unsigned below = (1u << lane) - 1u;
     for (;;) {
         int ci = 0;
@@ -442,55 +560,36 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const Sys
             ey[k] = o.y;
             ez[k] = o.z;
         }
-        // neighbour cells at or after this one (lane l < 27 takes stencil
-        // offset l, in z-y-x order; grids of 1 or 2 cells along an axis use
-        // the de-duplicated offsets of axis_offsets) as cluster ranges; the
-        // own cell's range starts at this cluster
-        int total;
-        {
-            const int cx = cell % gx, cy = (cell / gx) % gy, cz = cell / (gx * gy);
-            const int ix = lane % 3, iy = (lane / 3) % 3, iz = lane / 9;
-            const int nx = gx >= 3 ? 3 : gx, ny = gy >= 3 ? 3 : gy, nz = gz >= 3 ? 3 : gz;
-            int lo = 0, len = 0;
-            if (lane < 27 && ix < nx && iy < ny && iz < nz) {
-                const int ox = gx >= 3 ? ix - 1 : ix, oy = gy >= 3 ? iy - 1 : iy, oz = gz >= 3 ? iz - 1 : iz;
-                const int nc = imod(cx + ox, gx) + gx * (imod(cy + oy, gy) + gy * imod(cz + oz, gz));
-                if (nc >= cell) {
-                    lo = nc == cell ? ci : s.cell_nclus[nc];
-                    len = s.cell_nclus[nc + 1] - lo;
-                }
-            }
-            int incl = len;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const unsigned bseg = __ballot_sync(0xffffffffu, len > 0);
-            if (len > 0) {
-                const int r = __popc(bseg & below);
-                seg_lo[w][r] = lo;
-                seg_pre[w][r] = incl - len;
-            }
-            if (lane == 31) seg_pre[w][__popc(bseg)] = incl;
-            total = __shfl_sync(0xffffffffu, incl, 31);
-        }
-        __syncwarp();
+        // candidates, from the list of this cell and parity: run A from ci
+        // on (ci itself for its internal pairs), run B before ci, then the
+        // stencil cells' clusters
+        const int oc0 = s.cell_nclus[cell], oc1 = min(s.cell_nclus[cell + 1], s.max_clusters);
+        const int a0 = oc0 + ((oc0 - ci) & 1), b0 = oc0 + ((oc0 - ci - 1) & 1);
+        const int len_a = (oc1 - a0 + 1) >> 1, len_b = b0 < oc1 ? (oc1 - b0 + 1) >> 1 : 0;
+        const int skip_a = (ci - a0) >> 1;                       // A entries before ci
+        const int nb = b0 < ci ? (ci - b0 + 1) >> 1 : 0;         // B entries before ci
+        const int n_ab = len_a - skip_a + nb;                     // own-cell candidates
+        const int skip_ab = skip_a + len_b - nb;                  // + B entries after ci
+        const int lidx = 2 * cell + (ci & 1);
+        const int total = s.cell_ncand[lidx] - skip_ab;
+        const float4* __restrict__ cgeo = s.cand_geo + s.cell_cand[lidx];
+        const float4* __restrict__ cext = s.cand_ext + s.cell_cand[lidx];
         uint32_t* outs = s.wl_s + static_cast<size_t>(ci) * P.wcap;
         uint32_t* outl = s.wl_l + static_cast<size_t>(ci) * P.wcap;
-        int cnt_s = 0, cnt_l = 0, qn = 0, v0 = 0, sg = 0;
+        int cnt_s = 0, cnt_l = 0, qn = 0, v0 = 0;
         for (;;) {
             // sphere tests until 32 survivors are queued or the candidates end
             while (v0 < total && qn < 32) {
-                while (seg_pre[w][sg + 1] <= v0) ++sg;
                 const int v = v0 + lane;
                 bool surv = false;
                 int jc = 0;
+                float rj = 0.f;
                 if (v < total) {
-                    int g = sg;
-                    while (seg_pre[w][g + 1] <= v) ++g;
-                    jc = min(seg_lo[w][g] + (v - seg_pre[w][g]), nclus - 1);
-                    const float4 gj = geo[jc], hj = ext[jc];
+                    // list position: skip A's entries before ci, and B's after it
+                    const int pos = v + (v < n_ab ? skip_a : skip_ab);
+                    const float4 gj = cgeo[pos], hj = cext[pos];
+                    jc = min(max(__float_as_int(hj.w), 0), nclus - 1);
+                    rj = gj.w;
                     float dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
                     if (P.boundary) {
                         dx -= P.boxf[0] * rintf(dx * P.inv_boxf[0]);
@@ -504,22 +603,27 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const Sys
                     surv = dx * dx + dy * dy + dz * dz <= rcl * rcl;
                 }
                 const unsigned b = __ballot_sync(0xffffffffu, surv);
-                if (surv) q_jc[w][qn + __popc(b & below)] = jc;
+                if (surv) {
+                    q_jc[w][qn + __popc(b & below)] = jc;
+                    q_sp[w][qn + __popc(b & below)] = rj;
+                }
                 qn += __popc(b);
                 v0 += 32;
             }
             if (qn == 0) break;
             const int nq = min(qn, 32);
             __syncwarp();
-            // per survivor: the cluster-to-cluster vector C (FP64 image of the
-            // first atoms, rounded once) and, per member m, C - offset_m
-            if (lane < nq) {
-                const int jc = q_jc[w][lane];
-                const int n_j = s.clus_n[jc];
-                const float span = gi.w + geo[jc].w;
-                float4 o[W];
+            // lane q classifies survivor q: the cluster-to-cluster vector C
+            // (FP64 image of the first atoms, rounded once), then per member
+            // m the W x W pair vectors i offset + C - j offset (FP32)
+            int jc = 0;
+            unsigned ms[W], ml[W], am[W];
 #pragma unroll
-                for (int m = 0; m < W; ++m) o[m] = soff[jc * W + m];
+            for (int m = 0; m < W; ++m) ms[m] = ml[m] = am[m] = 0u;
+            if (lane < nq) {
+                jc = q_jc[w][lane];
+                const int n_j = s.clus_n[jc];
+                const float span = gi.w + q_sp[w][lane];
                 double cdx = X0 - x64[4 * jc], cdy = Y0 - x64[4 * jc + 1], cdz = Z0 - x64[4 * jc + 2];
                 if (P.boundary) {
                     cdx -= P.box[0] * rint(cdx * P.inv_box[0]);
@@ -532,58 +636,55 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const Sys
                 // minimum image of every member pair
                 const bool edge = P.boundary && !(fabsf(Cx) + span < limx && fabsf(Cy) + span < limy &&
                                                   fabsf(Cz) + span < limz);
+                // pairs {i_k, j_m} with k < n_i, m < n_j and i_k before j_m in sorted order
+                const unsigned valid_i = (1u << n_i) - 1u;
 #pragma unroll
                 for (int m = 0; m < W; ++m) {
-                    float Dx = Cx - o[m].x, Dy = Cy - o[m].y, Dz = Cz - o[m].z;
+                    const float4 o = soff[jc * W + m];
+                    float Dx = Cx - o.x, Dy = Cy - o.y, Dz = Cz - o.z;
                     if (edge) {  // the sum of two minimum images need not be one
                         Dx -= P.boxf[0] * rintf(Dx * P.inv_boxf[0]);
                         Dy -= P.boxf[1] * rintf(Dy * P.inv_boxf[1]);
                         Dz -= P.boxf[2] * rintf(Dz * P.inv_boxf[2]);
                     }
-                    const int flags = (m < n_j ? 1 : 0) | (edge ? 2 : 0);
-                    q_d[w][lane * W + m] = make_float4(Dx, Dy, Dz, __int_as_float(flags));
+                    unsigned valid = m < n_j ? valid_i : 0u;
+                    if (jc == ci) valid &= (1u << m) - 1u;
+                    unsigned s_m = 0, l_m = 0, a_m = 0;
+#pragma unroll
+                    for (int k = 0; k < W; ++k) {
+                        const float kx = ex[k] + Dx, ky = ey[k] + Dy, kz = ez[k] + Dz;
+                        const float d2 = kx * kx + ky * ky + kz * kz;
+                        s_m |= unsigned(d2 < s_lo) << k;
+                        l_m |= unsigned(d2 > s_hi && d2 < l_lo) << k;
+                        a_m |= unsigned((d2 >= s_lo && d2 <= s_hi) || (d2 >= l_lo && d2 <= l_hi)) << k;
+                        if (edge) {
+                            const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
+                            a_m |= unsigned(!inbox) << k;
+                        }
+                    }
+                    ms[m] = s_m & valid & ~a_m;
+                    ml[m] = l_m & valid & ~a_m;
+                    am[m] = a_m & valid;
                 }
             }
-            __syncwarp();
-            for (int p0 = 0; p0 < nq; p0 += kPer) {
-                const int q = p0 + lane / W, m = lane % W;
-                unsigned ms = 0, ml = 0, amb = 0;
-                int jc = 0;
-                if (q < nq) {
-                    jc = q_jc[w][q];
-                    const float4 D = q_d[w][q * W + m];
-                    const int flags = __float_as_int(D.w);
-                    if (flags & 1) {
-                        const bool edge = flags & 2;
-                        // pairs {i_k, j_m} with k < n_i and i_k before j_m in sorted order
-                        unsigned valid = (1u << n_i) - 1u;
-                        if (jc == ci) valid &= (1u << m) - 1u;
+            // the rare ambiguous pairs: the exact FP64 decision
+            // (nearest_image_exact + len2_exact, box from the kernel
+            // parameters) for the lanes that have some
+            unsigned any_am = 0u;
 #pragma unroll
-                        for (int k = 0; k < W; ++k) {
-                            const float kx = ex[k] + D.x, ky = ey[k] + D.y, kz = ez[k] + D.z;
-                            const float d2 = kx * kx + ky * ky + kz * kz;
-                            ms |= unsigned(d2 < s_lo) << k;
-                            ml |= unsigned(d2 > s_hi && d2 < l_lo) << k;
-                            amb |= unsigned((d2 >= s_lo && d2 <= s_hi) || (d2 >= l_lo && d2 <= l_hi)) << k;
-                            if (edge) {
-                                const bool inbox = fabsf(kx) < limx && fabsf(ky) < limy && fabsf(kz) < limz;
-                                amb |= unsigned(!inbox) << k;
-                            }
-                        }
-                        ms &= valid & ~amb;
-                        ml &= valid & ~amb;
-                        amb &= valid;
-                    }
-                }
-                // the rare ambiguous pairs: the exact FP64 decision
-                // (nearest_image_exact + len2_exact, box from the kernel
-                // parameters) for the lanes that have some
-                if (__any_sync(0xffffffffu, amb != 0u) && amb) {
-                    const int sp = s.clus_first[jc] + m;
+            for (int m = 0; m < W; ++m) any_am |= am[m];
+            if (__any_sync(0xffffffffu, any_am != 0u) && any_am) {
+                const int fj = s.clus_first[jc];
+#pragma unroll
+                for (int m = 0; m < W; ++m) {
+                    unsigned a = am[m];
+                    if (!a) continue;
+                    const int sp = fj + m;
                     const double tjx = sref[sp], tjy = sref[stride + sp], tjz = sref[2 * stride + sp];
-#pragma unroll 1
-                    for (int k = 0; k < W; ++k) {
-                        if (!((amb >> k) & 1u)) continue;
+                    unsigned add_s = 0u, add_l = 0u;
+                    while (a) {
+                        const int k = __ffs(a) - 1;
+                        a &= a - 1u;
                         double rx = __dsub_rn(sref[first_i + k], tjx);
                         double ry = __dsub_rn(sref[stride + first_i + k], tjy);
                         double rz = __dsub_rn(sref[2 * stride + first_i + k], tjz);
@@ -595,26 +696,32 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const Sys
                         const double e2 = len2_exact(rx, ry, rz);
                         if (!(e2 > P.c2l)) {
                             if (e2 > P.c2s)
-                                ml |= 1u << k;
+                                add_l |= 1u << k;
                             else
-                                ms |= 1u << k;
+                                add_s |= 1u << k;
                         }
                     }
+                    ms[m] |= add_s;
+                    ml[m] |= add_l;
                 }
+            }
+            // entries of member m of every lane's survivor, compacted in lane order
+#pragma unroll
+            for (int m = 0; m < W; ++m) {
                 const uint32_t slot = static_cast<uint32_t>(jc * W + m);
-                const unsigned bs = __ballot_sync(0xffffffffu, ms != 0);
-                const unsigned bl = __ballot_sync(0xffffffffu, ml != 0);
-                if (ms) {
+                const unsigned bs = __ballot_sync(0xffffffffu, ms[m] != 0u);
+                const unsigned bl = __ballot_sync(0xffffffffu, ml[m] != 0u);
+                if (ms[m]) {
                     const int p = cnt_s + __popc(bs & below);
-                    const uint32_t ent = (slot << 8) | ms;
+                    const uint32_t ent = (slot << 8) | ms[m];
                     if (p < kEntBuf)
                         ebuf_s[w][p] = ent;
                     else if (p < P.wcap)
                         outs[p] = ent;
                 }
-                if (ml) {
+                if (ml[m]) {
                     const int p = cnt_l + __popc(bl & below);
-                    const uint32_t ent = (slot << 8) | ml;
+                    const uint32_t ent = (slot << 8) | ml[m];
                     if (p < kEntBuf)
                         ebuf_l[w][p] = ent;
                     else if (p < P.wcap)
@@ -626,8 +733,12 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 6) k_water_search(const Sys
             // keep the survivors beyond the 32 just classified
             const int rem = qn - nq;
             const int keep = lane < rem ? q_jc[w][32 + lane] : 0;
+            const float keep_sp = lane < rem ? q_sp[w][32 + lane] : 0.f;
             __syncwarp();
-            if (lane < rem) q_jc[w][lane] = keep;
+            if (lane < rem) {
+                q_jc[w][lane] = keep;
+                q_sp[w][lane] = keep_sp;
+            }
             qn = rem;
             __syncwarp();
         }
