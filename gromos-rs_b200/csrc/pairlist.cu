@@ -523,7 +523,7 @@ __device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restric
 }
 
 template <int W, bool POPSORT>
-__global__ void __launch_bounds__(kSearchWarps * 32, W == 4 ? 6 : 4) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
+__global__ void __launch_bounds__(kSearchWarps * 32, W == 4 ? 8 : 4) k_water_search(const SysDev* __restrict__ sys, const SearchParams P) {
     const SysDev& s = sys[blockIdx.y];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     __shared__ uint32_t ebuf_s[kSearchWarps][kEntBuf], ebuf_l[kSearchWarps][kEntBuf];
