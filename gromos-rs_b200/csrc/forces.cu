@@ -64,16 +64,18 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     double e_excl = 0.0;
     float m = 0.f;
     if (w < nsolv) {
+        // every load is issued before the slot is tested: the coordinates do
+        // not depend on it
         const int slot = cg_slot[nscg + w];
+        const int a0 = nsa + 3 * w;  // solvent CGs are whole 3-site molecules
+        double p[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) p[q] = pos[3 * a0 + q];
+        double q3[3] = {0.0, 0.0, 0.0};
+        if (excl)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) q3[a] = charge[a0 + a];
         if (slot >= 0) {
-            const int a0 = nsa + 3 * w;  // solvent CGs are whole 3-site molecules
-            double p[9];
-#pragma unroll
-            for (int q = 0; q < 9; ++q) p[q] = pos[3 * a0 + q];
-            double q3[3] = {0.0, 0.0, 0.0};
-            if (excl)
-#pragma unroll
-                for (int a = 0; a < 3; ++a) q3[a] = charge[a0 + a];
             WaterRec w;
             w.x0 = p[0];
             w.y0 = p[1];
@@ -119,18 +121,26 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
             }
         }
     }
-    // one atomicMax per warp (the extents are >= 0, so their bit patterns order like the values)
+    // one atomicMax and one energy add per block (the extents are >= 0, so
+    // their bit patterns order like the values)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(reinterpret_cast<int*>(max_delta), __float_as_int(m));
-    if (excl) {
-        long long v = warp_sum_ll(to_fixed_d(e_excl, kEnergyScale));
-        __shared__ unsigned long long sh;
-        if (threadIdx.x == 0) sh = 0ull;
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh, static_cast<unsigned long long>(v));
-        __syncthreads();
-        if (threadIdx.x == 0 && sh) atomicAdd(reinterpret_cast<unsigned long long*>(acc_short + G * G + gs * G + gs), sh);
+    const long long v = excl ? warp_sum_ll(to_fixed_d(e_excl, kEnergyScale)) : 0ll;
+    __shared__ int mx;
+    __shared__ unsigned long long sh;
+    if (threadIdx.x == 0) {
+        mx = 0;
+        sh = 0ull;
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        if (m > 0.f) atomicMax(&mx, __float_as_int(m));
+        if (v) atomicAdd(&sh, static_cast<unsigned long long>(v));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (mx) atomicMax(reinterpret_cast<int*>(max_delta), mx);
+        if (sh) atomicAdd(reinterpret_cast<unsigned long long*>(acc_short + G * G + gs * G + gs), sh);
     }
 }
 
@@ -851,14 +861,18 @@ __global__ void k_finalize(const SysDev* __restrict__ sys, int plain) {
     float* max_delta = s.max_delta;
     int* n_deferred = s.n_deferred;
     const bool water = s.wrec != nullptr && !plain;
+    // a water atom's per-atom accumulators hold something only when solute
+    // kernels, excluded pairs or perturbation terms reach water atoms
+    const bool water_pa = plain || nscg > 0 || s.excl_atoms > nsa || s.n_pert > 0 || s.n_pp > 0;
     const double inv = 1.0 / kForceScale;
     // Every per-atom short-range accumulator is read by exactly one thread
     // here, which also clears it for the next evaluation (the per-slot water
     // sums are cleared by one contiguous memset; the long-range cache persists).
     if (i < n3) {
-        long long fx = f_short[i];
-        if (twin) fx += f_long[i];
         const int a = i / 3;
+        const bool pa = a < nsa || water_pa;
+        long long fx = pa ? f_short[i] : 0ll;
+        if (twin && pa) fx += f_long[i];
         if (a >= nsa && water) {
             const int w = (a - nsa) / 3;
             const int slot = cg_slot[nscg + w];
@@ -872,7 +886,7 @@ __global__ void k_finalize(const SysDev* __restrict__ sys, int plain) {
             if (twin) v += double(f32_long[i]);
         }
         f_out[i] = v;
-        f_short[i] = 0;
+        if (pa) f_short[i] = 0;
     }
     if (i < NA) {
         double v = double(acc_short[i]) / kEnergyScale;
