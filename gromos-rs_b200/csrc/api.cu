@@ -236,6 +236,7 @@ static gr_status validate(const gr_topology* t) {
 gr_status NbSystem::upload(const gr_topology* t) {
     gr_status st = validate(t);
     if (st) return st;
+    prepped_next = false;
     release();
     bytes = 0;
     N = t->n_atoms;
@@ -432,6 +433,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
 }
 
 gr_status NbSystem::set_params(const gr_nb_params* p) {
+    prepped_next = false;  // the records' excluded energies depend on the parameters
     if (!p || p->rcutp <= 0 || p->rcutl < p->rcutp || p->skin < 0 || p->nsnb <= 0) {
         set_error("gr_nb_params: need 0 < rcutp <= rcutl, skin >= 0, nsnb >= 1");
         return GR_ERR_INVALID;
@@ -516,6 +518,7 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
 }
 
 gr_status NbSystem::set_box(const double box[3]) {
+    prepped_next = false;
     if (prm.boundary == 1 && (!(box[0] > 0) || !(box[1] > 0) || !(box[2] > 0))) {
         set_error("gr_set_box: rectangular box edges must be positive");
         return GR_ERR_INVALID;
@@ -847,6 +850,10 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     if ((st = resolve_pending(&overflowed))) return st;
     if (overflowed) lr_computed = false;
     bool rebuild = !built || steps_since_update >= prm.nsnb || (flags & GR_EVAL_FORCE_REBUILD);
+    // the previous MD step wrote the water records of these positions (the
+    // lists, and so the slots, are kept); a recorded graph always holds the prep
+    const bool prepped = prepped_next && !rebuild && !in_capture;
+    prepped_next = false;
     // stage timing events are recorded kernel by kernel only: inside a recorded
     // graph each event node adds its own latency to the step, so a graph holds
     // just the first and last (the step's total device time)
@@ -891,7 +898,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         WaterParams wp;
         if (NCG > NSCG) {
             wp = water_params();
-            (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 128), 128, 0, s>>>(d_sys));
+            if (!prepped) (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 128), 128, 0, s>>>(d_sys));
             if ((st = launch_water(s, wp, false))) return st;
         }
         // solute work items: (CG, chunk of list entries), 4 warps per block
@@ -911,7 +918,7 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             lr_computed = true;
         }
     } else {
-        if (NCG > NSCG)  // per-step water data incl. the solvent excluded energies
+        if (NCG > NSCG && !prepped)  // per-step water data incl. the solvent excluded energies
             (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 128), 128, 0, s>>>(d_sys));
         (++launches, k_pos32<<<blocks_for(N, 256), 256, 0, s>>>(d_sys));
         GR_CUDA(cudaMemsetAsync(h.f32, 0, size_t(N) * 3 * sizeof(float), s));
@@ -1041,6 +1048,7 @@ gr_status NbSystem::eval_graph(cudaStream_t s, int flags) {
         }
         g_gen = alloc_gen;
     }
+    prepped_next = false;  // the graphs hold their own prep
     GR_CUDA(cudaGraphLaunch(g_step[rebuild ? 1 : 0], s));
     last_staged = false;
     GR_CUDA(cudaEventRecord(ev_step, s));
@@ -1390,6 +1398,7 @@ gr_status gr_positions_upload(gr_ctx* ctx, const double* xyz) {
         set_error("gr_positions_upload: no system or null positions");
         return GR_ERR_STATE;
     }
+    ctx->sys.prepped_next = false;
     cudaError_t e = cudaMemcpyAsync(ctx->sys.h.pos, xyz, size_t(ctx->sys.N) * 3 * sizeof(double),
                                     cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) {
@@ -1407,6 +1416,7 @@ gr_status gr_positions_device(gr_ctx* ctx, double** dev_xyz) {
         return GR_ERR_STATE;
     }
     *dev_xyz = ctx->sys.h.pos;
+    ctx->sys.prepped_next = false;  // the caller may write the coordinates
     ctx->sys.pos_set = true;
     return GR_OK;
 }

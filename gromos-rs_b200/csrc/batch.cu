@@ -219,6 +219,7 @@ gr_status batch_recover(gr_batch* b, gr_batch::Member& mb, int flags, int steps)
     }
     const size_t bytes3 = size_t(S.N) * 3 * sizeof(double);
     GR_CUDA(cudaMemcpyAsync(S.h.pos, S.md_pos_snap, bytes3, cudaMemcpyDeviceToDevice, si));
+    S.prepped_next = false;
     GR_CUDA(cudaMemcpyAsync(S.md_vel, S.md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, si));
     GR_CUDA(cudaMemcpyAsync(S.md_ke, S.md_ke_snap, sizeof(long long), cudaMemcpyDeviceToDevice, si));
     S.steps_since_update = S.prm.nsnb;
@@ -226,6 +227,7 @@ gr_status batch_recover(gr_batch* b, gr_batch::Member& mb, int flags, int steps)
     S.lr_computed = false;
     S.pending_check = false;
     gr_status st = S.md_run(si, steps, nullptr);
+    S.prepped_next = false;  // the batch's step graphs write their own water records
     if (st) return st;
     S.md_steps_total -= steps;  // counted once, by the batch step that failed
     S.md_rollbacks += 1;

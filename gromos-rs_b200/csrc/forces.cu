@@ -35,94 +35,73 @@ constexpr float kF = 4294967296.0f;   // force fixed-point scale (2^32)
 constexpr float kE = 16777216.0f;     // energy / virial fixed-point scale (2^24)
 
 // ---------------------------------------------------------------------------
-__global__ void k_water_prep(const SysDev* __restrict__ sys) {
-    // Descriptor fields and the molecule's coordinates are read into registers
-    // before the record is stored (a store through a descriptor pointer would
-    // otherwise make every later field read wait for it).  Solvent molecules
-    // are 3-site (checked at upload).
-    // One thread per solvent molecule in atom order (coalesced position
-    // reads); the record goes to the molecule's slot.
-    const SysDev& s = sys[blockIdx.y];
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nsolv = s.n_cg - s.n_solute_cg;
-    const int* __restrict__ cg_slot = s.cg_slot;
-    const double* __restrict__ pos = s.pos;
-    const double* __restrict__ charge = s.charge;
+// The per-step record of one solvent molecule (coordinates p, charges q3 when
+// the intra-molecular excluded pairs are done here): the slot's water record,
+// its short-range force sums cleared, the line of the cluster's short list
+// this member pulls into L2; returns the molecule's extent in m and adds its
+// excluded-pair RF energies (-q_i q_j fpe crf_2cut3i r^2, rf_excluded_interactions,
+// excluded.rs:81-96) to e_excl.  Used by k_water_prep and, for the next step,
+// by the MD step kernel.
+__device__ __forceinline__ void water_record(const SysDev& s, int slot, const double (&p)[9], const double (&q3)[3],
+                                             bool excl, double& e_excl, float& m) {
+    // descriptor fields first: the stores below go through pointers the
+    // compiler cannot tell apart from the descriptor
     WaterRec* __restrict__ wrec = s.wrec;
     long long* __restrict__ fs_short = s.fs_short;
     const uint32_t* __restrict__ wl_s = s.wl_s;
     const int W = s.W, wcap = s.wcap;
-    const int nsa = s.n_solute_atoms, nscg = s.n_solute_cg;
-    const bool excl = s.excl_atoms < s.n_atoms;
     const bool rect = s.boundary == 1;
     const double bx = s.box[0], by = s.box[1], bz = s.box[2];
     const double ibx = s.inv_box[0], iby = s.inv_box[1], ibz = s.inv_box[2];
     const double fpe = s.fpe, crf2 = s.crf_2cut3i;
-    float* max_delta = s.max_delta;
-    long long* acc_short = s.acc_short;
-    const int G = s.n_egroups, gs = s.solvent_group < 0 ? 0 : s.solvent_group;
-    double e_excl = 0.0;
-    float m = 0.f;
-    if (w < nsolv) {
-        // every load is issued before the slot is tested: the coordinates do
-        // not depend on it
-        const int slot = cg_slot[nscg + w];
-        const int a0 = nsa + 3 * w;  // solvent CGs are whole 3-site molecules
-        double p[9];
+    WaterRec w;
+    w.x0 = p[0];
+    w.y0 = p[1];
+    w.z0 = p[2];
+    w.h1x = float(p[3] - p[0]);
+    w.h1y = float(p[4] - p[1]);
+    w.h1z = float(p[5] - p[2]);
+    w.h2x = float(p[6] - p[0]);
+    w.h2y = float(p[7] - p[1]);
+    w.h2z = float(p[8] - p[2]);
+    // extent of the molecule (per-atom images of the long list need it)
+    m = fmaxf(m, fmaxf(fmaxf(fabsf(w.h1x), fabsf(w.h1y)), fmaxf(fabsf(w.h1z), fabsf(w.h2x))));
+    m = fmaxf(m, fmaxf(fabsf(w.h2y), fabsf(w.h2z)));
+    if (excl) {
 #pragma unroll
-        for (int q = 0; q < 9; ++q) p[q] = pos[3 * a0 + q];
-        double q3[3] = {0.0, 0.0, 0.0};
-        if (excl)
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int a = 0; a < 3; ++a) q3[a] = charge[a0 + a];
-        if (slot >= 0) {
-            WaterRec w;
-            w.x0 = p[0];
-            w.y0 = p[1];
-            w.z0 = p[2];
-            w.h1x = float(p[3] - p[0]);
-            w.h1y = float(p[4] - p[1]);
-            w.h1z = float(p[5] - p[2]);
-            w.h2x = float(p[6] - p[0]);
-            w.h2y = float(p[7] - p[1]);
-            w.h2z = float(p[8] - p[2]);
-            // extent of the molecule (per-atom images of the long list need it)
-            m = fmaxf(fmaxf(fabsf(w.h1x), fabsf(w.h1y)), fmaxf(fabsf(w.h1z), fabsf(w.h2x)));
-            m = fmaxf(m, fmaxf(fabsf(w.h2y), fabsf(w.h2z)));
-            // solvent excluded pairs: energy only, -q_i q_j fpe crf_2cut3i r^2
-            // (rf_excluded_interactions, excluded.rs:81-96)
-            if (excl)
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-#pragma unroll
-                    for (int b = a + 1; b < 3; ++b) {
-                        double rx = __dsub_rn(p[3 * a], p[3 * b]);
-                        double ry = __dsub_rn(p[3 * a + 1], p[3 * b + 1]);
-                        double rz = __dsub_rn(p[3 * a + 2], p[3 * b + 2]);
-                        if (rect) {
-                            rx = image_exact(rx, bx, ibx);
-                            ry = image_exact(ry, by, iby);
-                            rz = image_exact(rz, bz, ibz);
-                        }
-                        e_excl += -q3[a] * q3[b] * fpe * crf2 * len2_exact(rx, ry, rz);
-                    }
-            wrec[slot] = w;
-            // the slot's short-range force sums start at zero for this evaluation
-            // (only slots that hold a water are ever added to or read)
-            long long* __restrict__ fz = fs_short + static_cast<size_t>(slot) * 9;
-#pragma unroll
-            for (int c = 0; c < 9; ++c) fz[c] = 0;
-            // the member k of a cluster pulls line k of the cluster's short list
-            // into L2 for the force kernel (the list was written at the last rebuild)
-            const int k = slot % W;
-            if (32 * k < wcap) {
-                const uint32_t* line = wl_s + static_cast<size_t>(slot / W) * wcap + 32 * k;
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+            for (int b = a + 1; b < 3; ++b) {
+                double rx = __dsub_rn(p[3 * a], p[3 * b]);
+                double ry = __dsub_rn(p[3 * a + 1], p[3 * b + 1]);
+                double rz = __dsub_rn(p[3 * a + 2], p[3 * b + 2]);
+                if (rect) {
+                    rx = image_exact(rx, bx, ibx);
+                    ry = image_exact(ry, by, iby);
+                    rz = image_exact(rz, bz, ibz);
+                }
+                e_excl += -q3[a] * q3[b] * fpe * crf2 * len2_exact(rx, ry, rz);
             }
-        }
     }
-    // one atomicMax and one energy add per block (the extents are >= 0, so
-    // their bit patterns order like the values)
+    wrec[slot] = w;
+    // the slot's short-range force sums start at zero for this evaluation
+    // (only slots that hold a water are ever added to or read)
+    long long* __restrict__ fz = fs_short + static_cast<size_t>(slot) * 9;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) fz[c] = 0;
+    // the member k of a cluster pulls line k of the cluster's short list
+    // into L2 for the force kernel (the list was written at the last rebuild)
+    const int k = slot % W;
+    if (32 * k < wcap) {
+        const uint32_t* line = wl_s + static_cast<size_t>(slot / W) * wcap + 32 * k;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+    }
+}
+
+// Block-level flush of water_record's outputs: one atomicMax of the extent
+// and one energy add per block (the extents are >= 0, so their bit patterns
+// order like the values).  Every thread of the block calls it.
+__device__ __forceinline__ void water_record_flush(const SysDev& s, float m, double e_excl, bool excl) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     const long long v = excl ? warp_sum_ll(to_fixed_d(e_excl, kEnergyScale)) : 0ll;
@@ -139,9 +118,38 @@ __global__ void k_water_prep(const SysDev* __restrict__ sys) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        if (mx) atomicMax(reinterpret_cast<int*>(max_delta), mx);
-        if (sh) atomicAdd(reinterpret_cast<unsigned long long*>(acc_short + G * G + gs * G + gs), sh);
+        const int G = s.n_egroups, gs = s.solvent_group < 0 ? 0 : s.solvent_group;
+        long long* acc = s.acc_short;
+        if (mx) atomicMax(reinterpret_cast<int*>(s.max_delta), mx);
+        if (sh) atomicAdd(reinterpret_cast<unsigned long long*>(acc + G * G + gs * G + gs), sh);
     }
+}
+
+__global__ void k_water_prep(const SysDev* __restrict__ sys) {
+    // One thread per solvent molecule in atom order (coalesced position
+    // reads); the record goes to the molecule's slot.  Every load is issued
+    // before the slot is tested: the coordinates do not depend on it.
+    // Solvent molecules are 3-site (checked at upload).
+    const SysDev& s = sys[blockIdx.y];
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nsolv = s.n_cg - s.n_solute_cg;
+    const int nsa = s.n_solute_atoms, nscg = s.n_solute_cg;
+    const bool excl = s.excl_atoms < s.n_atoms;
+    double e_excl = 0.0;
+    float m = 0.f;
+    if (w < nsolv) {
+        const int slot = s.cg_slot[nscg + w];
+        const int a0 = nsa + 3 * w;  // solvent CGs are whole 3-site molecules
+        double p[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) p[q] = s.pos[3 * a0 + q];
+        double q3[3] = {0.0, 0.0, 0.0};
+        if (excl)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) q3[a] = s.charge[a0 + a];
+        if (slot >= 0) water_record(s, slot, p, q3, excl, e_excl, m);
+    }
+    water_record_flush(s, m, e_excl, excl);
 }
 
 // Per-block reduction of NV fixed-point accumulators into global memory.

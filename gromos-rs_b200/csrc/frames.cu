@@ -71,6 +71,7 @@ extern "C" gr_status gr_energy_frames(gr_ctx* ctx, int32_t n_frames, const doubl
         if (boxes && (q = S.set_box(boxes + 3 * size_t(f)))) return q;
         FR_CUDA(cudaMemcpyAsync(S.h.pos, frames + n3 * size_t(f), n3 * sizeof(double), cudaMemcpyHostToDevice, st));
         S.pos_set = true;
+        S.prepped_next = false;
         if ((q = S.eval(st, GR_EVAL_FORCE_REBUILD, false))) return q;
         FR_CUDA(cudaMemcpyAsync(dE + size_t(f) * NA, S.h.e_out, NA * sizeof(double), cudaMemcpyDeviceToDevice, st));
         FR_CUDA(cudaMemcpyAsync(pin_err + 4 * slot, S.h.err, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));

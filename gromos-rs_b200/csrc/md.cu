@@ -29,6 +29,7 @@ struct MdDev {
                               // of the velocities leaving it (fixed point 2^24), [2] blocks finished
     int* failures;            // [1] molecules SETTLE could not solve
     double t0, tau, dof;      // Berendsen bath (tau < 0: none)
+    int prep_next;            // also write the next step's water records (SETTLE units, no rebuild next)
 };
 
 // Berendsen weak coupling (berendsen_thermostat.rs:74-98): lambda from the
@@ -120,23 +121,38 @@ __device__ bool settle_molecule(const D3 old[3], D3 nw[3], D3 v[3], const MdDev&
 
 // One thread per unit: a solute atom (leap-frog only) or a solvent molecule
 // (leap-frog of its atoms, then SETTLE).  Forces are the finalized FP64
-// forces of this step's evaluation.
+// forces of this step's evaluation.  With prep_next the kernel also does the
+// next evaluation's k_water_prep for each molecule from its new coordinates
+// (same record, same cleared force sums, same excluded energies and extent;
+// the slots are those of the current lists, so only when the next step keeps
+// them): the next evaluation then skips k_water_prep.
 __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
     // descriptor pointers in registers and every load of a unit before its
     // stores (stores through descriptor pointers would otherwise order the
     // later reads behind them)
     const SysDev& s = *sys;
-    const int nsa = s.n_solute_atoms, n = s.n_atoms;
+    const int nsa = s.n_solute_atoms, n = s.n_atoms, nscg = s.n_solute_cg;
     const double* __restrict__ f_out = s.f_out;
     double* __restrict__ pos = s.pos;
+    const int* __restrict__ cg_slot = s.cg_slot;
+    const double* __restrict__ charge = s.charge;
+    const bool excl = s.excl_atoms < n;
     const int n_mol = md.settle ? (n - nsa) / 3 : 0;
     const int n_units = md.settle ? nsa + n_mol : n;
     const double lambda = berendsen_lambda(md);
     long long ke = 0;
+    double e_excl = 0.0;
+    float m_ext = 0.f;
     for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < n_units; u += gridDim.x * blockDim.x) {
         const bool mol = md.settle && u >= nsa;
         const int a0 = mol ? nsa + 3 * (u - nsa) : u;
         const int na = mol ? 3 : 1;
+        const bool rec = mol && md.prep_next;
+        const int slot = rec ? cg_slot[nscg + (u - nsa)] : -1;
+        double q3[3] = {0.0, 0.0, 0.0};
+        if (rec && excl)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) q3[a] = charge[a0 + a];
         D3 old[3], nw[3], v[3];
         double mass[3];
         for (int k = 0; k < na; ++k) {
@@ -149,6 +165,10 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
             nw[k] = old[k] + v[k] * md.dt;
         }
         if (mol && !settle_molecule(old, nw, v, md)) atomicAdd(md.failures, 1);
+        if (rec && slot >= 0) {
+            const double p[9] = {nw[0].x, nw[0].y, nw[0].z, nw[1].x, nw[1].y, nw[1].z, nw[2].x, nw[2].y, nw[2].z};
+            water_record(s, slot, p, q3, excl, e_excl, m_ext);
+        }
         for (int k = 0; k < na; ++k) {
             const int i = a0 + k;
             pos[3 * i] = nw[k].x;
@@ -160,6 +180,7 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
             ke += to_fixed_d(0.5 * mass[k] * dot3(v[k], v[k]), kEnergyScale);
         }
     }
+    if (md.prep_next) water_record_flush(s, m_ext, e_excl, excl);  // block-uniform
     ke = warp_sum_ll(ke);
     if ((threadIdx.x & 31) == 0 && ke) atomicAdd(reinterpret_cast<unsigned long long*>(md.ke + 1),
                                                   static_cast<unsigned long long>(ke));
@@ -182,6 +203,7 @@ __global__ void k_md_step(const SysDev* __restrict__ sys, MdDev md) {
 using namespace gnb;
 
 gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_params* p) {
+    prepped_next = false;
     if (!uploaded) {
         set_error("gr_md_init before gr_system_upload");
         return GR_ERR_STATE;
@@ -260,7 +282,7 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
 }
 
 // Zeroes the kinetic-energy accumulator and launches one MD step kernel.
-gr_status NbSystem::md_step_launch(cudaStream_t s) {
+gr_status NbSystem::md_step_launch(cudaStream_t s, bool fuse_prep) {
     MdDev md;
     md.vel = md_vel;
     md.inv_mass = md_inv_mass;
@@ -278,6 +300,11 @@ gr_status NbSystem::md_step_launch(cudaStream_t s) {
     md.t0 = mdp.temperature;
     md.tau = mdp.tau;
     md.dof = md_dof;
+    // the next evaluation keeps this period's lists (no rebuild): its water
+    // records come from this kernel
+    md.prep_next = fuse_prep && md_settle && NCG > NSCG && h.wrec && !in_capture && built &&
+                   steps_since_update < prm.nsnb;
+    prepped_next = md.prep_next != 0;
     const int n_units = md_settle ? NSA + (N - NSA) / 3 : N;
     const unsigned grid = std::max(1u, std::min(unsigned((n_units + 255) / 256), unsigned(sm_count() * 8)));
     (++launches, k_md_step<<<grid, 256, 0, s>>>(d_sys, md));
@@ -363,7 +390,7 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
                     md_psnap_valid = true;
                 }
                 if ((st = eval(s, 0, false))) return st;
-                if ((st = md_step_launch(s))) return st;
+                if ((st = md_step_launch(s, true))) return st;
                 ++md_step_idx;
                 if (r < replay) {
                     ++r;
@@ -405,6 +432,7 @@ gr_status NbSystem::md_run(cudaStream_t s, int n_steps, gr_md_stats* out) {
             GR_CUDA(cudaMemcpyAsync(h.pos, md_pos_snap, bytes3, cudaMemcpyDeviceToDevice, s));
             GR_CUDA(cudaMemcpyAsync(md_vel, md_vel_snap, bytes3, cudaMemcpyDeviceToDevice, s));
             GR_CUDA(cudaMemcpyAsync(md_ke, md_ke_snap, sizeof(long long), cudaMemcpyDeviceToDevice, s));
+            prepped_next = false;
             md_step_idx = idx0;
             steps_since_update = prm.nsnb;
             built = false;  // the rollback point starts a period: rebuilt there with the grown lists

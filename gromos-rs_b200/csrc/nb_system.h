@@ -47,7 +47,7 @@ class NbSystem {
     gr_status launch_water(cudaStream_t s, const WaterParams& wp, bool lr);
     gr_status md_init(const double* mass, const double* vel, const gr_md_params* p);
     gr_status md_run(cudaStream_t s, int n_steps, gr_md_stats* out);
-    gr_status md_step_launch(cudaStream_t s);
+    gr_status md_step_launch(cudaStream_t s, bool fuse_prep = false);
     gr_status md_stats(cudaStream_t s, gr_md_stats* out);
     gr_status ensure_capacity();
 
@@ -119,6 +119,7 @@ class NbSystem {
     bool step_check = false;
     bool in_capture = false;  // recording a CUDA graph: the device descriptor is already current
     bool last_staged = false; // the last timed evaluation recorded its stage events (kernel by kernel)
+    bool prepped_next = false; // the last MD step wrote this evaluation's water records (k_water_prep skipped)
 
    private:
     template <class T>

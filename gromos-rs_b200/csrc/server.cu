@@ -93,6 +93,7 @@ struct gr_server {
     std::vector<int64_t> resident;
     int64_t next_id = 1, resident_bytes = 0, max_resident_bytes = 0, steps_run = 0;
     int32_t max_resident_jobs = 0;
+    int64_t joined_running = 0;  // admitted while resident jobs had already stepped
     double bytes_per_atom = 8192.0;
     bool measured = false;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -159,10 +160,13 @@ gr_status admit(gr_server* srv) {
             destroy_job_ctx(j);  // does not fit after all: wait for memory
             return GR_OK;
         }
+        bool running = false;
+        for (int64_t id : srv->resident) running = running || srv->jobs[id].steps_done > 0;
         if ((st = gr_batch_add(srv->batch, j.ctx))) {
             destroy_job_ctx(j);
             return st;
         }
+        srv->joined_running += running ? 1 : 0;
         srv->queue.pop_front();
         j.state = GR_JOB_RUNNING;
         j.t_admit = srv->now();
@@ -387,6 +391,7 @@ gr_status gr_server_stats(gr_server* srv, gr_server_stats_t* out) {
     out->max_resident_bytes = srv->max_resident_bytes;
     out->max_resident_jobs = srv->max_resident_jobs;
     out->batch_steps = srv->steps_run;
+    out->jobs_joined_running = srv->joined_running;
     return GR_OK;
 }
 

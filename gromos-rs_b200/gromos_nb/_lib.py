@@ -107,7 +107,7 @@ class GrServerStats(C.Structure):
     _fields_ = [("jobs_done", C.c_int64), ("jobs_queued", C.c_int64), ("jobs_running", C.c_int64),
                 ("latency_p50_s", C.c_double), ("latency_p99_s", C.c_double), ("resident_bytes", C.c_int64),
                 ("max_resident_bytes", C.c_int64), ("max_resident_jobs", C.c_int32), ("batch_steps", C.c_int64),
-                ("jobs_failed", C.c_int64), ("jobs_cancelled", C.c_int64)]
+                ("jobs_failed", C.c_int64), ("jobs_cancelled", C.c_int64), ("jobs_joined_running", C.c_int64)]
 
 
 GR_JOB_QUEUED, GR_JOB_RUNNING, GR_JOB_DONE, GR_JOB_FAILED, GR_JOB_CANCELLED = 0, 1, 2, 3, 4

@@ -344,6 +344,7 @@ typedef struct {
     int32_t max_resident_jobs;
     int64_t batch_steps;
     int64_t jobs_failed, jobs_cancelled;
+    int64_t jobs_joined_running;  /* admitted while resident jobs had already stepped */
 } gr_server_stats_t;
 
 typedef struct gr_server gr_server;

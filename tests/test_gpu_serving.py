@@ -80,6 +80,7 @@ def test_native_server_results_equal_standalone():
     srv.close()
     assert st["jobs_done"] == len(jobs)
     assert st["max_resident_jobs"] >= 2
+    assert st["jobs_joined_running"] >= 1       # at least one joined a batch that was already stepping
     assert 0 < st["latency_p50_s"] <= st["latency_p99_s"]
     for job in jobs:
         x, v = standalone(job)
