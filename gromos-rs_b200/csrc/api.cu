@@ -383,6 +383,9 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&h.ref, size_t(NCG) * 3))) return st;
     if ((st = alloc(&h.keys, size_t(NCG)))) return st;
     if ((st = alloc(&d_cg_key, size_t(NCG)))) return st;
+    if ((st = alloc(&h.cg_rank, size_t(NCG)))) return st;
+    if ((st = alloc(&h.build_ctr, 4))) return st;
+    GR_CUDA(cudaMemset(h.build_ctr, 0, 4 * sizeof(int)));  // each last block leaves its counter at zero
     if ((st = alloc(&h.cg_cell, size_t(NCG)))) return st;
     if ((st = alloc(&h.sorted_cg, size_t(NCG)))) return st;
     if ((st = alloc(&h.sref, 3 * (size_t(NCG) + 2)))) return st;
@@ -565,7 +568,7 @@ gr_status NbSystem::ensure_capacity() {
     if (h.n_cells > cells_alloc) {
         int n = h.n_cells;
         if ((st = alloc(&h.cell_count, size_t(n)))) return st;
-        if ((st = alloc(&h.cell_fill, size_t(n)))) return st;
+        GR_CUDA(cudaMemset(h.cell_count, 0, size_t(n) * sizeof(int)));  // k_refpos clears it after use
         if ((st = alloc(&h.cell_start, size_t(n) + 1))) return st;
         if ((st = alloc(&h.cell_nsolute, size_t(n)))) return st;
         if ((st = alloc(&h.cell_nclus, size_t(n) + 1))) return st;
@@ -746,13 +749,9 @@ gr_status NbSystem::build_pairlist(cudaStream_t s, bool sync) {
         gr_status st = ensure_capacity();
         if (st) return st;
         if ((st = push_descriptor(s))) return st;
-        GR_CUDA(cudaMemsetAsync(h.cell_count, 0, size_t(h.n_cells) * sizeof(int), s));
-        GR_CUDA(cudaMemsetAsync(h.cell_fill, 0, size_t(h.n_cells) * sizeof(int), s));
         (++launches, k_refpos<<<blocks_for(NCG, 256), 256, 0, s>>>(d_sys, d_cg_key));
-        (++launches, k_scan_cells<<<1, 1024, 0, s>>>(d_sys));
         (++launches, k_scatter<<<blocks_for(NCG, 256), 256, 0, s>>>(d_sys, d_cg_key));
         (++launches, k_cell_sort<<<h.n_cells, 256, 0, s>>>(d_sys));
-        (++launches, k_scan_clusters<<<1, 1024, 0, s>>>(d_sys));
         (++launches, k_cluster_setup<<<h.n_cells, 128, 0, s>>>(d_sys));
         if (NCG > NSCG) {
             (++launches, k_cell_candidates<<<dim3(h.n_cells, 2), 256, 0, s>>>(d_sys));

@@ -5,10 +5,8 @@
 
 namespace gnb {
 __global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __restrict__ cg_key);
-__global__ void k_scan_cells(const SysDev* __restrict__ sys);
 __global__ void k_scatter(const SysDev* __restrict__ sys, const unsigned long long* __restrict__ cg_key);
 __global__ void k_cell_sort(const SysDev* __restrict__ sys);
-__global__ void k_scan_clusters(const SysDev* __restrict__ sys);
 __global__ void k_cluster_setup(const SysDev* __restrict__ sys);
 __global__ void k_cell_candidates(const SysDev* __restrict__ sys);
 struct SearchParams;

@@ -99,8 +99,9 @@ struct SysDev {
     double* ref;               // n_cg*3
     unsigned long long* keys;  // n_cg (unsorted scatter, then sorted within cells)
     int* cg_cell;              // n_cg
-    int* cell_count;           // n_cells
-    int* cell_fill;            // n_cells
+    int* cell_count;           // n_cells (zero between builds)
+    int* cg_rank;              // n_cg: rank of the CG among its cell's (arrival order)
+    int* build_ctr;            // [4] finished-block counters of the build kernels (zero between launches)
     int* cell_start;           // n_cells+1
     int* cell_nsolute;         // n_cells
     int* cell_nclus;           // n_cells+1 (scanned in place -> cluster start)

@@ -11,9 +11,10 @@
 //   * d2 = |nearest_image(ref_1, ref_2)|^2; d2 > (rcl+skin)^2 -> no pair,
 //     d2 > (rcs+skin)^2 -> long range, else short range (strict '>').
 //
-// Stages: k_refpos (reference positions, cell keys) -> k_scan_cells ->
-// k_scatter -> k_cell_sort (rank sort, per cell, deterministic) ->
-// k_scan_clusters -> k_cluster_setup (solvent i-clusters of W CGs) ->
+// Stages: k_refpos (reference positions, cell keys, ranks; its last block
+// scans the cell counts) -> k_scatter -> k_cell_sort (rank sort, per cell,
+// deterministic; its last block scans the cluster counts) ->
+// k_cluster_setup (solvent i-clusters of W CGs) ->
 // k_cell_candidates (each cell's j-cluster candidates, contiguous) ->
 // k_water_search (water-water j-lists with W-bit masks) and
 // k_solute_search (per solute CG j-lists with exclusion masks) ->
@@ -50,10 +51,7 @@ __device__ __forceinline__ int cell_coord(double x, double cs, int g, double* fr
 }
 
 // Reference positions + cell keys (pairlist.rs:196-198, 577-585, 658-663).
-__global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __restrict__ cg_key) {
-    const SysDev& s = sys[blockIdx.y];
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= s.n_cg) return;
+__device__ __forceinline__ void refpos_one(const SysDev& s, int c, unsigned long long* __restrict__ cg_key) {
     int a0 = s.cg_off[c], a1 = s.cg_off[c + 1];
     double rx, ry, rz;
     if (c < s.n_solute_cg) {
@@ -100,43 +98,52 @@ __global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __r
                 (static_cast<unsigned long long>(order) << 32) | static_cast<unsigned>(c);
     s.cg_cell[c] = cell;
     s.cg_slot[c] = -1;
-    atomicAdd(&s.cell_count[cell], 1);
+    s.cg_rank[c] = atomicAdd(&s.cell_count[cell], 1);
 }
 
-// Exclusive scan of n values (single block, blockDim.x == 1024).  out has n+1
-// entries; out may alias in.  Also returns the total in *total (if given).
-__device__ void block_exclusive_scan(const int* in, int* out, int n, int* total) {
-    __shared__ int warp_tot[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int base = 0; base < n; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int v = i < n ? in[i] : 0;
-        int x = v;
+// Exclusive scan of n ints by one block (blockDim a multiple of 32, at most
+// 1024): each pass takes 8 consecutive values per thread, so a grid of up to
+// 8 x blockDim cells is one pass.  out has n + 1 entries (out[n] = total) and
+// may alias in (each thread reads its values before writing them).  The
+// values are read past L1 (other blocks of the same kernel wrote them).
+__device__ void block_scan8(const int* in, int* out, int n, int* total) {
+    __shared__ int wsum[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int carry = 0;
+    for (int base = 0; base < n; base += 8 * blockDim.x) {
+        const int i0 = base + 8 * threadIdx.x;
+        int v[8], t = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            v[k] = i0 + k < n ? __ldcg(in + i0 + k) : 0;
+            t += v[k];
+        }
+        int x = t;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
-        if (lane == 31) warp_tot[wid] = x;
+        if (lane == 31) wsum[wid] = x;
         __syncthreads();
         if (wid == 0) {
-            int t = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
+            int w = lane < nw ? wsum[lane] : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, t, o);
-                if (lane >= o) t += y;
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
             }
-            warp_tot[lane] = t;
+            wsum[lane] = w;
         }
         __syncthreads();
-        int excl = x - v + (wid > 0 ? warp_tot[wid - 1] : 0) + carry;
-        __syncthreads();
-        if (i < n) out[i] = excl;
-        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-        __syncthreads();
+        int e = carry + (wid > 0 ? wsum[wid - 1] : 0) + x - t;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (i0 + k < n) out[i0 + k] = e;
+            e += v[k];
+        }
+        carry += wsum[nw - 1];
+        __syncthreads();  // wsum is reused by the next pass
     }
     if (threadIdx.x == 0) {
         out[n] = carry;
@@ -144,23 +151,47 @@ __device__ void block_exclusive_scan(const int* in, int* out, int n, int* total)
     }
 }
 
-__global__ void k_scan_cells(const SysDev* __restrict__ sys) {
+// Whether this block is the last of its grid to get here: every earlier
+// block's global writes (and atomics) are visible to it afterwards.  The
+// counter is left at zero for the next launch.
+__device__ __forceinline__ bool last_block(int* ctr) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(ctr, 1) == int(gridDim.x * gridDim.y) - 1;
+        if (last) *ctr = 0;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// Each CG's rank in its cell comes from the cell counter; the last block
+// scans the counts into the cell starts and clears them for the next build.
+__global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __restrict__ cg_key) {
     const SysDev& s = sys[blockIdx.y];
-    block_exclusive_scan(s.cell_count, s.cell_start, s.n_cells, nullptr);
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < s.n_cg) refpos_one(s, c, cg_key);
+    if (last_block(s.build_ctr)) {
+        block_scan8(s.cell_count, s.cell_start, s.n_cells, nullptr);
+        __syncthreads();
+        for (int i = threadIdx.x; i < s.n_cells; i += blockDim.x) s.cell_count[i] = 0;
+    }
 }
 
 __global__ void k_scatter(const SysDev* __restrict__ sys, const unsigned long long* __restrict__ cg_key) {
     const SysDev& s = sys[blockIdx.y];
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= s.n_cg) return;
-    int cell = s.cg_cell[c];
-    int p = s.cell_start[cell] + atomicAdd(&s.cell_fill[cell], 1);
+    const int p = s.cell_start[s.cg_cell[c]] + s.cg_rank[c];
     s.keys[p] = cg_key[c];
 }
 
 // One block per cell: rank sort of the cell's keys (keys are unique: they
 // end in the CG index), one barrier; each key is then written at its rank
-// with the sorted CG maps and the sorted FP64 reference positions.
+// with the sorted CG maps and the sorted FP64 reference positions.  The last
+// block scans the cells' cluster counts into cluster starts.
 __global__ void __launch_bounds__(256) k_cell_sort(const SysDev* __restrict__ sys) {
     const SysDev& s = sys[blockIdx.y];
     __shared__ unsigned long long sk[kMaxCellCGs];
@@ -168,58 +199,60 @@ __global__ void __launch_bounds__(256) k_cell_sort(const SysDev* __restrict__ sy
     const int cell = blockIdx.x;
     const int start = s.cell_start[cell], n = s.cell_start[cell + 1] - start;
     if (n > kMaxCellCGs) {
-        if (threadIdx.x == 0) atomicOr(&s.err[0], ERR_CELL_TOO_DENSE);
-        return;
-    }
-    unsigned long long* __restrict__ keys = s.keys;
-    int* __restrict__ sorted_cg = s.sorted_cg;
-    int* __restrict__ cg_spos = s.cg_spos;
-    double* __restrict__ sref = s.sref;
-    const double* __restrict__ ref = s.ref;
-    const int stride = s.n_cg + 2;
-    if (threadIdx.x == 0) nsol = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) sk[i] = keys[start + i];
-    __syncthreads();
-    int local = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const unsigned long long key = sk[i];
-        int rank = 0;
-        int j = 0;
-        for (; j + 4 <= n; j += 4)
-            rank += int(sk[j] < key) + int(sk[j + 1] < key) + int(sk[j + 2] < key) + int(sk[j + 3] < key);
-        for (; j < n; ++j) rank += int(sk[j] < key);
-        const int cg = static_cast<int>(key & 0xffffffffull);
-        const int p = start + rank;
-        const double rx = ref[3 * cg], ry = ref[3 * cg + 1], rz = ref[3 * cg + 2];
-        keys[p] = key;
-        sorted_cg[p] = cg;
-        cg_spos[cg] = p;
-        sref[p] = rx;
-        sref[stride + p] = ry;
-        sref[2 * stride + p] = rz;
-        if (((key >> 42) & 1ull) == 0ull) ++local;
-    }
-    if (local) atomicAdd(&nsol, local);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        s.cell_nsolute[cell] = nsol;
-        s.cell_nclus[cell] = (n - nsol + s.W - 1) / s.W;
-    }
-}
-
-__global__ void k_scan_clusters(const SysDev* __restrict__ sys) {
-    const SysDev& s = sys[blockIdx.y];
-    __shared__ int total;
-    block_exclusive_scan(s.cell_nclus, s.cell_nclus, s.n_cells, &total);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        s.n_deferred[6] = 0;  // the water search's cluster counter
-        s.n_deferred[7] = 0;  // the candidate lists' allocation counter
-        if (total > s.max_clusters) {
-            atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
-            total = s.max_clusters;
+        if (threadIdx.x == 0) {
+            atomicOr(&s.err[0], ERR_CELL_TOO_DENSE);
+            s.cell_nsolute[cell] = 0;
+            s.cell_nclus[cell] = 0;
         }
-        s.n_clusters[0] = total;
+    } else {
+        unsigned long long* __restrict__ keys = s.keys;
+        int* __restrict__ sorted_cg = s.sorted_cg;
+        int* __restrict__ cg_spos = s.cg_spos;
+        double* __restrict__ sref = s.sref;
+        const double* __restrict__ ref = s.ref;
+        const int stride = s.n_cg + 2;
+        if (threadIdx.x == 0) nsol = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) sk[i] = keys[start + i];
+        __syncthreads();
+        int local = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long key = sk[i];
+            int rank = 0;
+            int j = 0;
+            for (; j + 4 <= n; j += 4)
+                rank += int(sk[j] < key) + int(sk[j + 1] < key) + int(sk[j + 2] < key) + int(sk[j + 3] < key);
+            for (; j < n; ++j) rank += int(sk[j] < key);
+            const int cg = static_cast<int>(key & 0xffffffffull);
+            const int p = start + rank;
+            const double rx = ref[3 * cg], ry = ref[3 * cg + 1], rz = ref[3 * cg + 2];
+            keys[p] = key;
+            sorted_cg[p] = cg;
+            cg_spos[cg] = p;
+            sref[p] = rx;
+            sref[stride + p] = ry;
+            sref[2 * stride + p] = rz;
+            if (((key >> 42) & 1ull) == 0ull) ++local;
+        }
+        if (local) atomicAdd(&nsol, local);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s.cell_nsolute[cell] = nsol;
+            s.cell_nclus[cell] = (n - nsol + s.W - 1) / s.W;
+        }
+    }
+    if (last_block(s.build_ctr + 1)) {
+        __shared__ int total;
+        block_scan8(s.cell_nclus, s.cell_nclus, s.n_cells, &total);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s.n_deferred[6] = 0;  // the water search's cluster counter
+            s.n_deferred[7] = 0;  // the candidate lists' allocation counter
+            if (total > s.max_clusters) {
+                atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);
+                total = s.max_clusters;
+            }
+            s.n_clusters[0] = total;
+        }
     }
 }
 
