@@ -528,6 +528,43 @@ __device__ __forceinline__ void sort_write_entries(const uint32_t* __restrict__ 
 template <int W>
 __device__ __forceinline__ void sort_write_entries_pop(const uint32_t* __restrict__ buf, int nbuf,
                                                        uint32_t* __restrict__ out, int lane) {
+    if constexpr (W == 4) {
+        // popcount - 1 as two bits, one ballot each: the four class masks and
+        // counts follow from three ballots, and each lane stores once
+        const unsigned lt = (1u << lane) - 1u;
+        int n[4] = {0, 0, 0, 0};
+        for (int c = 0; c < nbuf; c += 32) {
+            const int e = c + lane;
+            const bool valid = e < nbuf;
+            const int k = valid ? __popc(buf[e] & 0xffu) - 1 : 0;
+            const unsigned bv = __ballot_sync(0xffffffffu, valid);
+            const unsigned b0 = __ballot_sync(0xffffffffu, valid && (k & 1));
+            const unsigned b1 = __ballot_sync(0xffffffffu, valid && (k & 2));
+            n[3] += __popc(b0 & b1);
+            n[2] += __popc(b1 & ~b0);
+            n[1] += __popc(b0 & ~b1);
+            n[0] += __popc(bv & ~(b0 | b1));
+        }
+        int o3 = 0, o2 = n[3], o1 = n[3] + n[2], o0 = n[3] + n[2] + n[1];  // most bits first
+        for (int c = 0; c < nbuf; c += 32) {
+            const int e = c + lane;
+            const bool valid = e < nbuf;
+            const uint32_t ent = valid ? buf[e] : 0u;
+            const int k = valid ? __popc(ent & 0xffu) - 1 : 0;
+            const unsigned bv = __ballot_sync(0xffffffffu, valid);
+            const unsigned b0 = __ballot_sync(0xffffffffu, valid && (k & 1));
+            const unsigned b1 = __ballot_sync(0xffffffffu, valid && (k & 2));
+            const unsigned m3 = b0 & b1, m2 = b1 & ~b0, m1 = b0 & ~b1, m0 = bv & ~(b0 | b1);
+            const unsigned mine = k == 3 ? m3 : k == 2 ? m2 : k == 1 ? m1 : m0;
+            const int base = k == 3 ? o3 : k == 2 ? o2 : k == 1 ? o1 : o0;
+            if (valid) out[base + __popc(mine & lt)] = ent;
+            o3 += __popc(m3);
+            o2 += __popc(m2);
+            o1 += __popc(m1);
+            o0 += __popc(m0);
+        }
+        return;
+    }
     int off[W + 1];
     int hist[W + 1];
 #pragma unroll
