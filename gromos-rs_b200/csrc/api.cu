@@ -383,7 +383,6 @@ gr_status NbSystem::upload(const gr_topology* t) {
     if ((st = alloc(&h.ref, size_t(NCG) * 3))) return st;
     if ((st = alloc(&h.keys, size_t(NCG)))) return st;
     if ((st = alloc(&d_cg_key, size_t(NCG)))) return st;
-    if ((st = alloc(&h.cg_rank, size_t(NCG)))) return st;
     if ((st = alloc(&h.build_ctr, 4))) return st;
     GR_CUDA(cudaMemset(h.build_ctr, 0, 4 * sizeof(int)));  // each last block leaves its counter at zero
     if ((st = alloc(&h.cg_cell, size_t(NCG)))) return st;
@@ -569,6 +568,8 @@ gr_status NbSystem::ensure_capacity() {
         int n = h.n_cells;
         if ((st = alloc(&h.cell_count, size_t(n)))) return st;
         GR_CUDA(cudaMemset(h.cell_count, 0, size_t(n) * sizeof(int)));  // k_refpos clears it after use
+        if ((st = alloc(&h.cell_fill, size_t(n)))) return st;
+        GR_CUDA(cudaMemset(h.cell_fill, 0, size_t(n) * sizeof(int)));  // likewise
         if ((st = alloc(&h.cell_start, size_t(n) + 1))) return st;
         if ((st = alloc(&h.cell_nsolute, size_t(n)))) return st;
         if ((st = alloc(&h.cell_nclus, size_t(n) + 1))) return st;

@@ -100,7 +100,7 @@ struct SysDev {
     unsigned long long* keys;  // n_cg (unsorted scatter, then sorted within cells)
     int* cg_cell;              // n_cg
     int* cell_count;           // n_cells (zero between builds)
-    int* cg_rank;              // n_cg: rank of the CG among its cell's (arrival order)
+    int* cell_fill;            // n_cells: the scatter's counters (zero between builds)
     int* build_ctr;            // [4] finished-block counters of the build kernels (zero between launches)
     int* cell_start;           // n_cells+1
     int* cell_nsolute;         // n_cells

@@ -11,7 +11,7 @@
 //   * d2 = |nearest_image(ref_1, ref_2)|^2; d2 > (rcl+skin)^2 -> no pair,
 //     d2 > (rcs+skin)^2 -> long range, else short range (strict '>').
 //
-// Stages: k_refpos (reference positions, cell keys, ranks; its last block
+// Stages: k_refpos (reference positions, cell keys, counts; its last block
 // scans the cell counts) -> k_scatter -> k_cell_sort (rank sort, per cell,
 // deterministic; its last block scans the cluster counts) ->
 // k_cluster_setup (solvent i-clusters of W CGs) ->
@@ -98,7 +98,7 @@ __device__ __forceinline__ void refpos_one(const SysDev& s, int c, unsigned long
                 (static_cast<unsigned long long>(order) << 32) | static_cast<unsigned>(c);
     s.cg_cell[c] = cell;
     s.cg_slot[c] = -1;
-    s.cg_rank[c] = atomicAdd(&s.cell_count[cell], 1);
+    atomicAdd(&s.cell_count[cell], 1);
 }
 
 // Exclusive scan of n ints by one block (blockDim a multiple of 32, at most
@@ -167,8 +167,8 @@ __device__ __forceinline__ bool last_block(int* ctr) {
     return last;
 }
 
-// Each CG's rank in its cell comes from the cell counter; the last block
-// scans the counts into the cell starts and clears them for the next build.
+// The last block scans the cell counts into the cell starts and clears the
+// counts and the scatter's fill counters for the next build.
 __global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __restrict__ cg_key) {
     const SysDev& s = sys[blockIdx.y];
     int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -176,7 +176,10 @@ __global__ void k_refpos(const SysDev* __restrict__ sys, unsigned long long* __r
     if (last_block(s.build_ctr)) {
         block_scan8(s.cell_count, s.cell_start, s.n_cells, nullptr);
         __syncthreads();
-        for (int i = threadIdx.x; i < s.n_cells; i += blockDim.x) s.cell_count[i] = 0;
+        for (int i = threadIdx.x; i < s.n_cells; i += blockDim.x) {
+            s.cell_count[i] = 0;
+            s.cell_fill[i] = 0;
+        }
     }
 }
 
@@ -184,7 +187,8 @@ __global__ void k_scatter(const SysDev* __restrict__ sys, const unsigned long lo
     const SysDev& s = sys[blockIdx.y];
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= s.n_cg) return;
-    const int p = s.cell_start[s.cg_cell[c]] + s.cg_rank[c];
+    const int cell = s.cg_cell[c];
+    const int p = s.cell_start[cell] + atomicAdd(&s.cell_fill[cell], 1);
     s.keys[p] = cg_key[c];
 }
 
