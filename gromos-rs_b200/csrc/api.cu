@@ -1431,7 +1431,7 @@ gr_status gr_pairlist_build(gr_ctx* ctx) {
     if (st) return st;
     ctx->sys.ever_built = true;
     ctx->sys.pair_count_valid = false;
-    return ctx->sys.expand_cg_pairs(ctx->stream);
+    return GR_OK;  // the explicit CG-pair lists are expanded when first asked for
 }
 
 // The four reference lists from the device CG pair set (pairlist.rs:59-70):
