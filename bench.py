@@ -41,8 +41,9 @@ METRIC = "pair-int/s"
 WORKLOAD = "spc30000_twinrange_0.8_1.4_nsnb5"
 # DRAM bytes (read + write) of one short-range water-kernel launch on this
 # workload, dram__bytes_read.sum + dram__bytes_write.sum from an ncu capture of
-# the kernel (a recorded constant: this run does not measure it)
-SHORT_KERNEL_DRAM_BYTES = 6.951424e6
+# the first short-range launch of this script's small run (--steps 3 --warmup 3):
+# 6,675,712 B read, 0 written.  A recorded constant: this run does not measure it.
+SHORT_KERNEL_DRAM_BYTES = 6.675712e6
 
 
 def ns_per_day(ms_per_step: float) -> float:
@@ -369,8 +370,8 @@ def run_gpu(args, rank, world, local_rank):
                             "kernel": "short-range window: k_water_prep + k_water_force_it (deferred pairs in its last block)",
                             "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s (FP32 pipe)",
                             "frac": achieved / peak, "traffic": SHORT_KERNEL_DRAM_BYTES,
-                            "traffic_source": "ncu dram bytes of one short-range launch, recorded from an "
-                                              "earlier capture (not measured by this run)",
+                            "traffic_source": "ncu dram bytes of one short-range launch, recorded from a "
+                                              "capture of this build's kernel (not measured by this run)",
                             "peak_source": "measured FFMA-chain kernel (gr_ffma_peak), one FFMA = one op",
                             "ops_per_pair": OPS_PER_PAIR, "short_kernel_ms": t_short,
                             "long_kernel_ms": statistics.median(long_ms) if long_ms else None},

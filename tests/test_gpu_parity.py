@@ -79,6 +79,15 @@ def test_pairlist_bit_exact_spc30000_twin_range():
     check_pairlist(generators.config2_spc30000())
 
 
+def test_many_cells_sparse_box():
+    """3000 waters in a 12 nm box with a 0.9 nm cutoff: 13^3 = 2197 cells, most nearly empty,
+    so the cell and cluster scans take more than one pass of their block (2048 cells each)."""
+    s = generators.spc_water_system(3000, 12.0, 7, rcutp=0.9, rcutl=0.9, epsrf=61.0, nsnb=5, name="sparse3000")
+    assert int(12.0 / 0.9) ** 3 > 2048
+    check_pairlist(s)
+    compare_eval(s, steps=2, move=0.002)
+
+
 def compare_eval(s, kernel="fixed", steps=1, tol_rms=1e-5, tol_e=1e-5, move=0.0, seed=0, cluster_size=0,
                  layout=0, list_capacity=0):
     ff = Forcefield(s, kernel=kernel, cluster_size=cluster_size, water_layout=layout, list_capacity=list_capacity)
