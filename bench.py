@@ -281,6 +281,7 @@ def run_gpu(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     step_ms, short_ms, long_ms, build_ms = [], [], [], []
+    kshort_ms, klong_ms, prep_ms = [], [], []
     pairs = 0
     rebuilds = 0
     for k in range(args.steps):
@@ -309,11 +310,17 @@ def run_gpu(args, rank, world, local_rank):
         ff.eval_async(graph=False)
         evals_done += 1
         t = ff.timings()
+        kt = ff.kernel_timings()
         if rebuild:
             long_ms.append(t[2])
             build_ms.append(t[0])
+            if kt[2] >= 0:
+                klong_ms.append(kt[2])
         else:
             short_ms.append(t[1])
+            if kt[1] >= 0:
+                kshort_ms.append(kt[1])
+                prep_ms.append(kt[0])
     torch.cuda.synchronize()
     total_ms, pairs_all = aggregate(float(sum(step_ms)), float(pairs), device="cuda")
     value = pairs_all / (total_ms * 1e-3)
@@ -347,7 +354,10 @@ def run_gpu(args, rank, world, local_rank):
     if rank == 0:
         peak = ffma_peak(local_rank)
         t_short = statistics.median(short_ms) if short_ms else float("nan")
-        achieved = OPS_PER_PAIR * n_short / (t_short * 1e-3)
+        t_kshort = statistics.median(kshort_ms) if kshort_ms else float("nan")
+        t_klong = statistics.median(klong_ms) if klong_ms else float("nan")
+        achieved = OPS_PER_PAIR * n_short / (t_kshort * 1e-3)
+        achieved_window = OPS_PER_PAIR * n_short / (t_short * 1e-3)
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline_sample()
@@ -367,14 +377,19 @@ def run_gpu(args, rank, world, local_rank):
                           "parallelism": "replicas" if world > 1 else "single system"},
                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "roofline": {"bound": "fp32",
-                            "kernel": "short-range window: k_water_prep + k_water_force_it (deferred pairs in its last block)",
+                            "kernel": "short-range water force kernel (k_water_force_it, deferred pairs in its "
+                                      "last block), CUDA events around its launch on the library's stream",
                             "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Tops/s (FP32 pipe)",
                             "frac": achieved / peak, "traffic": SHORT_KERNEL_DRAM_BYTES,
                             "traffic_source": "ncu dram bytes of one short-range launch, recorded from a "
                                               "capture of this build's kernel (not measured by this run)",
                             "peak_source": "measured FFMA-chain kernel (gr_ffma_peak), one FFMA = one op",
-                            "ops_per_pair": OPS_PER_PAIR, "short_kernel_ms": t_short,
-                            "long_kernel_ms": statistics.median(long_ms) if long_ms else None},
+                            "ops_per_pair": OPS_PER_PAIR, "short_kernel_ms": t_kshort,
+                            "prep_kernel_ms": statistics.median(prep_ms) if prep_ms else None,
+                            "short_window_ms": t_short, "frac_short_window": achieved_window / peak,
+                            "long_kernel_ms": t_klong,
+                            "frac_long_kernel": OPS_PER_PAIR * n_long / (t_klong * 1e-3) / peak,
+                            "long_window_ms": statistics.median(long_ms) if long_ms else None},
                "pairlist": pairlist_summary(s, n_short, n_long, build_ms, ms_per_step),
                "md": md, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches}
     ff.close()

@@ -99,6 +99,9 @@ void NbSystem::release() {
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : ev) e = nullptr;
+    for (auto& e : evk)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : evk) e = nullptr;
     if (ev_err) cudaEventDestroy(ev_err);
     ev_err = nullptr;
     if (err_host) cudaFreeHost(err_host);
@@ -415,6 +418,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     GR_CUDA(cudaMemset(h.e64_long, 0, 16 * sizeof(double)));
     GR_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_sys), sizeof(SysDev)));
     for (auto& e : ev) GR_CUDA(cudaEventCreate(&e));
+    for (auto& e : evk) GR_CUDA(cudaEventCreate(&e));
     GR_CUDA(cudaEventCreateWithFlags(&ev_err, cudaEventDisableTiming));
     if (!err_host) GR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&err_host), 4 * sizeof(int)));
     err_host[0] = 0;
@@ -460,8 +464,8 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
         set_error("gr_nb_params: the pair-stream layout supports cluster_size 4 only");
         return GR_ERR_INVALID;
     }
-    if (p->water_layout < 0 || p->water_layout > 3) {
-        set_error("gr_nb_params: water_layout must be 0, 1, 2 or 3");
+    if (p->water_layout < 0 || p->water_layout > 4) {
+        set_error("gr_nb_params: water_layout must be 0, 1, 2, 3 or 4");
         return GR_ERR_INVALID;
     }
     if (p->list_capacity < 0) {
@@ -487,9 +491,10 @@ gr_status NbSystem::set_params(const gr_nb_params* p) {
     // water kernel layout: 1 = lanes share the mask bits (width 4 only),
     // 2 = each lane iterates over its own bits (width 4 or 8), 3 = each lane
     // streams its own water pairs over units of two clusters (width 4; short
-    // range, the long range runs layout 2)
-    layout = p->water_layout == 1 ? 1 : (p->water_layout == 3 ? 3 : 2);
-    W = (layout == 2 && p->cluster_size == 8) ? 8 : 4;
+    // range, the long range runs layout 2), 4 = layout 2 with the atom pairs
+    // evaluated two at a time in packed FP32x2 arithmetic (width 4 or 8)
+    layout = p->water_layout == 1 ? 1 : p->water_layout == 3 ? 3 : p->water_layout == 4 ? 4 : 2;
+    W = ((layout == 2 || layout == 4) && p->cluster_size == 8) ? 8 : 4;
     h.W = W;
     clus_alloc = 0;  // cluster arrays depend on W
     wcap_want = 0;   // list capacity from the (new) parameters
@@ -859,6 +864,10 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
     // just the first and last (the step's total device time)
     const bool stage = record_events && !in_capture;
     if (stage) last_staged = true;
+    if (stage) {
+        evk_valid = prm.kernel == GR_KERNEL_FIXED && NCG > NSCG;
+        evk_long = false;
+    }
     if (record_events) GR_CUDA(record_event(ev[0], s));
     if (rebuild) {
         // the first build of a system synchronises to size the list capacities
@@ -899,7 +908,9 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
         if (NCG > NSCG) {
             wp = water_params();
             if (!prepped) (++launches, k_water_prep<<<blocks_for(NCG - NSCG, 128), 128, 0, s>>>(d_sys));
+            if (stage) GR_CUDA(record_event(evk[0], s));
             if ((st = launch_water(s, wp, false))) return st;
+            if (stage) GR_CUDA(record_event(evk[1], s));
         }
         // solute work items: (CG, chunk of list entries), 4 warps per block
         const unsigned sgrid = std::max(1u, std::min(blocks_for((long long)NSCG * ((h.scap + kSoluteChunk - 1) / kSoluteChunk), 4),
@@ -912,10 +923,13 @@ gr_status NbSystem::eval(cudaStream_t s, int flags, bool record_events) {
             if (NCG > NSCG)
                 GR_CUDA(cudaMemsetAsync(h.fs_long, 0, size_t(h.max_clusters) * W * 9 * sizeof(long long), s));
             if (NCG > NSCG) {
+                if (stage) GR_CUDA(record_event(evk[2], s));
                 if ((st = launch_water(s, wp, true))) return st;
+                if (stage) GR_CUDA(record_event(evk[3], s));
             }
             if (NSCG > 0) (++launches, k_solute_force<true><<<sgrid, 128, shg, s>>>(d_sys));
             lr_computed = true;
+            if (stage && NCG > NSCG) evk_long = true;
         }
     } else {
         if (NCG > NSCG && !prepped)  // per-step water data incl. the solvent excluded energies
@@ -1111,6 +1125,17 @@ WaterScaled NbSystem::water_scaled(const WaterParams& wp) const {
         pp.c12f[t] = float(12.0 * double(wp.c12[t]) * sc);
     }
     pp.crfc_sumq = float(h.crf_cut * w_qq_sum);
+    for (int u = 0; u < 4; ++u) {
+        const int t0 = unit_t(u, 0), t1 = unit_t(u, 1);
+        pp.pqf[u] = make_float2(pp.qf[t0], pp.qf[t1]);
+        pp.pqcf[u] = make_float2(pp.qcf[t0], pp.qcf[t1]);
+        pp.pqq[u] = make_float2(wp.qq[t0], wp.qq[t1]);
+        pp.pc12[u] = make_float2(wp.c12[t0], wp.c12[t1]);
+        pp.pnc6[u] = make_float2(-wp.c6[t0], -wp.c6[t1]);
+        pp.pc12f[u] = make_float2(pp.c12f[t0], pp.c12f[t1]);
+        pp.pnc6f[u] = make_float2(-pp.c6f[t0], -pp.c6f[t1]);
+    }
+    pp.ncrf2 = make_float2(-wp.crf2, -wp.crf2);
     return pp;
 }
 
@@ -1132,8 +1157,15 @@ gr_status NbSystem::launch_water(cudaStream_t s, const WaterParams& wp, bool lr)
     do {                                                                                                 \
         const size_t smem = water_it_smem<WW>();                                                         \
         int occ = 1;                                                                                     \
-        GR_CUDA(occupancy(k_water_force_it<WW, LJ, LL>, 128, smem, &occ));                               \
-        (++launches, k_water_force_it<WW, LJ, LL><<<water_grid(sm * occ), 128, smem, s>>>(d_sys, wp, ws)); \
+        if (layout == 4) {                                                                               \
+            GR_CUDA(occupancy(k_water_force_it<WW, LJ, LL, true>, 128, smem, &occ));                     \
+            (++launches,                                                                                 \
+             k_water_force_it<WW, LJ, LL, true><<<water_grid(sm * occ), 128, smem, s>>>(d_sys, wp, ws));   \
+        } else {                                                                                         \
+            GR_CUDA(occupancy(k_water_force_it<WW, LJ, LL, false>, 128, smem, &occ));                    \
+            (++launches,                                                                                 \
+             k_water_force_it<WW, LJ, LL, false><<<water_grid(sm * occ), 128, smem, s>>>(d_sys, wp, ws));  \
+        }                                                                                                \
     } while (0)
 #define GR_WATER_SHARED(LJ, LL)                                                                          \
     do {                                                                                                 \
@@ -1673,6 +1705,26 @@ gr_status gr_last_timings(gr_ctx* ctx, float ms[5]) {
         ms[0] = ms[1] = ms[2] = ms[3] = -1.f;  // a graph step: its total only
     }
     cudaEventElapsedTime(&ms[4], S.ev[0], S.ev[4]);
+    return GR_OK;
+}
+
+gr_status gr_last_kernel_timings(gr_ctx* ctx, float ms[3]) {
+    CTX_GUARD(ctx);
+    if (!ms) {
+        set_error("gr_last_kernel_timings: null ms");
+        return GR_ERR_INVALID;
+    }
+    NbSystem& S = ctx->sys;
+    if (cudaEventSynchronize(S.ev[4]) != cudaSuccess) {
+        set_error("no timed evaluation");
+        return GR_ERR_STATE;
+    }
+    ms[0] = ms[1] = ms[2] = -1.f;
+    if (S.last_staged && S.evk_valid) {
+        cudaEventElapsedTime(&ms[0], S.ev[1], S.evk[0]);
+        cudaEventElapsedTime(&ms[1], S.evk[0], S.evk[1]);
+        if (S.evk_long) cudaEventElapsedTime(&ms[2], S.evk[2], S.evk[3]);
+    }
     return GR_OK;
 }
 

@@ -23,7 +23,7 @@ template <bool LJ00, bool LONG>
 __global__ void k_water_force(const SysDev* __restrict__ sys, const WaterParams wp);
 template <bool LJ00, bool LONG>
 __global__ void k_water_deferred(const SysDev* __restrict__ sys, const WaterParams wp);
-template <int W, bool LJ00, bool LONG>
+template <int W, bool LJ00, bool LONG, bool PK>
 __global__ void k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp, const WaterScaled ws);
 template <bool LONG>
 __global__ void k_solute_force(const SysDev* __restrict__ sys);

@@ -78,6 +78,11 @@ class NbSystem {
     int regrow_count = 0;
     size_t bytes = 0;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // kernel-level events of a staged evaluation: after the water prep, after the
+    // short-range water kernel, around the long-range water kernel
+    cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool evk_valid = false;  // the last staged evaluation recorded evk (a solvent, fixed-point kernel)
+    bool evk_long = false;   // ... and ran the long-range water kernel
     cudaEvent_t ev_err = nullptr;
     int* err_host = nullptr;  // pinned copy of the device error flags
     bool pending_check = false, ever_built = false;

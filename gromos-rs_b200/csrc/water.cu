@@ -51,7 +51,20 @@ struct WaterScaled {
     float c6f[9];    // 6 c6 2^32
     float c12f[9];   // 12 c12 2^32
     float crfc_sumq; // crf_cut * sum over the 9 atom pairs of q_a q_b fpe (one water pair's constant CRF term)
+    // The packed (FP32x2) kernel evaluates the eight atom pairs other than
+    // first-first as four pairs of pairs ("units"), one per 64-bit register
+    // pair: u = 0: (0,1)|(0,2), 1: (1,0)|(2,0), 2: (1,1)|(2,2), 3: (1,2)|(2,1)
+    // (t = 3 a + b of the lo and hi half).  The constants of both halves:
+    float2 pqf[4], pqcf[4], pqq[4];  // qf, qcf, qq (energy, unscaled)
+    float2 pc12[4], pnc6[4];         // c12, -c6 (energy)
+    float2 pc12f[4], pnc6f[4];       // 12 c12 2^32, -6 c6 2^32 (force)
+    float2 ncrf2;                    // -crf_2cut3i in both halves
 };
+
+// The (lo, hi) atom-pair index t of packed unit u (see WaterScaled).
+__host__ __device__ constexpr int unit_t(int u, int half) {
+    return half == 0 ? (u == 0 ? 1 : u == 1 ? 3 : u == 2 ? 4 : 5) : (u == 0 ? 2 : u == 1 ? 6 : u == 2 ? 8 : 7);
+}
 
 __device__ __forceinline__ float rsqrt_fast(float x) {
     float y;
@@ -516,6 +529,336 @@ __device__ __forceinline__ void process_deferred(const SysDev& s, const WaterPar
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32x2 evaluation (layout 4).  Blackwell executes one FP32x2
+// instruction (fma/add/mul .f32x2) for two lanes' worth of FP32 work per
+// issue slot, so the eight atom pairs of a water pair other than first-first
+// are evaluated as four packed units (see WaterScaled) and the first-first
+// pair, the only one with Lennard-Jones terms in SPC-like solvents, in scalar
+// arithmetic.  Per unit the i and j operands sit in 64-bit register pairs:
+//   u = 0 (0,1)|(0,2): i {p0, p0},  j {q1, q2};  i-force -> F00, j-force -> G12
+//   u = 1 (1,0)|(2,0): i {p1, p2},  j {q0, q0};  i-force -> F12, j-force -> G00
+//   u = 2 (1,1)|(2,2): i {p1, p2},  j {q1, q2};  i-force -> F12, j-force -> G12
+//   u = 3 (1,2)|(2,1): i {p1, p2},  j {q2, q1};  i-force -> F12, j-force -> G21
+// so that every accumulator is a register pair too: the i rows hold F00 =
+// {f0 part, f0 part} and F12 = {f1, f2}; the j sums G00 = {g0 part, g0 part},
+// G12 = {g1, g2}, G21 = {g2, g1} (accumulated with the i sign and negated once
+// per entry).  The arithmetic per atom pair is that of water_pair_math.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+template <bool LJ00, int U>
+__device__ __forceinline__ void packed_unit(float2 X, float2 Y, float2 Z, float2 R2, float2& Fx, float2& Fy,
+                                            float2& Fz, float2& Gx, float2& Gy, float2& Gz, float2& E, float2& EL,
+                                            const WaterScaled& ws) {
+    const float2 RI = make_float2(rsqrt_fast(R2.x), rsqrt_fast(R2.y));
+    const float2 RI2 = mul2(RI, RI);
+    float2 FS = fma2(ws.pqf[U], mul2(RI2, RI), ws.pqcf[U]);
+    E = fma2(ws.pqq[U], fma2(ws.ncrf2, R2, RI), E);
+    if (!LJ00) {
+        const float2 RI6 = mul2(mul2(RI2, RI2), RI2);
+        EL = fma2(fma2(ws.pc12[U], RI6, ws.pnc6[U]), RI6, EL);
+        FS = fma2(fma2(ws.pc12f[U], RI6, ws.pnc6f[U]), mul2(RI6, RI2), FS);
+    }
+    Fx = fma2(X, FS, Fx);
+    Fy = fma2(Y, FS, Fy);
+    Fz = fma2(Z, FS, Fz);
+    Gx = fma2(X, FS, Gx);
+    Gy = fma2(Y, FS, Gy);
+    Gz = fma2(Z, FS, Gz);
+}
+
+// One j-water entry of the bit-iterating kernel, packed: the CG-pair image,
+// every set bit of the mask (i water k of the cluster), the j-part of the
+// virial and the j forces (reductions, or staged in st for the long range).
+template <bool LJ00, bool LONG>
+__device__ __forceinline__ void water_entry_packed(const SysDev& s, const WaterParams& wp, const WaterScaled& pp,
+                                                   const float4* __restrict__ sp, float4* __restrict__ myrow,
+                                                   const float4* __restrict__ jrec, double x00, double y00, double z00,
+                                                   float limx, float limy, float limz, int base, int js, unsigned mask,
+                                                   long long* __restrict__ FS, long long* __restrict__ st, float& ecrf,
+                                                   float& elj, float2& ecrf2, float2& elj2, float& v0s, float& v1s,
+                                                   float& v2s, float& v3s, float& v4s, float& v5s, int& n_wp) {
+    const float4 r0 = jrec[0], r1 = jrec[1], r2 = jrec[2];
+    double dx = x00 - rec_x(r0), dy = y00 - rec_y(r0), dz = z00 - rec_x(r1);
+    if (wp.boundary) {
+        dx -= wp.box[0] * rint(dx * wp.inv_box[0]);
+        dy -= wp.box[1] * rint(dy * wp.inv_box[1]);
+        dz -= wp.box[2] * rint(dz * wp.inv_box[2]);
+    }
+    // j atoms relative to the cluster origin: q0 = -D, q1, q2
+    const float Dx = float(dx), Dy = float(dy), Dz = float(dz);
+    const float q1x = r1.z - Dx, q1y = r1.w - Dy, q1z = r2.x - Dz;
+    const float q2x = r2.y - Dx, q2y = r2.z - Dy, q2z = r2.w - Dz;
+    // negated j operands: X = P + N equals P - Q exactly
+    const float2 N0x = make_float2(Dx, Dx), N0y = make_float2(Dy, Dy), N0z = make_float2(Dz, Dz);
+    const float2 N12x = make_float2(-q1x, -q2x), N12y = make_float2(-q1y, -q2y), N12z = make_float2(-q1z, -q2z);
+    const float2 N21x = make_float2(-q2x, -q1x), N21y = make_float2(-q2y, -q1y), N21z = make_float2(-q2z, -q1z);
+    const float2 zero2 = make_float2(0.f, 0.f);
+    float2 G00x = zero2, G00y = zero2, G00z = zero2, G12x = zero2, G12y = zero2, G12z = zero2;
+    float2 G21x = zero2, G21y = zero2, G21z = zero2;
+    while (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const float4 B = sp[k * 3], C = sp[k * 3 + 1], E4 = sp[k * 3 + 2];
+        float2 P0x = make_float2(B.x, B.y), P0y = make_float2(B.z, B.w), P0z = make_float2(C.x, C.y);
+        float2 P12x = make_float2(C.z, C.w), P12y = make_float2(E4.x, E4.y), P12z = make_float2(E4.z, E4.w);
+        // first-atom vector: decides whether the FP32 image is certain (as in
+        // the scalar kernel: FP32 re-image, else deferred to exact FP64)
+        float r0x = B.x + Dx, r0y = B.z + Dy, r0z = C.x + Dz;
+        float shx = 0.f, shy = 0.f, shz = 0.f;
+        bool shifted = false;
+        if (!(fabsf(r0x) < limx && fabsf(r0y) < limy && fabsf(r0z) < limz)) {
+            if (wp.boundary) {
+                shx = -wp.boxf[0] * rintf(r0x * wp.inv_boxf[0]);
+                shy = -wp.boxf[1] * rintf(r0y * wp.inv_boxf[1]);
+                shz = -wp.boxf[2] * rintf(r0z * wp.inv_boxf[2]);
+            }
+            r0x += shx;
+            r0y += shy;
+            r0z += shz;
+            if (!(fabsf(r0x) < limx && fabsf(r0y) < limy && fabsf(r0z) < limz)) {
+                const int d = atomicAdd(&s.n_deferred[LONG ? 1 : 0], 1);
+                if (d < s.defer_cap) {
+                    s.deferred[2 * (LONG ? s.defer_cap + d : d)] = base + k;
+                    s.deferred[2 * (LONG ? s.defer_cap + d : d) + 1] = js;
+                } else {
+                    atomicOr(&s.err[0], ERR_DEFER_OVERFLOW);
+                }
+                continue;
+            }
+            const float2 sx2 = make_float2(shx, shx), sy2 = make_float2(shy, shy), sz2 = make_float2(shz, shz);
+            P0x = add2(P0x, sx2);
+            P0y = add2(P0y, sy2);
+            P0z = add2(P0z, sz2);
+            P12x = add2(P12x, sx2);
+            P12y = add2(P12y, sy2);
+            P12z = add2(P12z, sz2);
+            shifted = true;
+        }
+        const float4 R0 = myrow[k * 3], R1 = myrow[k * 3 + 1], R2 = myrow[k * 3 + 2];
+        float2 F00x = make_float2(R0.x, R0.y), F00y = make_float2(R0.z, R0.w), F00z = make_float2(R1.x, R1.y);
+        float2 F12x = make_float2(R1.z, R1.w), F12y = make_float2(R2.x, R2.y), F12z = make_float2(R2.z, R2.w);
+        float gs0 = 0.f, gs1 = 0.f, gs2 = 0.f;
+        if (shifted) {
+            gs0 = G00x.x + G00x.y + G12x.x + G12x.y + G21x.x + G21x.y;
+            gs1 = G00y.x + G00y.y + G12y.x + G12y.y + G21y.x + G21y.y;
+            gs2 = G00z.x + G00z.y + G12z.x + G12z.y + G21z.x + G21z.y;
+        }
+        // atom-pair vectors i - j of the four units and the first-first pair
+        const float2 XA = add2(P0x, N12x), YA = add2(P0y, N12y), ZA = add2(P0z, N12z);
+        const float2 XB = add2(P12x, N0x), YB = add2(P12y, N0y), ZB = add2(P12z, N0z);
+        const float2 XC = add2(P12x, N12x), YC = add2(P12y, N12y), ZC = add2(P12z, N12z);
+        const float2 XD = add2(P12x, N21x), YD = add2(P12y, N21y), ZD = add2(P12z, N21z);
+        const float2 R2A = fma2(XA, XA, fma2(YA, YA, mul2(ZA, ZA)));
+        const float2 R2B = fma2(XB, XB, fma2(YB, YB, mul2(ZB, ZB)));
+        const float2 R2C = fma2(XC, XC, fma2(YC, YC, mul2(ZC, ZC)));
+        const float2 R2D = fma2(XD, XD, fma2(YD, YD, mul2(ZD, ZD)));
+        const float r2s = fmaf(r0x, r0x, fmaf(r0y, r0y, r0z * r0z));
+        const float m2 = fminf(fminf(fminf(r2s, fminf(R2A.x, R2A.y)), fminf(R2B.x, R2B.y)),
+                               fminf(fminf(R2C.x, R2C.y), fminf(R2D.x, R2D.y)));
+        if (m2 >= 1e-10f) {
+            {  // first-first pair, scalar, with Lennard-Jones
+                const float ri = rsqrt_fast(r2s);
+                const float ri2 = ri * ri;
+                float fs = fmaf(pp.qf[0], ri2 * ri, pp.qcf[0]);
+                ecrf = fmaf(wp.qq[0], fmaf(-wp.crf2, r2s, ri), ecrf);
+                const float ri6 = ri2 * ri2 * ri2;
+                elj = fmaf(fmaf(wp.c12[0], ri6, -wp.c6[0]), ri6, elj);
+                fs = fmaf(fmaf(pp.c12f[0], ri6, -pp.c6f[0]), ri6 * ri2, fs);
+                F00x.x = fmaf(r0x, fs, F00x.x);
+                F00y.x = fmaf(r0y, fs, F00y.x);
+                F00z.x = fmaf(r0z, fs, F00z.x);
+                G00x.x = fmaf(r0x, fs, G00x.x);
+                G00y.x = fmaf(r0y, fs, G00y.x);
+                G00z.x = fmaf(r0z, fs, G00z.x);
+            }
+            packed_unit<LJ00, 0>(XA, YA, ZA, R2A, F00x, F00y, F00z, G12x, G12y, G12z, ecrf2, elj2, pp);
+            packed_unit<LJ00, 1>(XB, YB, ZB, R2B, F12x, F12y, F12z, G00x, G00y, G00z, ecrf2, elj2, pp);
+            packed_unit<LJ00, 2>(XC, YC, ZC, R2C, F12x, F12y, F12z, G12x, G12y, G12z, ecrf2, elj2, pp);
+            packed_unit<LJ00, 3>(XD, YD, ZD, R2D, F12x, F12y, F12z, G21x, G21y, G21z, ecrf2, elj2, pp);
+        } else {
+            // an atom pair at r^2 < 1e-10: scalar, with the reference's zeros
+            const float xs[9] = {r0x, XA.x, XA.y, XB.x, XC.x, XD.x, XB.y, XD.y, XC.y};
+            const float ys[9] = {r0y, YA.x, YA.y, YB.x, YC.x, YD.x, YB.y, YD.y, YC.y};
+            const float zs[9] = {r0z, ZA.x, ZA.y, ZB.x, ZC.x, ZD.x, ZB.y, ZD.y, ZC.y};
+            const float rs[9] = {r2s, R2A.x, R2A.y, R2B.x, R2C.x, R2D.x, R2B.y, R2D.y, R2C.y};
+            float fx[9], fy[9], fz[9];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                fx[t] = fy[t] = fz[t] = 0.f;
+                if (rs[t] < 1e-10f) {
+                    ecrf = fmaf(wp.qq[t], wp.crfc, ecrf);
+                    continue;
+                }
+                const float ri = rsqrt_fast(rs[t]);
+                const float ri2 = ri * ri;
+                float fs = fmaf(pp.qf[t], ri2 * ri, pp.qcf[t]);
+                ecrf = fmaf(wp.qq[t], fmaf(-wp.crf2, rs[t], ri), ecrf);
+                if (!LJ00 || t == 0) {
+                    const float ri6 = ri2 * ri2 * ri2;
+                    elj = fmaf(fmaf(wp.c12[t], ri6, -wp.c6[t]), ri6, elj);
+                    fs = fmaf(fmaf(pp.c12f[t], ri6, -pp.c6f[t]), ri6 * ri2, fs);
+                }
+                fx[t] = xs[t] * fs;
+                fy[t] = ys[t] * fs;
+                fz[t] = zs[t] * fs;
+            }
+            // i: atom 0 <- t 0, 1, 2; atom 1 <- 3, 4, 5; atom 2 <- 6, 7, 8
+            F00x.x += fx[0] + fx[1];
+            F00y.x += fy[0] + fy[1];
+            F00z.x += fz[0] + fz[1];
+            F00x.y += fx[2];
+            F00y.y += fy[2];
+            F00z.y += fz[2];
+            F12x.x += fx[3] + fx[4] + fx[5];
+            F12y.x += fy[3] + fy[4] + fy[5];
+            F12z.x += fz[3] + fz[4] + fz[5];
+            F12x.y += fx[6] + fx[7] + fx[8];
+            F12y.y += fy[6] + fy[7] + fy[8];
+            F12z.y += fz[6] + fz[7] + fz[8];
+            // j: atom 0 <- t 0, 3, 6; atom 1 <- 1, 4, 7; atom 2 <- 2, 5, 8
+            G00x.x += fx[0] + fx[3];
+            G00y.x += fy[0] + fy[3];
+            G00z.x += fz[0] + fz[3];
+            G00x.y += fx[6];
+            G00y.y += fy[6];
+            G00z.y += fz[6];
+            G12x.x += fx[1] + fx[4];
+            G12y.x += fy[1] + fy[4];
+            G12z.x += fz[1] + fz[4];
+            G12x.y += fx[2] + fx[8];
+            G12y.y += fy[2] + fy[8];
+            G12z.y += fz[2] + fz[8];
+            G21x.x += fx[5];
+            G21y.x += fy[5];
+            G21z.x += fz[5];
+            G21x.y += fx[7];
+            G21y.y += fy[7];
+            G21z.y += fz[7];
+        }
+        myrow[k * 3] = make_float4(F00x.x, F00x.y, F00y.x, F00y.y);
+        myrow[k * 3 + 1] = make_float4(F00z.x, F00z.y, F12x.x, F12x.y);
+        myrow[k * 3 + 2] = make_float4(F12y.x, F12y.y, F12z.x, F12z.y);
+        ++n_wp;
+        if (shifted) {  // shift (x) sum_a fi_a = shift (x) (change of the j sums with the i sign)
+            const float sx = G00x.x + G00x.y + G12x.x + G12x.y + G21x.x + G21x.y - gs0;
+            const float sy = G00y.x + G00y.y + G12y.x + G12y.y + G21y.x + G21y.y - gs1;
+            const float sz = G00z.x + G00z.y + G12z.x + G12z.y + G21z.x + G21z.y - gs2;
+            v0s = fmaf(shx, sx, v0s);
+            v1s = fmaf(shx, sy, v1s);
+            v2s = fmaf(shx, sz, v2s);
+            v3s = fmaf(shy, sy, v3s);
+            v4s = fmaf(shy, sz, v4s);
+            v5s = fmaf(shz, sz, v5s);
+        }
+    }
+    // the j forces g_b = -(sums with the i sign)
+    const float gx[3] = {-(G00x.x + G00x.y), -(G12x.x + G21x.y), -(G12x.y + G21x.x)};
+    const float gy[3] = {-(G00y.x + G00y.y), -(G12y.x + G21y.y), -(G12y.y + G21y.x)};
+    const float gz[3] = {-(G00z.x + G00z.y), -(G12z.x + G21z.y), -(G12z.y + G21z.x)};
+    const float qx[3] = {-Dx, q1x, q2x}, qy[3] = {-Dy, q1y, q2y}, qz[3] = {-Dz, q1z, q2z};
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {  // the j-part of the virial: Q_b (x) g_b
+        v0s = fmaf(qx[b], gx[b], v0s);
+        v1s = fmaf(qx[b], gy[b], v1s);
+        v2s = fmaf(qx[b], gz[b], v2s);
+        v3s = fmaf(qy[b], gy[b], v3s);
+        v4s = fmaf(qy[b], gz[b], v4s);
+        v5s = fmaf(qz[b], gz[b], v5s);
+    }
+    if (LONG) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {  // the forces carry the 2^32 scale already
+            st[3 * b] = __float2ll_rn(gx[b]);
+            st[3 * b + 1] = __float2ll_rn(gy[b]);
+            st[3 * b + 2] = __float2ll_rn(gz[b]);
+        }
+    } else {
+        long long* __restrict__ fj = FS + static_cast<size_t>(js) * 9;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            red_add(fj + 3 * b, __float2ll_rn(gx[b]));
+            red_add(fj + 3 * b + 1, __float2ll_rn(gy[b]));
+            red_add(fj + 3 * b + 2, __float2ll_rn(gz[b]));
+        }
+    }
+}
+
+// Cluster end of the packed kernel: column sums of the lane rows (lane c < 3W
+// sums float4 c of every row), per-atom i forces assembled from the packed
+// halves, their reductions, and the i-part of the virial P (x) F.  Called by
+// the whole warp (shuffles).
+template <int W>
+__device__ __forceinline__ void packed_column_sums(const float4* __restrict__ fis, const float4* __restrict__ sp,
+                                                   long long* __restrict__ fo_base, int lane, int n, float& v0s,
+                                                   float& v1s, float& v2s, float& v3s, float& v4s, float& v5s) {
+    constexpr int ROW = W * 3 + 1;
+    float4 S = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lane < W * 3) {
+#pragma unroll 8
+        for (int r = 0; r < 32; ++r) {
+            const float4 f = fis[r * ROW + lane];
+            S.x += f.x;
+            S.y += f.y;
+            S.z += f.z;
+            S.w += f.w;
+        }
+    }
+    const int k3 = (lane / 3) * 3;
+    float4 S0, S1, S2;
+    S0.x = __shfl_sync(0xffffffffu, S.x, k3);
+    S0.y = __shfl_sync(0xffffffffu, S.y, k3);
+    S0.z = __shfl_sync(0xffffffffu, S.z, k3);
+    S0.w = __shfl_sync(0xffffffffu, S.w, k3);
+    S1.x = __shfl_sync(0xffffffffu, S.x, k3 + 1);
+    S1.y = __shfl_sync(0xffffffffu, S.y, k3 + 1);
+    S1.z = __shfl_sync(0xffffffffu, S.z, k3 + 1);
+    S1.w = __shfl_sync(0xffffffffu, S.w, k3 + 1);
+    S2.x = __shfl_sync(0xffffffffu, S.x, k3 + 2);
+    S2.y = __shfl_sync(0xffffffffu, S.y, k3 + 2);
+    S2.z = __shfl_sync(0xffffffffu, S.z, k3 + 2);
+    S2.w = __shfl_sync(0xffffffffu, S.w, k3 + 2);
+    if (lane < W * 3 && lane / 3 < n) {
+        const int a = lane - k3;
+        float sx, sy, sz, px, py, pz;
+        const float4 B = sp[k3], C = sp[k3 + 1], E4 = sp[k3 + 2];
+        if (a == 0) {
+            sx = S0.x + S0.y;
+            sy = S0.z + S0.w;
+            sz = S1.x + S1.y;
+            px = B.x;
+            py = B.z;
+            pz = C.x;
+        } else if (a == 1) {
+            sx = S1.z;
+            sy = S2.x;
+            sz = S2.z;
+            px = C.z;
+            py = E4.x;
+            pz = E4.z;
+        } else {
+            sx = S1.w;
+            sy = S2.y;
+            sz = S2.w;
+            px = C.w;
+            py = E4.y;
+            pz = E4.w;
+        }
+        long long* __restrict__ fo = fo_base + 3 * lane;
+        red_add(fo, __float2ll_rn(sx));
+        red_add(fo + 1, __float2ll_rn(sy));
+        red_add(fo + 2, __float2ll_rn(sz));
+        v0s = fmaf(px, sx, v0s);
+        v1s = fmaf(px, sy, v1s);
+        v2s = fmaf(px, sz, v2s);
+        v3s = fmaf(py, sy, v3s);
+        v4s = fmaf(py, sz, v4s);
+        v5s = fmaf(pz, sz, v5s);
+    }
+}
+
 // Bit-iterating layout: one warp per i-cluster of W waters, one lane per
 // j-water entry; each lane loops over the set bits of its own mask only, so
 // no lane idles on another lane's bits (entries are sorted by popcount, so
@@ -523,7 +866,7 @@ __device__ __forceinline__ void process_deferred(const SysDev& s, const WaterPar
 // read from shared memory by bit index; i-forces accumulate in a lane-private
 // shared-memory row (no atomics, so the result does not depend on the order
 // of lanes) and the rows are summed once per cluster.
-template <int W, bool LJ00, bool LONG>
+template <int W, bool LJ00, bool LONG, bool PK>
 __global__ void __launch_bounds__(128, 3)
     k_water_force_it(const SysDev* __restrict__ sys, const WaterParams wp, const WaterScaled pp) {
     constexpr int ROW = W * 3 + 1;  // float4 per lane row (+1 keeps 8 consecutive lanes on distinct banks)
@@ -616,6 +959,7 @@ __global__ void __launch_bounds__(128, 3)
         __syncwarp();
         const double x00 = rec_x(ibuf[wid][ib][0]), y00 = rec_y(ibuf[wid][ib][0]);
         const double z00 = rec_x(ibuf[wid][ib][1]);
+        float4 pk_p = make_float4(0.f, 0.f, 0.f, 0.f);
         if (lane < W * 3) {
             const int k = lane / 3, a = lane % 3;
             float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -628,9 +972,26 @@ __global__ void __launch_bounds__(128, 3)
                 p.y = float(rec_y(v0) - y00) + dy;
                 p.z = float(rec_x(v1) - z00) + dz;
             }
-            sp[lane] = p;
+            if (!PK) sp[lane] = p;
+            pk_p = p;
+        }
+        if constexpr (PK) {
+            // water k's three float4: {p0x, p0x, p0y, p0y}, {p0z, p0z, p1x, p2x},
+            // {p1y, p2y, p1z, p2z} (the operand pairs of the packed units)
+            const int k3 = (lane / 3) * 3;
+            const float a0x = __shfl_sync(0xffffffffu, pk_p.x, k3), a0y = __shfl_sync(0xffffffffu, pk_p.y, k3);
+            const float a0z = __shfl_sync(0xffffffffu, pk_p.z, k3);
+            const float a1x = __shfl_sync(0xffffffffu, pk_p.x, k3 + 1), a1y = __shfl_sync(0xffffffffu, pk_p.y, k3 + 1);
+            const float a1z = __shfl_sync(0xffffffffu, pk_p.z, k3 + 1);
+            const float a2x = __shfl_sync(0xffffffffu, pk_p.x, k3 + 2), a2y = __shfl_sync(0xffffffffu, pk_p.y, k3 + 2);
+            const float a2z = __shfl_sync(0xffffffffu, pk_p.z, k3 + 2);
+            const int r = lane - k3;
+            if (lane < W * 3)
+                sp[lane] = r == 0 ? make_float4(a0x, a0x, a0y, a0y)
+                                  : (r == 1 ? make_float4(a0z, a0z, a1x, a2x) : make_float4(a1y, a2y, a1z, a2z));
         }
         float elj = 0.f, ecrf = 0.f, v0s = 0.f, v1s = 0.f, v2s = 0.f, v3s = 0.f, v4s = 0.f, v5s = 0.f;
+        float2 ecrf2 = make_float2(0.f, 0.f), elj2 = make_float2(0.f, 0.f);  // packed units' energies
         int n_wp = 0;  // water pairs evaluated (the CRF constant term is added per pair at the end)
         uint32_t e_cur_n = 0u, e_nx_n = 0u;
         for (int c = 0; c < nch; ++c) {
@@ -660,7 +1021,11 @@ __global__ void __launch_bounds__(128, 3)
             unsigned mask = e_cur & 0xffu;
             const int js = static_cast<int>(e_cur >> 8);
             if (LONG) jsl[wid][lane] = mask ? js : -1;
-            if (mask) {
+            if (PK && mask) {
+                water_entry_packed<LJ00, LONG>(s, wp, pp, sp, myrow, jbuf[wid][jb] + 3 * lane, x00, y00, z00, limx,
+                                               limy, limz, base, js, mask, FS, LONG ? jst[wid] + lane * 9 : nullptr,
+                                               ecrf, elj, ecrf2, elj2, v0s, v1s, v2s, v3s, v4s, v5s, n_wp);
+            } else if (mask) {
                 const float4 r0 = jbuf[wid][jb][3 * lane], r1 = jbuf[wid][jb][3 * lane + 1], r2 = jbuf[wid][jb][3 * lane + 2];
                 double dx = x00 - rec_x(r0), dy = y00 - rec_y(r0), dz = z00 - rec_x(r1);
                 if (wp.boundary) {
@@ -809,7 +1174,10 @@ __global__ void __launch_bounds__(128, 3)
         }
         __syncwarp();
         // column sums of the lane rows: lane c < 3W owns i atom c (water c / 3)
-        if (lane < W * 3) {
+        if constexpr (PK) {
+            packed_column_sums<W>(fis, sp, FS + static_cast<size_t>(base) * 9, lane, n, v0s, v1s, v2s, v3s, v4s,
+                                  v5s);
+        } else if (lane < W * 3) {
             float sx = 0.f, sy = 0.f, sz = 0.f;
 #pragma unroll 8
             for (int r = 0; r < 32; ++r) {
@@ -836,6 +1204,10 @@ __global__ void __launch_bounds__(128, 3)
         __syncwarp();
 #pragma unroll
         for (int cc = 0; cc < W * 3; ++cc) myrow[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (PK) {
+            elj += elj2.x + elj2.y;
+            ecrf += ecrf2.x + ecrf2.y;
+        }
         acc[0] += to_fixed_f(elj, 16777216.0f);
         acc[1] += to_fixed_f(fmaf(-pp.crfc_sumq, float(n_wp), ecrf), 16777216.0f);
         // the virial sums carry the forces' 2^32; its fixed point is 2^24
@@ -907,12 +1279,20 @@ template __global__ void k_water_force<false, true>(const SysDev*, const WaterPa
 }  // namespace gnb
 
 namespace gnb {
-template __global__ void k_water_force_it<4, true, false>(const SysDev*, const WaterParams, const WaterScaled);
-template __global__ void k_water_force_it<4, true, true>(const SysDev*, const WaterParams, const WaterScaled);
-template __global__ void k_water_force_it<4, false, false>(const SysDev*, const WaterParams, const WaterScaled);
-template __global__ void k_water_force_it<4, false, true>(const SysDev*, const WaterParams, const WaterScaled);
-template __global__ void k_water_force_it<8, true, false>(const SysDev*, const WaterParams, const WaterScaled);
-template __global__ void k_water_force_it<8, true, true>(const SysDev*, const WaterParams, const WaterScaled);
-template __global__ void k_water_force_it<8, false, false>(const SysDev*, const WaterParams, const WaterScaled);
-template __global__ void k_water_force_it<8, false, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, true, false, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, true, true, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, false, false, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, false, true, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, true, false, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, true, true, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, false, false, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, false, true, false>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, true, false, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, true, true, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, false, false, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<4, false, true, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, true, false, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, true, true, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, false, false, true>(const SysDev*, const WaterParams, const WaterScaled);
+template __global__ void k_water_force_it<8, false, true, true>(const SysDev*, const WaterParams, const WaterScaled);
 }  // namespace gnb

@@ -132,6 +132,7 @@ _SIGNATURES = {
     "gr_forces_device": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "gr_result_download": (C.c_int32, [C.c_void_p, C.POINTER(GrResult)]),
     "gr_last_timings": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
+    "gr_last_kernel_timings": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
     "gr_ctx_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_ffma_peak": (C.c_int32, [C.c_int, C.POINTER(C.c_double)]),
     "gr_md_init": (C.c_int32, [C.c_void_p, _f64p, _f64p, C.POINTER(GrMdParams)]),

@@ -221,6 +221,13 @@ class Forcefield:
         check(self._L.gr_last_timings(self._h, ms))
         return list(ms)
 
+    def kernel_timings(self) -> List[float]:
+        """[water prep, short-range water kernel, long-range water kernel] in ms of the last
+        kernel-by-kernel evaluation (-1 where a kernel did not run)."""
+        ms = (C.c_float * 3)()
+        check(self._L.gr_last_kernel_timings(self._h, ms))
+        return list(ms)
+
     def launches(self) -> int:
         n = C.c_int64(0)
         check(self._L.gr_ctx_launches(self._h, C.byref(n)))

@@ -188,6 +188,14 @@ gr_status gr_result_download(gr_ctx* ctx, gr_result* out);
  * recorded graph (GR_EVAL_GRAPH) records only its first and last event (the
  * step's device time, [4]); [0]-[3] read -1 for it. */
 gr_status gr_last_timings(gr_ctx* ctx, float ms[5]);
+/* Device-event timing of single kernels of the last evaluation, in ms, when it
+ * was launched kernel by kernel (not from a graph) with solvent and the
+ * fixed-point kernel: [0] the per-step water records (k_water_prep; ~0 when
+ * the MD step wrote them), [1] the short-range water force kernel, [2] the
+ * long-range water force kernel (-1 when that step kept the twin-range
+ * cache).  Entries that do not apply read -1.  Part of the same stage timing
+ * as gr_last_timings (Forcefield::apply has no kernel-level timers). */
+gr_status gr_last_kernel_timings(gr_ctx* ctx, float ms[3]);
 
 /* ---- measurement utilities (no counterpart in gromos-rs) ---------------- */
 /* Kernels launched by this context since creation (for launch accounting). */

@@ -183,7 +183,7 @@ def test_solute_small_box_per_atom_images():
     compare_eval(s, "fixed", steps=3, move=0.002)
 
 
-WATER_KERNELS = [(1, 4), (2, 4), (2, 8), (3, 4)]
+WATER_KERNELS = [(1, 4), (2, 4), (2, 8), (3, 4), (4, 4), (4, 8)]
 
 
 @pytest.mark.parametrize("layout,width", WATER_KERNELS)
