@@ -122,6 +122,7 @@ void NbSystem::release() {
     md_vel = md_mass = md_inv_mass = md_pos_snap = md_vel_snap = nullptr;
     md_ke = nullptr;
     md_ke_snap = nullptr;
+    md_t0 = nullptr;
     md_psnap_pos = md_psnap_vel = nullptr;
     md_psnap_ke = nullptr;
     md_psnap_valid = false;

@@ -28,7 +28,9 @@ struct MdDev {
     long long* ke;            // [3]: [0] kinetic energy of the velocities entering the step, [1] accumulator
                               // of the velocities leaving it (fixed point 2^24), [2] blocks finished
     int* failures;            // [1] molecules SETTLE could not solve
-    double t0, tau, dof;      // Berendsen bath (tau < 0: none)
+    const double* t0;         // [1] Berendsen bath temperature (device memory: a replica exchange changes it
+                              // without touching recorded graphs)
+    double tau, dof;          // Berendsen bath (tau < 0: none)
     int prep_next;            // also write the next step's water records (SETTLE units, no rebuild next)
 };
 
@@ -38,10 +40,11 @@ __device__ __forceinline__ double berendsen_lambda(const MdDev& md) {
     if (md.tau < 0.0) return 1.0;
     const double kB = 0.00831446261815324;
     const double ekin = double(md.ke[0]) / kEnergyScale;
+    const double t0 = *md.t0;
     double t = md.dof > 0.0 ? 2.0 * ekin / (md.dof * kB) : 0.0;
-    if (t < 1e-10) t = md.t0;
+    if (t < 1e-10) t = t0;
     if (t < 1e-10) return 1.0;
-    return md.tau == 0.0 ? sqrt(md.t0 / t) : sqrt(1.0 + md.dt / md.tau * (md.t0 / t - 1.0));
+    return md.tau == 0.0 ? sqrt(t0 / t) : sqrt(1.0 + md.dt / md.tau * (t0 / t - 1.0));
 }
 
 // Velocities scaled by `f` (temperature exchange), kinetic energy with them.
@@ -246,8 +249,9 @@ gr_status NbSystem::md_init(const double* mass, const double* vel, const gr_md_p
         (st = upload_array(&md_vel, v0.data(), size_t(N) * 3)) || (st = alloc(&md_pos_snap, size_t(N) * 3)) ||
         (st = alloc(&md_vel_snap, size_t(N) * 3)) || (st = alloc(&md_ke, 3)) || (st = alloc(&md_ke_snap, 1)) ||
         (st = alloc(&md_psnap_pos, size_t(N) * 3)) || (st = alloc(&md_psnap_vel, size_t(N) * 3)) ||
-        (st = alloc(&md_psnap_ke, 1)) || (st = alloc(&md_fail, 1)))
+        (st = alloc(&md_psnap_ke, 1)) || (st = alloc(&md_fail, 1)) || (st = alloc(&md_t0, 1)))
         return st;
+    GR_CUDA(cudaMemcpy(md_t0, &p->temperature, sizeof(double), cudaMemcpyHostToDevice));
     {
         double ke0 = 0.0;
         for (int i = 0; i < N; ++i)
@@ -297,7 +301,7 @@ gr_status NbSystem::md_step_launch(cudaStream_t s, bool fuse_prep) {
     md.rc = md_rc;
     md.ke = md_ke;
     md.failures = md_fail;
-    md.t0 = mdp.temperature;
+    md.t0 = md_t0;
     md.tau = mdp.tau;
     md.dof = md_dof;
     // the next evaluation keeps this period's lists (no rebuild): its water
@@ -476,6 +480,10 @@ gr_status gr_md_set_temperature(gr_ctx* ctx, double t0, int32_t rescale_velociti
         set_error("gr_md_set_temperature: t0 must be positive");
         return GR_ERR_INVALID;
     }
+    // the bath temperature lives in device memory (k_md_step reads it every
+    // step): recorded step graphs stay valid, and the write is ordered after
+    // the steps already enqueued on this context's stream
+    GR_CUDA(cudaMemcpyAsync(S.md_t0, &t0, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     if (rescale_velocities) {
         // Replica::rescale_velocities (replica.rs:355-371): scale to t0 from the
         // instantaneous temperature over 3N degrees of freedom
@@ -485,7 +493,7 @@ gr_status gr_md_set_temperature(gr_ctx* ctx, double t0, int32_t rescale_velociti
         const double t_now = 2.0 * (double(ke) / gnb::kEnergyScale) / (3.0 * S.N * 0.00831446261815324);
         if (!(t_now > 0.0)) {
             S.mdp.temperature = t0;
-            S.alloc_gen++;
+            GR_CUDA(cudaStreamSynchronize(ctx->stream));
             return GR_OK;
         }
         const double f = std::sqrt(t0 / t_now);
@@ -495,7 +503,8 @@ gr_status gr_md_set_temperature(gr_ctx* ctx, double t0, int32_t rescale_velociti
         GR_CUDA(cudaGetLastError());
     }
     S.mdp.temperature = t0;
-    S.alloc_gen++;  // the thermostat target is a kernel parameter of recorded graphs
+    // complete before returning: a batch launches its members' steps on its own stream
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
     return GR_OK;
 }
 

@@ -96,6 +96,7 @@ class NbSystem {
     double *md_pos_snap = nullptr, *md_vel_snap = nullptr;
     long long* md_ke = nullptr;      // [2]: kinetic energy entering the next step, accumulator
     long long* md_ke_snap = nullptr;
+    double* md_t0 = nullptr;         // [1] Berendsen bath temperature, read by k_md_step every step
     double md_dof = 0.0;
     int* md_fail = nullptr;
     long long* md_err_host = nullptr;  // pinned

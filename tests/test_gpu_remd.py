@@ -57,3 +57,37 @@ def test_replica_exchange_reproducible_and_consistent():
             r.close()
     assert finals[0][0] == finals[1][0]
     assert all(np.array_equal(a, b) for a, b in zip(finals[0][1], finals[1][1]))
+
+
+def test_temperature_change_keeps_batch_graphs_and_matches_standalone():
+    """The bath temperature is read from device memory by the MD step kernel, so an
+    exchange (gr_md_set_temperature) between batch steps records no graph again (the
+    members' own launch counters, which only recording advances, stay put) and the
+    trajectories equal standalone runs with the same temperature change, bit for bit."""
+    from gromos_nb.nonbonded import Batch
+
+    T = [300.0, 330.0]
+    rs = replicas(2, T)
+    b = Batch()
+    for r in rs:
+        b.add(r)
+    b.md_run(7)
+    before = [r.launches() for r in rs]
+    rs[0].md_set_temperature(330.0, rescale_velocities=False)
+    rs[1].md_set_temperature(300.0, rescale_velocities=False)
+    b.md_run(8)
+    assert [r.launches() for r in rs] == before
+    got = [r.md_state() for r in rs]
+    b.close()
+    for r in rs:
+        r.close()
+    alone = replicas(2, T)
+    alone[0].md_run(7)
+    alone[1].md_run(7)
+    alone[0].md_set_temperature(330.0, rescale_velocities=False)
+    alone[1].md_set_temperature(300.0, rescale_velocities=False)
+    for r, (x, v) in zip(alone, got):
+        r.md_run(8)
+        xa, va = r.md_state()
+        assert np.array_equal(x, xa) and np.array_equal(v, va)
+        r.close()
