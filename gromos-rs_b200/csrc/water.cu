@@ -410,9 +410,12 @@ __global__ void __launch_bounds__(128, 4) k_water_force(const SysDev* __restrict
                         const float y = (a == 0 && b == 0) ? r0y : (pyk[a] + shy) - qy[b];
                         const float z = (a == 0 && b == 0) ? r0z : (pzk[a] + shz) - qz[b];
                         const float r2 = fmaf(x, x, fmaf(y, y, z * z));
-                        const float ri = r2 < 1e-10f ? 0.f : rsqrt_fast(r2);
+                        // an atom pair at r^2 < 1e-10 contributes nothing (innerloops.rs:32):
+                        // 1/r and the charge product (hence the CRF constant) are zero
+                        const bool zero = r2 < 1e-10f;
+                        const float ri = zero ? 0.f : rsqrt_fast(r2);
                         const float ri2 = ri * ri;
-                        const float q = wp.qq[t];
+                        const float q = zero ? 0.f : wp.qq[t];
                         ecrf = fmaf(q, fmaf(-wp.crf2, r2, ri) - wp.crfc, ecrf);
                         float fs = q * fmaf(ri, ri2, wp.crf3);
                         if (!LJ00 || t == 0) {

@@ -201,6 +201,30 @@ def test_water_kernel_variants_twin_range_steps(layout, width):
     compare_eval(s, "fixed", steps=4, move=0.002, seed=6, cluster_size=width, layout=layout)
 
 
+def coincident_water_system():
+    """512 SPC waters with one hydrogen placed exactly on another water's hydrogen: water b
+    (water 0's nearest neighbour) is moved rigidly so that its atom 1 sits on water 0's atom 2."""
+    s = generators.spc_water_system(512, box=generators.box_for_waters(512), seed=77, rcutp=0.8, rcutl=1.2,
+                                    nsnb=5)
+    pos = s.pos.copy()
+    o = pos[0::3]
+    d = o[1:] - o[0]
+    d -= s.box * np.round(d / s.box)
+    b = 1 + int(np.argmin((d * d).sum(1)))
+    pos[3 * b:3 * b + 3] += pos[2] - pos[3 * b + 1]
+    out = s.copy()
+    out.pos = pos
+    out.name = "spc512_coincident_h"
+    return out
+
+
+@pytest.mark.parametrize("layout,width", WATER_KERNELS)
+def test_water_kernels_coincident_atoms(layout, width):
+    """An atom pair at r^2 < 1e-10 contributes nothing, as lj_crf_interaction's guard
+    (innerloops.rs:32) has it: every solvent kernel's slow path against the oracle."""
+    compare_eval(coincident_water_system(), "fixed", cluster_size=width, layout=layout)
+
+
 def test_deterministic_bits():
     s = generators.config1_spc1000()
     ff = Forcefield(s, kernel="fixed")
