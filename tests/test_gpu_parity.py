@@ -11,6 +11,8 @@
   largest magnitude in the set (FP32 pair arithmetic).
 * dH/dlambda: relative 1e-5 (FP64 perturbation kernels).
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -223,6 +225,24 @@ def test_water_kernels_coincident_atoms(layout, width):
     """An atom pair at r^2 < 1e-10 contributes nothing, as lj_crf_interaction's guard
     (innerloops.rs:32) has it: every solvent kernel's slow path against the oracle."""
     compare_eval(coincident_water_system(), "fixed", cluster_size=width, layout=layout)
+
+
+def vacuum_droplet():
+    s = generators.spc_water_system(216, box=generators.box_for_waters(216), seed=91, rcutp=0.8, rcutl=1.2, nsnb=2)
+    s.params = dataclasses.replace(s.params, boundary=0)
+    s.name = "spc216_vacuum"
+    return s
+
+
+@pytest.mark.parametrize("layout,width", WATER_KERNELS)
+def test_water_kernels_vacuum(layout, width):
+    """Solvent without periodic boundaries (no images, the cell grid spans the molecules'
+    extent): every solvent kernel over twin-range steps with motion against the oracle."""
+    compare_eval(vacuum_droplet(), "fixed", steps=3, move=0.002, seed=5, cluster_size=width, layout=layout)
+
+
+def test_plain_kernel_vacuum():
+    compare_eval(vacuum_droplet(), "plain", tol_rms=1e-4, tol_e=1e-4)
 
 
 def test_deterministic_bits():
