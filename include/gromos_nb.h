@@ -111,7 +111,8 @@ typedef struct {
     int32_t kernel;              /* GR_KERNEL_* */
     int32_t cluster_size;        /* solvent i-cluster width 4 or 8 (0 = 4) */
     int32_t water_layout;        /* 0 default, 1 lanes share mask bits (width 4), 2 lanes iterate own bits,
-                                    3 lanes stream their own water pairs (width 4, short range) */
+                                    3 lanes stream their own water pairs (width 4, short range), 4 as 2 with
+                                    the atom pairs evaluated two at a time in packed FP32x2 arithmetic */
     int32_t list_capacity;       /* entries per solvent i-cluster list, 0 = sized from the density; a list
                                     that overflows is grown (doubling) and its step evaluated again.  A
                                     gr_set_params call that changes only this field keeps the current
