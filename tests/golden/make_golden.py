@@ -58,7 +58,7 @@ MD_FIXTURES = {"nacl_1water_settle"}
 # Fixtures that gromos-rs's own harness marks #[ignore] (the reason is recorded in the .npz)
 REFERENCE_IGNORES = {
     "aladip_vacuum_fep": "crates/gromos-md/tests/test_gromosXX_references.rs:562 ignores this fixture "
-                         "(PLAN.md: known FEP mismatch with gromosXX)",
+                         "(gromos-rs notes it as a known FEP mismatch with gromosXX)",
 }
 
 
