@@ -8,6 +8,10 @@
 // small members fill the SMs that large ones leave idle.  Each member keeps
 // its own rebuild phase (members may join at any step), so the graph of batch
 // step t depends only on t mod NSNB: NSNB graphs are captured and replayed.
+// Inside a recorded step a member's work depends only on whether it starts a
+// pairlist period there, so phases with the same set of rebuilding members
+// share one recorded graph (members on a common phase need two recordings,
+// not NSNB).
 // After every step a gather kernel collects the members' error flags into
 // pinned host memory; a member whose lists overflowed is rolled back to the
 // snapshot taken at the start of its pairlist period (inside its rebuild
@@ -55,8 +59,12 @@ struct gr_batch {
     float last_ms = 0.f;               // device time of the last gr_batch_md_run / gr_batch_eval
 
     void drop_graphs() {
-        for (auto& x : g)
-            if (x) cudaGraphExecDestroy(x);
+        for (size_t i = 0; i < g.size(); ++i) {  // phases may share one graph: destroy it once
+            if (!g[i]) continue;
+            bool seen = false;
+            for (size_t k = 0; k < i; ++k) seen = seen || g[k] == g[i];
+            if (!seen) cudaGraphExecDestroy(g[i]);
+        }
         g.clear();
         g_launches.clear();
         valid = false;
@@ -132,7 +140,18 @@ gr_status batch_capture(gr_batch* b) {
     for (int i = 0; i < n; ++i) launches0[i] = b->m[i].ctx->sys.launches;
     b->g.assign(b->nsnb, nullptr);
     b->g_launches.assign(b->nsnb, 0);
+    std::vector<std::vector<char>> rebuilds(b->nsnb, std::vector<char>(n, 0));
+    for (int p = 0; p < b->nsnb; ++p)
+        for (int i = 0; i < n; ++i) rebuilds[p][i] = (p + b->m[i].offset) % b->nsnb == 0;
     for (int p = 0; p < b->nsnb; ++p) {
+        int same = -1;  // an earlier phase with the same rebuilding members
+        for (int q = 0; q < p && same < 0; ++q)
+            if (rebuilds[q] == rebuilds[p]) same = q;
+        if (same >= 0) {
+            b->g[p] = b->g[same];
+            b->g_launches[p] = b->g_launches[same];
+            continue;
+        }
         long long l0 = 0;
         for (auto& mb : b->m) l0 += mb.ctx->sys.launches;
         cudaGraph_t graph = nullptr;
@@ -460,6 +479,22 @@ gr_status gr_batch_last_ms(gr_batch* b, float* ms) {
     BATCH_GUARD(b);
     if (!ms) return GR_ERR_INVALID;
     *ms = b->last_ms;
+    return GR_OK;
+}
+
+gr_status gr_batch_phase(gr_batch* b, int32_t* phase, int32_t* period) {
+    BATCH_GUARD(b);
+    if (!phase || !period) return GR_ERR_INVALID;
+    *period = b->nsnb > 0 ? b->nsnb : 1;
+    *phase = -1;
+    for (size_t i = 0; i < b->m.size(); ++i) {
+        const int ph = member_phase(*b, b->m[i]);
+        if (i == 0) *phase = ph;
+        else if (ph != *phase) {
+            *phase = -1;
+            break;
+        }
+    }
     return GR_OK;
 }
 

@@ -20,7 +20,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
-from typing import Dict, List, Optional
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
@@ -429,6 +429,14 @@ class Batch:
         n = C.c_int64(0)
         check(self._L.gr_batch_launches(self._h, C.byref(n)))
         return int(n.value)
+
+    def phase(self) -> Tuple[int, int]:
+        """(phase, period): the step of their pairlist period (NSNB = period) the members
+        take at the next batch step, 0 when every member rebuilds there, -1 when the batch
+        is empty or its members stand at different steps (``gr_batch_phase``)."""
+        ph, per = C.c_int32(0), C.c_int32(0)
+        check(self._L.gr_batch_phase(self._h, C.byref(ph), C.byref(per)))
+        return int(ph.value), int(per.value)
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -275,6 +275,14 @@ gr_status gr_batch_eval(gr_batch* b, int32_t flags);
 gr_status gr_batch_last_ms(gr_batch* b, float* ms);
 /* Kernels launched by the batch's graphs so far. */
 gr_status gr_batch_launches(gr_batch* b, int64_t* n);
+/* Where the members stand in their pairlist periods (no counterpart in
+ * gromos-rs): *period = NSNB, *phase = the step of the period the next batch
+ * step is (0: every member rebuilds its lists there), or -1 when the batch is
+ * empty or its members are at different steps of their periods.  A member
+ * added to the batch starts a period at its first batch step, so adding
+ * members only at phase 0 keeps every member on one phase, which the batch
+ * records with two step graphs instead of NSNB. */
+gr_status gr_batch_phase(gr_batch* b, int32_t* phase, int32_t* period);
 /* Autotuner (no counterpart in gromos-rs): times full pairlist periods
  * (rebuild + long-range refresh + NSNB short-range steps) of the system(s)
  * for every solvent kernel variant -- lane layout x i-cluster width: (2, 4),

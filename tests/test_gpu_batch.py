@@ -271,3 +271,29 @@ def test_batch_member_rollback_after_list_overflow():
     b.close()
     for ff in [small] + others:
         ff.close()
+
+
+def test_batch_phase_reports_the_members_period_step():
+    """gr_batch_phase: members added together share a phase (their graphs are recorded once
+    per distinct set of rebuilding members); a member added mid-period makes it -1, and both
+    keep their standalone trajectories bit for bit."""
+    sy = systems()[:2]
+    b = Batch()
+    assert b.phase()[0] == -1                      # empty
+    a = member(sy[0], 201)
+    b.add(a)
+    assert b.phase() == (0, 5)
+    b.md_run(3)
+    assert b.phase() == (3, 5)
+    c = member(sy[1], 202)
+    b.add(c)
+    assert b.phase() == (-1, 5)                    # a at step 3 of its period, c at step 0
+    b.md_run(9)
+    xa, va = a.md_state()
+    xc, vc = c.md_state()
+    b.close()
+    for ff in (a, c):
+        ff.close()
+    for s, seed, n, (x, v) in ((sy[0], 201, 12, (xa, va)), (sy[1], 202, 9, (xc, vc))):
+        xr, vr = standalone(s, seed, n)
+        assert np.array_equal(x, xr) and np.array_equal(v, vr)
