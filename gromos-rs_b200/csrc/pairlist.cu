@@ -817,12 +817,15 @@ __global__ void __launch_bounds__(kSearchWarps * 32, W == 4 ? 8 : 4) k_water_sea
             __syncwarp();
         }
         __syncwarp();
+        // an overflowing list (more entries than its capacity; the build is redone with
+        // grown lists) writes no further than its capacity
+        const int nws = min(min(cnt_s, kEntBuf), P.wcap), nwl = min(min(cnt_l, kEntBuf), P.wcap);
         if (POPSORT) {
-            sort_write_entries_pop<W>(ebuf_s[w], min(cnt_s, kEntBuf), outs, lane);
-            sort_write_entries_pop<W>(ebuf_l[w], min(cnt_l, kEntBuf), outl, lane);
+            sort_write_entries_pop<W>(ebuf_s[w], nws, outs, lane);
+            sort_write_entries_pop<W>(ebuf_l[w], nwl, outl, lane);
         } else {
-            sort_write_entries(ebuf_s[w], min(cnt_s, kEntBuf), outs, lane);
-            sort_write_entries(ebuf_l[w], min(cnt_l, kEntBuf), outl, lane);
+            sort_write_entries(ebuf_s[w], nws, outs, lane);
+            sort_write_entries(ebuf_l[w], nwl, outl, lane);
         }
         if (lane == 0) {
             if (cnt_s > P.wcap || cnt_l > P.wcap) atomicOr(&s.err[0], ERR_WLIST_OVERFLOW);

@@ -953,7 +953,7 @@ __global__ void __launch_bounds__(128, 3)
                 cnt_n = wn[cn];
                 n_next = clus_n[cn];
                 const uint32_t* __restrict__ ln = wl + static_cast<size_t>(cn) * wcap;
-                raw0 = __ldg(ln + lane);
+                if (lane < wcap) raw0 = __ldg(ln + lane);
                 if (32 + lane < wcap) raw1 = __ldg(ln + 32 + lane);
             }
         };
