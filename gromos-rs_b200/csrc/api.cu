@@ -13,7 +13,9 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -87,13 +89,63 @@ void lambda_params(double lam, int n, double lp[17]) {
     lp[16] = double(n);
 }
 
+// Device memory of every context comes from one stream-ordered pool per GPU
+// that keeps freed blocks for reuse: a context created after another was
+// released (a serving job after a finished one) reuses that memory, and
+// releasing a context synchronises only its own stream -- cudaFree would
+// synchronise the whole device, stalling every other context's work.
+cudaError_t device_pool(cudaMemPool_t* pool) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        if ((e = cudaMemPoolCreate(&pools[dev], &props)) != cudaSuccess) {
+            pools[dev] = nullptr;
+            return e;
+        }
+        uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool until the process exits
+        if ((e = cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
+            return e;
+    }
+    *pool = pools[dev];
+    return cudaSuccess;
+}
+
+// A pool allocation, complete before it returns (so any stream and synchronous
+// copies may use it at once), and its release after the work on this
+// context's stream.  Buffers are reallocated or released only when no other
+// stream has work on them (batch steps synchronise before members change).
+cudaError_t NbSystem::dev_malloc(void** p, size_t n) {
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = device_pool(&pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, n, pool, mem_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(mem_stream);
+    return e;
+}
+
+void NbSystem::dev_free(void* p) {
+    if (!p) return;
+    cudaStreamSynchronize(mem_stream);
+    cudaFreeAsync(p, mem_stream);
+}
+
 NbSystem::~NbSystem() { release(); }
 
 void NbSystem::release() {
-    for (void* p : allocs) cudaFree(p);
+    const bool any = !allocs.empty() || d_sys;
+    for (void* p : allocs) dev_free(p);
     allocs.clear();
-    if (d_sys) cudaFree(d_sys);
+    if (d_sys) dev_free(d_sys);
     d_sys = nullptr;
+    if (any) cudaStreamSynchronize(mem_stream);  // the blocks are back in the pool before the stream goes
     std::memset(&h, 0, sizeof(h));
     d_cg_key = nullptr;
     for (auto& e : ev)
@@ -140,16 +192,17 @@ gr_status NbSystem::alloc(T** p, size_t n) {
     if (*p) {
         for (size_t k = 0; k < allocs.size(); ++k)
             if (allocs[k] == static_cast<void*>(*p)) {
-                cudaFree(*p);
+                dev_free(*p);
                 allocs.erase(allocs.begin() + long(k));
                 break;
             }
         *p = nullptr;
     }
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+    cudaError_t e = dev_malloc(reinterpret_cast<void**>(p), n * sizeof(T));
     if (e != cudaSuccess) {
-        set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        *p = nullptr;
+        set_error(std::string("device allocation: ") + cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? GR_ERR_OOM : GR_ERR_CUDA;
     }
     allocs.push_back(*p);
@@ -417,7 +470,7 @@ gr_status NbSystem::upload(const gr_topology* t) {
     GR_CUDA(cudaMemset(h.acc_long, 0, size_t(acc_size(G)) * sizeof(long long)));
     GR_CUDA(cudaMemset(h.f32_long, 0, size_t(N) * 3 * sizeof(float)));
     GR_CUDA(cudaMemset(h.e64_long, 0, 16 * sizeof(double)));
-    GR_CUDA(cudaMalloc(reinterpret_cast<void**>(&d_sys), sizeof(SysDev)));
+    GR_CUDA(dev_malloc(reinterpret_cast<void**>(&d_sys), sizeof(SysDev)));
     for (auto& e : ev) GR_CUDA(cudaEventCreate(&e));
     for (auto& e : evk) GR_CUDA(cudaEventCreate(&e));
     GR_CUDA(cudaEventCreateWithFlags(&ev_err, cudaEventDisableTiming));
@@ -1378,6 +1431,7 @@ gr_status gr_ctx_create(int device, gr_ctx** out) {
         set_error("gr_ctx_create: stream creation failed");
         return GR_ERR_CUDA;
     }
+    c->sys.mem_stream = c->stream;
     *out = c;
     return GR_OK;
 }
@@ -1392,6 +1446,7 @@ gr_status gr_ctx_destroy(gr_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     ctx->sys.release();
     cudaStreamDestroy(ctx->stream);
+    ctx->sys.mem_stream = nullptr;
     delete ctx;
     return GR_OK;
 }

@@ -57,6 +57,8 @@ struct gr_batch {
     int cap = 0;
     long long launches = 0;
     float last_ms = 0.f;               // device time of the last gr_batch_md_run / gr_batch_eval
+    long long records = 0;             // step graphs recorded (distinct graphs, every membership)
+    double record_s = 0.0;             // host time spent recording and instantiating them
 
     void drop_graphs() {
         for (size_t i = 0; i < g.size(); ++i) {  // phases may share one graph: destroy it once
@@ -119,8 +121,17 @@ gr_status batch_prepare(gr_batch* b, bool need_md) {
     return GR_OK;
 }
 
-// Records the NSNB step graphs.
+gr_status batch_capture_graphs(gr_batch* b);
+
+// Records the NSNB step graphs (host time and count kept for gr_batch_record_stats).
 gr_status batch_capture(gr_batch* b) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const gr_status st = batch_capture_graphs(b);
+    b->record_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return st;
+}
+
+gr_status batch_capture_graphs(gr_batch* b) {
     b->drop_graphs();
     gr_status st;
     const int n = int(b->m.size());
@@ -191,6 +202,7 @@ gr_status batch_capture(gr_batch* b) {
         cudaError_t e2 = cudaStreamEndCapture(b->s0, &graph);
         if (e == cudaSuccess) e = e2;
         if (e == cudaSuccess && !st) e = cudaGraphInstantiate(&b->g[p], graph, 0);
+        if (e == cudaSuccess && !st) b->records += 1;
         if (graph) cudaGraphDestroy(graph);
         long long l1 = 0;
         for (auto& mb : b->m) l1 += mb.ctx->sys.launches;
@@ -479,6 +491,14 @@ gr_status gr_batch_last_ms(gr_batch* b, float* ms) {
     BATCH_GUARD(b);
     if (!ms) return GR_ERR_INVALID;
     *ms = b->last_ms;
+    return GR_OK;
+}
+
+gr_status gr_batch_record_stats(gr_batch* b, int64_t* graphs, double* seconds) {
+    BATCH_GUARD(b);
+    if (!graphs || !seconds) return GR_ERR_INVALID;
+    *graphs = b->records;
+    *seconds = b->record_s;
     return GR_OK;
 }
 

@@ -34,6 +34,9 @@ class NbSystem {
     gr_status download(cudaStream_t s, gr_result* out);
     gr_status pair_counts(cudaStream_t s, long long* n_short, long long* n_long);
     gr_status push_descriptor(cudaStream_t s);
+    cudaError_t dev_malloc(void** p, size_t n);
+    void dev_free(void* p);
+    cudaStream_t mem_stream = nullptr;  // the context's stream: pool allocations and releases are ordered on it
     cudaError_t record_event(cudaEvent_t e, cudaStream_t s);
     int sm_count();
     // Resident blocks per SM of `kernel` at this launch shape, looked up once

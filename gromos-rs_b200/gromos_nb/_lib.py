@@ -150,6 +150,7 @@ _SIGNATURES = {
     "gr_batch_last_ms": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float)]),
     "gr_batch_launches": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_batch_phase": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "gr_batch_record_stats": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
     "gr_ctx_device_bytes": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "gr_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(GrAutotuneResult)]),
     "gr_energy_frames": (C.c_int32, [C.c_void_p, C.c_int32, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]),

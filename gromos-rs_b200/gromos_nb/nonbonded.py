@@ -430,6 +430,12 @@ class Batch:
         check(self._L.gr_batch_launches(self._h, C.byref(n)))
         return int(n.value)
 
+    def record_stats(self) -> Tuple[int, float]:
+        """(step graphs recorded so far, host seconds spent recording them)."""
+        n, sec = C.c_int64(0), C.c_double(0.0)
+        check(self._L.gr_batch_record_stats(self._h, C.byref(n), C.byref(sec)))
+        return int(n.value), float(sec.value)
+
     def phase(self) -> Tuple[int, int]:
         """(phase, period): the step of their pairlist period (NSNB = period) the members
         take at the next batch step, 0 when every member rebuilds there, -1 when the batch

@@ -86,6 +86,10 @@ class Server:
         self.max_resident_jobs = 0
         self.max_resident_bytes = 0
         self.joined_running = 0                # jobs admitted into a batch that was already stepping
+        # host time split of the serving loop (wall-clock seconds)
+        self.setup_s = 0.0                     # job contexts: upload, first pairlist, MD set-up
+        self.step_s = 0.0                      # batch steps, graph recording included
+        self.retire_s = 0.0                    # results read back, contexts released
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -95,6 +99,13 @@ class Server:
 
     # ---- admission / retirement
     def _admit(self) -> None:
+        t0 = time.perf_counter()
+        try:
+            self._admit_jobs()
+        finally:
+            self.setup_s += time.perf_counter() - t0
+
+    def _admit_jobs(self) -> None:
         while self.queue:
             job = self.queue[0]
             est = int(job.system.topo.n_atoms * self.bytes_per_atom)
@@ -127,6 +138,13 @@ class Server:
             self.max_resident_bytes = max(self.max_resident_bytes, self.resident_bytes)
 
     def _retire(self) -> None:
+        t0 = time.perf_counter()
+        try:
+            self._retire_jobs()
+        finally:
+            self.retire_s += time.perf_counter() - t0
+
+    def _retire_jobs(self) -> None:
         for jid in [j for j, (job, _) in self.resident.items() if job.steps_done >= job.n_steps]:
             job, ff = self.resident.pop(jid)
             self.batch.remove(ff)
@@ -144,7 +162,9 @@ class Server:
         if not self.resident:
             return 0
         n = min(self.chunk, min(job.n_steps - job.steps_done for job, _ in self.resident.values()))
+        t0 = time.perf_counter()
         self.gpu_ms += self.batch.md_run(n)
+        self.step_s += time.perf_counter() - t0
         self.steps_run += n
         for job, _ in self.resident.values():
             job.steps_done += n
@@ -168,6 +188,7 @@ class Server:
 
     # ---- report
     def report(self) -> Dict:
+        records, record_s = self.batch.record_stats()
         lat = np.array([j.latency for j in self.done])
         wall = max((j.finished for j in self.done), default=0.0)
         return {
@@ -183,6 +204,13 @@ class Server:
             "max_resident_jobs": self.max_resident_jobs,
             "joined_running": self.joined_running,
             "max_resident_bytes": self.max_resident_bytes,
+            # where the wall time goes: job set-up, batch steps (device time plus the step
+            # graphs recorded on membership changes), retirement; the rest is waiting for arrivals
+            "host_setup_s": self.setup_s,
+            "host_step_s": self.step_s,
+            "host_retire_s": self.retire_s,
+            "graph_records": records,
+            "graph_record_s": record_s,
         }
 
     def close(self) -> None:

@@ -283,6 +283,10 @@ gr_status gr_batch_launches(gr_batch* b, int64_t* n);
  * members only at phase 0 keeps every member on one phase, which the batch
  * records with two step graphs instead of NSNB. */
 gr_status gr_batch_phase(gr_batch* b, int32_t* phase, int32_t* period);
+/* Step graphs the batch has recorded so far (after membership and capacity
+ * changes; phases sharing a graph count once) and the host time spent
+ * recording and instantiating them, in seconds (no counterpart in gromos-rs). */
+gr_status gr_batch_record_stats(gr_batch* b, int64_t* graphs, double* seconds);
 /* Autotuner (no counterpart in gromos-rs): times full pairlist periods
  * (rebuild + long-range refresh + NSNB short-range steps) of the system(s)
  * for every solvent kernel variant -- lane layout x i-cluster width: (2, 4),

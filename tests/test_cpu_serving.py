@@ -67,6 +67,9 @@ class FakeBatch:
     def launches(self):
         return 0
 
+    def record_stats(self):
+        return 0, 0.0
+
     def close(self):
         pass
 

@@ -285,10 +285,13 @@ def test_batch_phase_reports_the_members_period_step():
     assert b.phase() == (0, 5)
     b.md_run(3)
     assert b.phase() == (3, 5)
+    assert b.record_stats()[0] == 2                # a rebuilds at one phase: two distinct step graphs
     c = member(sy[1], 202)
     b.add(c)
     assert b.phase() == (-1, 5)                    # a at step 3 of its period, c at step 0
     b.md_run(9)
+    n_graphs, seconds = b.record_stats()
+    assert n_graphs == 5 and seconds > 0.0         # + {c}, {a}, {} rebuilding: three more
     xa, va = a.md_state()
     xc, vc = c.md_state()
     b.close()
