@@ -147,6 +147,10 @@ def test_results_latency_and_report():
     assert rep["jobs"] == 3 and rep["batch_steps"] == 12
     assert 0 < rep["latency_p50_s"] <= rep["latency_p99_s"]
     assert rep["pair_int_per_s"] > 0
+    # the wall-time split: set-up, batch steps and retirement are timed, graph recording is the batch's
+    assert all(rep[k] >= 0.0 for k in ("host_setup_s", "host_step_s", "host_retire_s", "graph_record_s"))
+    assert rep["host_setup_s"] + rep["host_step_s"] + rep["host_retire_s"] <= rep["wall_s"] + 0.05
+    assert rep["graph_records"] == 0                      # the fake batch records nothing
     for j in jobs:
         assert j.finished >= j.admitted >= 0.0
         assert np.all(j.result_pos == float(j.job_id))   # each job gets its own final state back
